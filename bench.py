@@ -1,0 +1,296 @@
+"""Benchmark: primary-ray throughput of the Gaussian ray tracer.
+
+Workload (default): 1,000,000 Gaussians in 64 clusters, one 1920x1080 view,
+k = 16, alpha_min = 0.01, T_min = 0.01, SH degree 3, camera at radius 12 (the
+configuration the headline metric is quoted on).  A step is one render of
+that view.  Scene data lives in HBM (~360 MB, larger than the 126 MB L2, so
+no explicit L2 flush is done between steps).
+
+Our arm prints one JSON line with
+  value          Mrays/s of the trace kernel launches, inputs resident on the
+                 device, timed with CUDA events on the library's stream
+  e2e            Mrays/s through gt_render with a host (pinned) output buffer,
+                 the device-to-host copy of every image inside the wall-clock
+                 timed region
+  roofline       algorithmic bytes per launch (16 B per pixel + 44 B per
+                 composited entry + 192 B of SH per contributing entry) over
+                 the average trace-kernel time, against the measured HBM peak
+  cpu_baseline   the CPU restatement of the reference algorithm (oracle,
+                 per-round k-buffer traversal), all host threads, on a
+                 stratified pixel subset
+
+``--impl reference`` times only that CPU restatement (the reference itself is
+a browser WebGPU application and cannot run here).
+
+Multi-GPU: ``torchrun --nproc-per-node N bench.py --gpus N``; every rank
+renders the same workload on its own GPU (replicas; the path has no
+exchange), value = total rays of all ranks over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "webgpu-gaussiantracer_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "Mrays/s at 1080p/1M Gaussians, batched vs plain; fwd+bwd ms/view; HBM GB/s"
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "100"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def make_workload(name: str):
+    from gtrace import synth
+    if name == "clusters-1m-1080p":
+        pg, amin, v = synth.clusters_1m_config()
+        desc = "1M Gaussians (64 clusters), 1920x1080, k=16, alpha_min=0.01, T_min=0.01, SH3, camera radius 12"
+    elif name == "small-256":
+        pg, amin, v = synth.small_config()
+        desc = "16,384 Gaussians (uniform), 256x256, k=6, alpha_min=0.01, T_min=0.01, SH3, camera at distance 4"
+    elif name == "clusters-200k-800":
+        raw, amin, v = synth.clusters_200k_config()
+        pg = synth.pack(raw)
+        desc = "200k Gaussians (64 clusters), 800x800, k=8, alpha_min=0.01, T_min=0.01, SH3, camera radius 12"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return pg, amin, v, desc
+
+
+def cpu_port_throughput(pg, amin, v, budget_s: float, threads: int = 0):
+    """Times the CPU restatement of the reference algorithm (oracle, per-round
+    k-buffer traversal) on stratified pixel subsets; returns Mrays/s and the
+    sample description.  Scene preparation is not timed."""
+    from oracle import oracle
+    t0 = time.perf_counter()
+    s = oracle.Scene(pg.gaussiansBuffer, amin, "f32")
+    prep = time.perf_counter() - t0
+    w, h = v.width, v.height
+    stride = 8
+    while True:
+        xs = np.arange(stride // 2, w, stride)
+        ys = np.arange(stride // 2, h, stride)
+        pix = (ys[:, None] * w + xs[None, :]).reshape(-1).astype(np.uint32)
+        t = time.perf_counter()
+        s.render(v.uniforms, w, h, pixels=pix, algo=1, threads=threads)
+        dt = time.perf_counter() - t
+        if dt >= 0.5 * budget_s or stride <= 1:
+            break
+        stride = max(1, int(stride / math.sqrt(max(2.0, 0.6 * budget_s / max(dt, 1e-3)))))
+    return len(pix) / dt / 1e6, len(pix), stride, dt, prep
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="clusters-1m-1080p")
+    ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU baseline work")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+
+    pg, amin, v, desc = make_workload(args.workload)
+    w, h = v.width, v.height
+    rays = w * h
+    threads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            if dist:
+                dist.destroy_process_group()
+            return
+        vals = []
+        sample = None
+        for i in range(args.warmup + args.steps):
+            mr, n, stride, dt, prep = cpu_port_throughput(pg, amin, v, budget_s=max(2.0, 60.0 / (args.steps + 3)))
+            sample = f"{n} pixels (every {stride}th pixel in x and y) of the {w}x{h} view"
+            if i >= args.warmup:
+                vals.append(mr)
+        val = statistics.median(vals)
+        line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "Mrays/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": rays / (val * 1e6) * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded)", "config": {"workload": desc, "width": w, "height": h},
+                "cpu_baseline": {"value": val, "unit": "Mrays/s", "cores": threads, "kind": "port",
+                                 "sample": sample + "; CPU restatement of the reference traversal (oracle algo 1); "
+                                           "the reference runs only as a browser WebGPU app"},
+                "e2e": {"value": val, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    from gtrace.tracer import Context, Scene
+    ctx = Context(local)
+    scene = Scene(ctx, pg.gaussiansBuffer, amin)
+    info = scene.info()
+    out_dev = ctx.device_alloc(rays * 16)
+    # one synchronous render: counters for the algorithmic byte count
+    st0 = ctx.render_device(scene, v.uniforms, w, h, out_dev)
+    alg_bytes = 16 * st0["rays"] + 44 * st0["entries"] + 192 * st0["contributing"]
+    for _ in range(args.warmup):
+        ctx.render_device(scene, v.uniforms, w, h, out_dev, asynchronous=True)
+    ctx.synchronize()
+    ctx.kernel_times()
+    if dist:
+        dist.barrier()
+    n_launch0 = ctx.launch_count()
+    with ClockSampler(local) as clk:
+        ctx.synchronize()
+        ctx.timer_start()
+        for _ in range(args.steps):
+            ctx.render_device(scene, v.uniforms, w, h, out_dev, asynchronous=True)
+        ms = ctx.timer_stop()
+    n_launch = ctx.launch_count() - n_launch0
+    ktimes = ctx.kernel_times()
+    ms_step = ms / args.steps
+    if dist:
+        import torch
+        t = torch.tensor([ms_step], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_step = float(t.item())
+    value = world * rays / (ms_step * 1e-3) / 1e6
+
+    # end to end: host output buffer (pinned), copy inside the timed region
+    host = ctx.host_alloc(rays * 16, np.float32, (h, w, 4))
+    for _ in range(2):
+        ctx.render(scene, v.uniforms, w, h, out=host)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.render(scene, v.uniforms, w, h, out=host)
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if dist:
+        import torch
+        t = torch.tensor([e2e_s], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = world * rays / e2e_s / 1e6
+    checksum = float(np.float64(host[..., :3]).sum())
+    ctx.host_free(host)
+    ctx.device_free(out_dev)
+
+    peak, peak_kind = load_peaks()
+    k_ms = statistics.mean(ktimes) if ktimes else ms_step
+    achieved = alg_bytes / (k_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "trace_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(args.workload)
+        except Exception:
+            traffic = None
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        mr, n, stride, dt, prep = cpu_port_throughput(pg, amin, v, budget_s=args.cpu_budget)
+        cpu = {"value": mr, "unit": "Mrays/s", "cores": threads, "kind": "port",
+               "sample": f"{n} pixels (every {stride}th pixel in x and y) of the {w}x{h} view, {dt:.1f} s; "
+                         f"CPU restatement of the reference traversal"}
+    clocks = clk.summary()
+    line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, no dataset)",
+            "config": {"workload": desc, "width": w, "height": h, "n_gaussians": int(info["n_particles"]),
+                       "n_proxies": int(info["n_kept"]), "k": 16 if "1m" in args.workload else None,
+                       "scene_build_ms": info["build_ms"], "bvh_depth": info["bvh_depth"],
+                       "l2": "inputs larger than L2 (scene %.0f MB > 126 MB), no flush" % (info["device_bytes"] / 1e6),
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "alg_bytes_per_launch": alg_bytes, "kernel_ms": k_ms},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": 112 + 256,
+                    "d2h_bytes_per_step": rays * 16},
+            "gpu_launches": n_launch, "clocks": clocks,
+            "counters": {k2: st0[k2] for k2 in ("rounds", "entries", "contributing", "proxy_tests", "node_visits",
+                                                 "anyhits")},
+            "image_checksum": checksum}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    scene.close()
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

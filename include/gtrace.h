@@ -1,0 +1,279 @@
+/*
+ * gtrace.h — C ABI of the B200-native Gaussian ray tracer.
+ *
+ * The reference (DeepGPU/WebGPU-GaussianTracer) renders through the WebRTX
+ * emulation of the Vulkan ray-tracing API on WebGPU:
+ *
+ *   device.createRayTracingAccelerationContainer(tlasDesc)       webrtx/src/patch.ts:211-213
+ *   device.hostBuildRayTracingAccelerationContainer(tlas)        webrtx/src/patch.ts:216-219
+ *   passEncoder.traceRays(device, sbt, width, height)            webrtx/src/pass_encoder.ts:35-65
+ *
+ * with the bind group of src/main.ts:497-512 (binding 0 = TLAS, 1 = RGBA-f32
+ * pixel buffer, 2 = packed particle buffer, 3 = 112-byte uniform block).
+ * This header replaces that call chain with plain C: a scene handle built on
+ * the GPU from the same packed particle buffer, and one render call that
+ * takes the same uniform block and writes the same pixel buffer.
+ *
+ * Conventions
+ *   - Every entry point returns a gt_status; GT_OK is 0.  No entry point
+ *     aborts, traps or throws.  gt_last_error() gives a one-line message for
+ *     the last failing call on a context.
+ *   - The caller owns every buffer it passes.  The library never keeps a
+ *     caller pointer after the call returns.  Context and scene handles are
+ *     opaque and owned by the library.
+ *   - A pointer is a host pointer unless the matching GT_*_DEVICE flag is set,
+ *     in which case it is a device pointer on the context's GPU.
+ *   - One context owns one CUDA stream.  Calls on one context must be
+ *     serialised by the caller; different contexts are independent.
+ *   - Calls are synchronous unless GT_FLAG_ASYNC is given (device buffers
+ *     only); an asynchronous call returns once its work is queued.
+ */
+#ifndef GTRACE_H
+#define GTRACE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GT_ABI_VERSION 1u
+
+/* ---------------------------------------------------------------- status */
+typedef int32_t gt_status;
+enum {
+  GT_OK = 0,
+  GT_ERR_INVALID_ARG = 1,     /* bad pointer, size, k, stride ...            */
+  GT_ERR_OOM = 2,             /* device or host allocation failed            */
+  GT_ERR_CUDA = 3,            /* a CUDA runtime call failed                  */
+  GT_ERR_DEVICE_TIMEOUT = 4,  /* a device loop hit its iteration limit       */
+  GT_ERR_STACK_OVERFLOW = 5,  /* traversal stack overflowed (status word)    */
+  GT_ERR_UNSUPPORTED = 6,     /* valid request this build does not support  */
+  GT_ERR_NO_DEVICE = 7        /* no CUDA device, or the ordinal is invalid   */
+};
+
+/* ----------------------------------------------------------------- flags */
+#define GT_FLAG_INPUT_DEVICE   0x1u  /* input buffers are device pointers     */
+#define GT_FLAG_OUTPUT_DEVICE  0x2u  /* output buffers are device pointers    */
+#define GT_FLAG_ASYNC          0x4u  /* do not wait (device buffers only)     */
+#define GT_FLAG_ACCUMULATE     0x8u  /* backward: add into dL_dparams         */
+
+/* -------------------------------------------------------- opaque handles */
+typedef struct gt_context gt_context;
+typedef struct gt_scene gt_scene;
+
+/* ------------------------------------------------------ uniform block
+ * Byte-identical to the reference's 112-byte `rtUniforms` block
+ * (src/GS_shader.ts:96-108), packed by src/main.ts:516-534. */
+typedef struct gt_uniforms {
+  float to_world[16];          /*   0  camera matrix, column-major: right, up, back, position */
+  float camera_aspect[2];      /*  64  tan(hfov/2), tan(hfov/2) * height / width            */
+  float t_min;                 /*  72                                                       */
+  float t_max;                 /*  76                                                       */
+  float T_min;                 /*  80  transmittance cutoff                                 */
+  float alpha_min;             /*  84  compositing threshold                                */
+  uint32_t k;                  /*  88  hit_array_size: hits collected per round (1..32)     */
+  uint32_t sh_degree_max;      /*  92  0..3                                                 */
+  uint32_t accumulated_frames; /*  96  progressive-average frame index                      */
+  uint32_t early_stop;         /* 100  stop before round `early_stop`; 0xFFFFFFFF = off      */
+  uint32_t debug_mode;         /* 104  0 = render, 1 = proxy view, 2 = any-hit count        */
+  uint32_t _pad;               /* 108                                                       */
+} gt_uniforms;
+
+/* Per-particle record of the packed buffer: the std430 `GaussianParticle`
+ * (src/GS_shader.ts:78-89, packed by src/GS_ply.ts:199-252): position vec3 @0,
+ * scale vec3 @16, rotation (w,x,y,z) vec4 @32, opacity f32 @48, sh vec3[16]
+ * (array stride 16) @64.  320 bytes for SH degree 3. */
+#define GT_PARTICLE_STRIDE 320u
+#define GT_PARAMS_PER_PARTICLE 59u   /* 3 pos + 3 scale + 4 rot + 1 opacity + 48 sh */
+
+/* ----------------------------------------------------------- statistics */
+typedef struct gt_render_stats {
+  float kernel_ms;        /* device time of the trace kernel (CUDA events)        */
+  float total_ms;         /* device time of the whole call, copies included       */
+  uint64_t rays;          /* primary rays traced                                  */
+  uint64_t rounds;        /* traversal rounds, summed over rays                   */
+  uint64_t entries;       /* valid hit entries composited (any alpha)             */
+  uint64_t contributing;  /* entries with alpha > alpha_min                       */
+  uint64_t proxy_tests;   /* ray-proxy tests                                      */
+  uint64_t node_visits;   /* BVH nodes popped                                     */
+  uint64_t anyhits;       /* front-face proxy hits offered to the k-buffer         */
+  uint32_t status_flags;  /* device status word (0 = clean)                       */
+  uint32_t _pad;
+} gt_render_stats;
+
+typedef struct gt_scene_info {
+  uint64_t n_particles;   /* particles in the packed buffer                       */
+  uint64_t n_kept;        /* particles with opacity > alpha_min (proxies)         */
+  uint64_t device_bytes;  /* device memory held by the scene                      */
+  uint32_t bvh_depth;     /* deepest leaf                                         */
+  uint32_t _pad;
+  float build_ms;         /* device time of the GPU build                         */
+  float bounds[6];        /* world AABB of the proxies: min xyz, max xyz          */
+  float _pad2;
+} gt_scene_info;
+
+/* ============================================================ context */
+
+/* Library version (GT_ABI_VERSION of the built library). */
+uint32_t gt_version(void);
+
+/* Creates a context on CUDA device `device`.  Replaces the adapter/device
+ * request of src/main.ts:396-427. */
+gt_status gt_context_create(int device, gt_context** out);
+gt_status gt_context_destroy(gt_context* ctx);
+
+/* Copies the last error message of `ctx` (NUL-terminated, truncated to
+ * `len`).  With ctx == NULL it reports the last context-less error (for
+ * example a failed gt_context_create). */
+gt_status gt_last_error(const gt_context* ctx, char* buf, size_t len);
+
+/* ============================================================== scene */
+
+/* Builds a scene from the packed particle buffer.
+ * Replaces gaussianSceneToBvh (src/main.ts:30-111) together with
+ * createRayTracingAccelerationContainer/hostBuildRayTracingAccelerationContainer
+ * (webrtx/src/patch.ts:211-219 → webrtx/src/wasm_bvh_builder.ts:260-377 →
+ * webrtx/bvh/src/lib.rs:254-347, 512-603) and the shader binding table of
+ * src/main.ts:335-393.
+ *   packed        n records of `stride_bytes` (>= 320) in the layout above,
+ *                 already activated (scale = exp, unit quaternion, sigmoid
+ *                 opacity), exactly what PackedGaussians.gaussiansBuffer holds
+ *   alpha_min     proxy cut: particle i gets a proxy iff opacity > alpha_min;
+ *                 its icosahedron is scaled by sqrt(2 ln(opacity/alpha_min))
+ *                 (src/main.ts:79-87).  A double, like the JS number it replaces.
+ *   flags         GT_FLAG_INPUT_DEVICE if `packed` is a device pointer
+ * The build (proxy transforms, Morton codes, radix sort, hierarchy, refit)
+ * runs on the GPU.  n == 0 gives an empty scene that renders black. */
+gt_status gt_scene_create(gt_context* ctx, const void* packed, uint64_t n,
+                          uint32_t stride_bytes, double alpha_min,
+                          uint32_t flags, gt_scene** out);
+gt_status gt_scene_destroy(gt_scene* scene);
+gt_status gt_scene_get_info(const gt_scene* scene, gt_scene_info* info);
+
+/* ============================================================= render */
+
+/* Renders one view.  Replaces traceRays (webrtx/src/pass_encoder.ts:35-65),
+ * i.e. one invocation of the ray-generation shader per pixel
+ * (src/GS_shader.ts:275-309) with its tracePath rounds (:192-273), any-hit
+ * k-buffer (:323-367) and compositing.
+ *   u          the 112-byte uniform block (debug_mode 0, 1 and 2 are supported)
+ *   w, h       image size; any value >= 1 (the reference needs multiples of 8)
+ *   out_rgba   w*h*4 floats, pixel (x, y) at index 4*(w*y + x); RGB = radiance,
+ *              A = 1 (src/GS_shader.ts:300-301)
+ *   flags      GT_FLAG_OUTPUT_DEVICE, GT_FLAG_ASYNC
+ *   stats      optional (NULL allowed); not filled for asynchronous calls */
+gt_status gt_render(gt_context* ctx, const gt_scene* scene, const gt_uniforms* u,
+                    uint32_t w, uint32_t h, float* out_rgba, uint32_t flags,
+                    gt_render_stats* stats);
+
+/* Parity/inspection variant of gt_render: for the `n_pix` pixel indices
+ * (w*y + x) in `pixels` it records the composited hit sequence, in the order
+ * entries were composited: particle index, hit t and alpha of each valid
+ * k-buffer entry (src/GS_shader.ts:250-269), at most `max_entries` per pixel.
+ * out_count[i] is the full number of valid entries of pixel i (it may exceed
+ * max_entries; only the first max_entries are stored).  out_rounds[i] is the
+ * number of traversal rounds.  out_rgba (4 floats per listed pixel) may be
+ * NULL.  All buffers are host buffers. */
+gt_status gt_render_hits(gt_context* ctx, const gt_scene* scene, const gt_uniforms* u,
+                         uint32_t w, uint32_t h, const uint32_t* pixels, uint32_t n_pix,
+                         uint32_t max_entries, uint32_t* out_pidx, float* out_t,
+                         float* out_alpha, uint32_t* out_count, uint32_t* out_rounds,
+                         float* out_rgba);
+
+/* ============================================================ backward
+ * No counterpart in the reference (it has no training path, README.md:69). */
+typedef struct gt_bwd_opts {
+  uint32_t mode;          /* 0 = auto (checkpoint if it fits), 1 = checkpoint, 2 = replay */
+  uint32_t max_rounds;    /* per-ray round capacity of the checkpoint; 0 = 64            */
+  uint64_t mem_budget;    /* bytes the checkpoint may use; 0 = 1/2 of free device memory */
+  uint32_t used_mode;     /* out: 1 = checkpoint, 2 = replay                              */
+  uint32_t _pad;
+  float fwd_ms;           /* out: device time of the forward (checkpointing) pass         */
+  float bwd_ms;           /* out: device time of the adjoint pass                         */
+} gt_bwd_opts;
+
+/* Gradient of a loss with respect to every particle parameter, given the
+ * gradient with respect to the rendered RGBA image.
+ *   dL_drgba     w*h*4 floats (the A channel is ignored: the rendered A is 1)
+ *   dL_dparams   59 * n floats, parameter-major (SoA): row p holds parameter p
+ *                of every particle.  Rows: 0-2 position, 3-5 scale,
+ *                6-9 rotation (w,x,y,z as stored), 10 opacity, 11-58 sh
+ *                (coefficient c, channel ch at row 11 + 3*c + ch).  Particles
+ *                without a proxy get 0.  Overwritten unless GT_FLAG_ACCUMULATE.
+ *   flags        GT_FLAG_INPUT_DEVICE (dL_drgba), GT_FLAG_OUTPUT_DEVICE
+ *                (dL_dparams), GT_FLAG_ACCUMULATE
+ * Hit sets are held fixed (the proxy geometry is piecewise constant); the
+ * response, opacity, SH colour and compositing are differentiated exactly. */
+gt_status gt_backward(gt_context* ctx, const gt_scene* scene, const gt_uniforms* u,
+                      uint32_t w, uint32_t h, const float* dL_drgba,
+                      float* dL_dparams, uint32_t flags, gt_bwd_opts* opts,
+                      gt_render_stats* stats);
+
+/* ============================================================= batches
+ * No counterpart in the reference.  Many views of several scenes, traced by
+ * one persistent kernel launch (captured in a CUDA graph and replayed when
+ * the batch shape repeats). */
+typedef struct gt_batch_item {
+  const gt_scene* scene;
+  gt_uniforms u;          /* per-view uniform block (its k is used)            */
+  uint32_t w, h;
+  float* out_rgba;        /* w*h*4 floats; host unless GT_FLAG_OUTPUT_DEVICE  */
+  const float* dL_drgba;  /* backward batches only                              */
+} gt_batch_item;
+
+gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items, uint32_t count,
+                          uint32_t flags, gt_render_stats* stats);
+
+/* Accumulates, per scene, the gradients of all its views in one launch.
+ * dL_dparams[s] receives the sum over the items whose scene is scenes[s]. */
+gt_status gt_backward_batch(gt_context* ctx, const gt_batch_item* items, uint32_t count,
+                            const gt_scene* const* scenes, float* const* dL_dparams,
+                            uint32_t n_scenes, uint32_t flags, gt_bwd_opts* opts,
+                            gt_render_stats* stats);
+
+/* ============================================================ tuning
+ * No counterpart in the reference.  Times the tracer's launch shapes on the
+ * given view and caches the fastest per (GPU, scene-size bucket, image-size
+ * bucket, k).  gt_render and gt_render_batch use the cached choice. */
+typedef struct gt_tune_result {
+  uint32_t block_threads; /* threads per block                                  */
+  uint32_t blocks_per_sm; /* resident blocks per SM of the persistent grid      */
+  uint32_t tile_w, tile_h;/* pixel tile a warp takes per work-stealing step     */
+  float best_ms;          /* fastest trace time measured                        */
+  float default_ms;       /* trace time of the default launch shape             */
+} gt_tune_result;
+
+gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const gt_uniforms* u,
+                      uint32_t w, uint32_t h, gt_tune_result* result);
+/* Drops every cached tuning result of the context. */
+gt_status gt_autotune_reset(gt_context* ctx);
+
+/* ====================================================== device helpers
+ * For callers without a CUDA binding of their own (the N-API addon, the
+ * benchmark): plain device buffers on the context's GPU, and CUDA-event
+ * timing on the context's stream. */
+gt_status gt_device_alloc(gt_context* ctx, uint64_t bytes, void** out);
+gt_status gt_device_free(gt_context* ctx, void* ptr);
+/* Page-locked host buffers (fast host<->device copies). */
+gt_status gt_host_alloc(gt_context* ctx, uint64_t bytes, void** out);
+gt_status gt_host_free(gt_context* ctx, void* ptr);
+/* kind: 0 = host to device, 1 = device to host, 2 = device to device. */
+gt_status gt_memcpy(gt_context* ctx, void* dst, const void* src, uint64_t bytes, int kind);
+gt_status gt_synchronize(gt_context* ctx);
+/* Records a CUDA event on the context stream; gt_timer_stop records a second
+ * one, waits for it and returns the elapsed device milliseconds. */
+gt_status gt_timer_start(gt_context* ctx);
+gt_status gt_timer_stop(gt_context* ctx, float* ms);
+/* Device durations of the trace-kernel launches made since the previous call
+ * (at most `max`, oldest first; each launch is bracketed by CUDA events on
+ * the context stream).  Waits for them to finish. */
+gt_status gt_kernel_times(gt_context* ctx, float* out_ms, uint32_t max, uint32_t* n);
+/* Number of kernel launches the library has made on this context. */
+gt_status gt_launch_count(const gt_context* ctx, uint64_t* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GTRACE_H */

@@ -1,0 +1,225 @@
+"""GPU parity: the CUDA tracer against the oracle's float build.
+
+The tracer and the oracle follow the same binary32 operation order, so
+images, hit sequences, hit t values and alphas must match bit for bit.  The
+oracle's double build gives the FP64 error statistics."""
+import numpy as np
+import pytest
+
+from conftest import small_scene, view
+from oracle import oracle
+from gtrace import synth
+from gtrace import _lib as L
+from gtrace.tracer import Scene
+from gtrace.uniforms import with_fields
+
+pytestmark = pytest.mark.gpu
+
+
+def _both(ctx, packed, amin):
+    return Scene(ctx, packed, amin), oracle.Scene(packed, amin, "f32")
+
+
+def _assert_hits_equal(got, ref, max_entries):
+    np.testing.assert_array_equal(got["count"], ref["count"])
+    np.testing.assert_array_equal(got["rounds"], ref["rounds"])
+    n = np.minimum(got["count"], max_entries)
+    for q in range(len(n)):
+        m = n[q]
+        np.testing.assert_array_equal(got["pidx"][q, :m], ref["pidx"][q, :m])
+        np.testing.assert_array_equal(got["t"][q, :m].view(np.uint32), ref["t"][q, :m].view(np.uint32))
+        np.testing.assert_array_equal(got["alpha"][q, :m].view(np.uint32), ref["alpha"][q, :m].view(np.uint32))
+
+
+@pytest.mark.parametrize("k", [1, 2, 4, 6, 8, 11, 16, 24, 32])
+def test_image_bit_exact_across_k(ctx, k):
+    pg = small_scene(n=2048, seed=7)
+    g, o = _both(ctx, pg.gaussiansBuffer, 0.01)
+    w, h = 64, 48
+    v = view(w, h, k=k)
+    img = ctx.render(g, v.uniforms, w, h)
+    ref, _ = o.render(v.uniforms, w, h)
+    np.testing.assert_array_equal(img.reshape(-1, 4).view(np.uint32), ref.view(np.uint32))
+
+
+@pytest.mark.parametrize("k", [1, 6, 16])
+def test_hit_sequences_bit_exact(ctx, k):
+    pg = small_scene(n=2048, seed=9)
+    g, o = _both(ctx, pg.gaussiansBuffer, 0.01)
+    w, h = 40, 30
+    v = view(w, h, k=k)
+    pix = np.arange(w * h, dtype=np.uint32)
+    got = ctx.render_hits(g, v.uniforms, w, h, pix, max_entries=256)
+    _, ref = o.render(v.uniforms, w, h, pixels=pix, max_entries=256)
+    _assert_hits_equal(got, ref, 256)
+    assert got["count"].max() > k  # several rounds happened
+
+
+def test_small_config_full_image(ctx):
+    """16,384 Gaussians, 256x256, k = 6, alpha_min 0.01, T_min 0.01: every
+    pixel bit-exact; hit sequences of a stratified subset equal; FP64 RMSE."""
+    pg, amin, v = synth.small_config()
+    g, o = _both(ctx, pg.gaussiansBuffer, amin)
+    img, st = ctx.render(g, v.uniforms, v.width, v.height, stats=True)
+    ref, rh = o.render(v.uniforms, v.width, v.height, max_entries=0)
+    np.testing.assert_array_equal(img.reshape(-1, 4).view(np.uint32), ref.view(np.uint32))
+    assert st["rays"] == v.width * v.height
+    assert st["entries"] == int(rh["count"].sum())
+    pix = np.arange(0, v.width * v.height, 97, dtype=np.uint32)
+    got = ctx.render_hits(g, v.uniforms, v.width, v.height, pix, max_entries=256)
+    _, ref_h = o.render(v.uniforms, v.width, v.height, pixels=pix, max_entries=256)
+    _assert_hits_equal(got, ref_h, 256)
+    o64 = oracle.Scene(pg.gaussiansBuffer, amin, "f64")
+    r64, _ = o64.render(v.uniforms, v.width, v.height)
+    rmse = float(np.sqrt(np.mean((img.reshape(-1, 4)[:, :3] - r64[:, :3]) ** 2)))
+    assert rmse < 1e-4
+
+
+@pytest.mark.parametrize("w,h", [(1, 1), (37, 23), (9, 5), (130, 7)])
+def test_any_image_size(ctx, w, h):
+    """Sizes need not be multiples of 8 (the reference requires that,
+    webrtx/src/pass_encoder.ts:52-56)."""
+    pg = small_scene(n=800, seed=4)
+    g, o = _both(ctx, pg.gaussiansBuffer, 0.01)
+    v = view(w, h, k=4)
+    img = ctx.render(g, v.uniforms, w, h)
+    ref, _ = o.render(v.uniforms, w, h)
+    np.testing.assert_array_equal(img.reshape(-1, 4).view(np.uint32), ref.view(np.uint32))
+
+
+def test_empty_and_culled_scenes(ctx):
+    v = view(16, 16)
+    empty = Scene(ctx, np.zeros((0, 80), np.float32), 0.01)
+    img = ctx.render(empty, v.uniforms, 16, 16)
+    assert (img[..., :3] == 0).all() and (img[..., 3] == 1).all()
+    pg = small_scene(n=100, seed=1)
+    rec = pg.gaussiansBuffer.copy()
+    rec[:, 12] = 0.005  # every opacity below alpha_min: no proxies
+    culled = Scene(ctx, rec, 0.01)
+    assert culled.info()["n_kept"] == 0
+    img = ctx.render(culled, v.uniforms, 16, 16)
+    assert (img[..., :3] == 0).all()
+
+
+def test_single_proxy_scene(ctx):
+    rec = np.zeros((1, 80), np.float32)
+    rec[0, 4:7] = 0.3
+    rec[0, 8] = 1.0
+    rec[0, 12] = 0.9
+    rec[0, 16:19] = (0.5, 0.1, -0.3)
+    g, o = _both(ctx, rec, 0.01)
+    assert g.info()["n_kept"] == 1
+    v = view(32, 32, k=2)
+    img = ctx.render(g, v.uniforms, 32, 32)
+    ref, _ = o.render(v.uniforms, 32, 32)
+    np.testing.assert_array_equal(img.reshape(-1, 4).view(np.uint32), ref.view(np.uint32))
+    assert img[..., :3].max() > 0
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_debug_modes(ctx, mode):
+    """debugMode 1 (closest proxy hit coloured by SH along the ray) and 2
+    (front-face hit count, bucketed) against the oracle."""
+    pg = small_scene(n=1500, seed=8)
+    g, o = _both(ctx, pg.gaussiansBuffer, 0.2)
+    v = view(48, 32, k=6, debug_mode=mode)
+    img = ctx.render(g, v.uniforms, 48, 32)
+    ref, _ = o.render(v.uniforms, 48, 32)
+    np.testing.assert_array_equal(img.reshape(-1, 4).view(np.uint32), ref.view(np.uint32))
+
+
+def test_uniform_variants(ctx):
+    pg = small_scene(n=1500, seed=12)
+    g, o = _both(ctx, pg.gaussiansBuffer, 0.05)
+    base = view(32, 24, k=4).uniforms
+    for u in [with_fields(base, early_stop=1), with_fields(base, early_stop=3), with_fields(base, T_min=0.5),
+              with_fields(base, sh_degree_max=0), with_fields(base, sh_degree_max=1),
+              with_fields(base, sh_degree_max=2), with_fields(base, alpha_min=0.3),
+              with_fields(base, t_min=3.9), with_fields(base, t_max=4.2)]:
+        img = ctx.render(g, u, 32, 24)
+        ref, _ = o.render(u, 32, 24)
+        np.testing.assert_array_equal(img.reshape(-1, 4).view(np.uint32), ref.view(np.uint32))
+
+
+def test_camera_inside_scene(ctx):
+    """Proxies containing the camera give no front-face hit (skipped)."""
+    pg = small_scene(n=2000, seed=13)
+    g, o = _both(ctx, pg.gaussiansBuffer, 0.01)
+    v = view(40, 40, pos=(0.05, -0.02, 0.1), target=(1.0, 0.3, -2.0), k=6)
+    img = ctx.render(g, v.uniforms, 40, 40)
+    ref, _ = o.render(v.uniforms, 40, 40)
+    np.testing.assert_array_equal(img.reshape(-1, 4).view(np.uint32), ref.view(np.uint32))
+
+
+def test_invalid_arguments(ctx):
+    pg = small_scene(n=10, seed=1)
+    g = Scene(ctx, pg.gaussiansBuffer, 0.01)
+    v = view(8, 8)
+    for bad in [with_fields(v.uniforms, k=0), with_fields(v.uniforms, k=33), with_fields(v.uniforms, debug_mode=3)]:
+        with pytest.raises(L.GTraceError) as e:
+            ctx.render(g, bad, 8, 8)
+        assert e.value.status == L.GT_ERR_INVALID_ARG
+    with pytest.raises(L.GTraceError):
+        ctx.render(g, v.uniforms, 0, 8, out=np.zeros(0, np.float32))
+    with pytest.raises(L.GTraceError) as e:
+        Scene(ctx, pg.gaussiansBuffer, 1.5)
+    assert e.value.status == L.GT_ERR_INVALID_ARG
+
+
+def test_device_output_and_async(ctx):
+    pg = small_scene(n=1000, seed=14)
+    g = Scene(ctx, pg.gaussiansBuffer, 0.01)
+    w, h = 33, 17
+    v = view(w, h, k=6)
+    host = ctx.render(g, v.uniforms, w, h)
+    dev = ctx.device_alloc(w * h * 16)
+    try:
+        ctx.render_device(g, v.uniforms, w, h, dev, asynchronous=True)
+        ctx.synchronize()
+        out = np.zeros((h, w, 4), np.float32)
+        ctx.memcpy(out.ctypes.data, dev, w * h * 16, 1)
+    finally:
+        ctx.device_free(dev)
+    np.testing.assert_array_equal(out, host)
+
+
+def test_scene_from_device_buffer(ctx):
+    pg = small_scene(n=700, seed=15)
+    rec = np.ascontiguousarray(pg.gaussiansBuffer)
+    dev = ctx.device_alloc(rec.nbytes)
+    try:
+        ctx.memcpy(dev, rec.ctypes.data, rec.nbytes, 0)
+        g1 = Scene(ctx, None, 0.01, device_ptr=dev, n=rec.shape[0], stride=320)
+    finally:
+        pass
+    g2 = Scene(ctx, rec, 0.01)
+    v = view(24, 24)
+    a = ctx.render(g1, v.uniforms, 24, 24)
+    b = ctx.render(g2, v.uniforms, 24, 24)
+    ctx.device_free(dev)
+    np.testing.assert_array_equal(a, b)
+
+
+def test_batch_equals_single_views(ctx):
+    """Views of several scenes and sizes in one persistent launch (replayed
+    from a captured graph on the second call) equal separate renders."""
+    s1 = Scene(ctx, small_scene(n=900, seed=21).gaussiansBuffer, 0.01)
+    s2 = Scene(ctx, small_scene(n=1700, seed=22).gaussiansBuffer, 0.05)
+    views = [(s1, view(31, 17, k=4).uniforms, 31, 17), (s2, view(20, 40, pos=(1.0, 2.0, 3.5), k=16).uniforms, 20, 40),
+             (s1, view(8, 8, k=1).uniforms, 8, 8)]
+    for _ in range(2):
+        outs, st = ctx.render_batch(views)
+        for (sc, u, w, h), out in zip(views, outs):
+            np.testing.assert_array_equal(out, ctx.render(sc, u, w, h))
+        assert st["rays"] == 31 * 17 + 20 * 40 + 64
+
+
+def test_autotune_keeps_results(ctx):
+    pg = small_scene(n=1200, seed=23)
+    g = Scene(ctx, pg.gaussiansBuffer, 0.01)
+    v = view(64, 64, k=6)
+    before = ctx.render(g, v.uniforms, 64, 64)
+    r = ctx.autotune(g, v.uniforms, 64, 64)
+    assert r["blocks_per_sm"] >= 1 and r["best_ms"] > 0
+    after = ctx.render(g, v.uniforms, 64, 64)
+    np.testing.assert_array_equal(before, after)

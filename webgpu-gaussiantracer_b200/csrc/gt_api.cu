@@ -1,0 +1,645 @@
+// gt_api.cu — the C ABI (include/gtrace.h): contexts, scenes, render calls,
+// batches, tuning and device helpers.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "gt_internal.cuh"
+
+using namespace gt;
+
+namespace {
+thread_local std::string g_last_error;  // errors without a context
+constexpr int kEventRing = 256;
+
+struct GraphEntry {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+}  // namespace
+
+struct gt_context {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  FaceTable faces;
+  DevCounters* d_ctr = nullptr;
+  DevCounters* h_ctr = nullptr;  // pinned
+  ViewDev* d_views = nullptr;
+  uint32_t d_views_cap = 0;
+  ViewDev* h_views = nullptr;    // pinned staging for view tables
+  uint32_t h_views_cap = 0;
+  float4* staging = nullptr;
+  size_t staging_bytes = 0;
+  cudaEvent_t call0 = nullptr, call1 = nullptr, timer0 = nullptr, timer1 = nullptr;
+  cudaEvent_t ring[2 * kEventRing];
+  uint64_t ring_head = 0, ring_tail = 0;
+  uint64_t launches = 0;
+  std::map<std::tuple<uint64_t, uint32_t, uint32_t, uint32_t>, gt_tune_result> tune;
+  std::map<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t>, GraphEntry> graphs;
+};
+
+struct gt_scene {
+  gt_context* ctx = nullptr;
+  SceneBuffers b;
+  uint64_t n = 0;
+  uint32_t stride = 0;
+  double alpha_min = 0.0;
+  float build_ms = 0.0f;
+};
+
+// ----------------------------------------------------------------- helpers
+static gt_status fail(gt_context* ctx, gt_status code, const std::string& msg) {
+  if (ctx)
+    ctx->err = msg;
+  else
+    g_last_error = msg;
+  return code;
+}
+static gt_status fail(gt_context* ctx, const Err& e) { return fail(ctx, e.code, e.msg); }
+
+#define API_CUDA(ctx, expr)                                                                        \
+  do {                                                                                             \
+    cudaError_t e_ = (expr);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      return fail(ctx, e_ == cudaErrorMemoryAllocation ? GT_ERR_OOM : GT_ERR_CUDA,                 \
+                  std::string(#expr) + ": " + cudaGetErrorString(e_));                             \
+  } while (0)
+
+static gt_status status_to_error(gt_context* ctx, uint32_t status) {
+  if (status & kStatusStackOverflow) return fail(ctx, GT_ERR_STACK_OVERFLOW, "traversal stack overflow");
+  if (status & (kStatusVisitCap | kStatusRoundCap))
+    return fail(ctx, GT_ERR_DEVICE_TIMEOUT, "a device loop reached its iteration limit");
+  if (status & kStatusCheckpointFull) return fail(ctx, GT_ERR_DEVICE_TIMEOUT, "checkpoint capacity exceeded");
+  return GT_OK;
+}
+
+static gt_status check_uniforms(gt_context* ctx, const gt_uniforms* u) {
+  if (!u) return fail(ctx, GT_ERR_INVALID_ARG, "uniforms is NULL");
+  if (u->debug_mode > 2) return fail(ctx, GT_ERR_INVALID_ARG, "debug_mode must be 0, 1 or 2");
+  if (u->debug_mode == 0 && (u->k == 0 || u->k > 32))
+    return fail(ctx, GT_ERR_INVALID_ARG, "k (hit_array_size) must be in 1..32");
+  return GT_OK;
+}
+
+static void drop_graphs(gt_context* ctx) {
+  for (auto& kv : ctx->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+  }
+  ctx->graphs.clear();
+}
+
+static gt_status ensure_views(gt_context* ctx, uint32_t n) {
+  if (n > ctx->d_views_cap || n > ctx->h_views_cap) {
+    // captured graphs hold the old table addresses
+    cudaStreamSynchronize(ctx->stream);
+    drop_graphs(ctx);
+  }
+  if (n > ctx->d_views_cap) {
+    cudaFree(ctx->d_views);
+    ctx->d_views = nullptr;
+    uint32_t cap = std::max<uint32_t>(n, 2 * ctx->d_views_cap);
+    API_CUDA(ctx, cudaMalloc(&ctx->d_views, sizeof(ViewDev) * cap));
+    ctx->d_views_cap = cap;
+  }
+  if (n > ctx->h_views_cap) {
+    cudaFreeHost(ctx->h_views);
+    ctx->h_views = nullptr;
+    uint32_t cap = std::max<uint32_t>(n, 2 * ctx->h_views_cap);
+    API_CUDA(ctx, cudaHostAlloc((void**)&ctx->h_views, sizeof(ViewDev) * cap, cudaHostAllocDefault));
+    ctx->h_views_cap = cap;
+  }
+  return GT_OK;
+}
+
+static gt_status ensure_staging(gt_context* ctx, size_t bytes) {
+  if (bytes > ctx->staging_bytes) {
+    cudaFree(ctx->staging);
+    ctx->staging = nullptr;
+    ctx->staging_bytes = 0;
+    API_CUDA(ctx, cudaMalloc(&ctx->staging, bytes));
+    ctx->staging_bytes = bytes;
+  }
+  return GT_OK;
+}
+
+static SceneDev scene_dev(const gt_scene* s) {
+  SceneDev d;
+  d.nodes = s->b.nodes;
+  d.w2o = s->b.w2o;
+  d.leaf_pidx = s->b.leaf_pidx;
+  d.shade = s->b.shade;
+  d.sh = s->b.sh;
+  d.root = s->b.root;
+  d.n_kept = (uint32_t)s->b.n_kept;
+  d.n_sh = s->b.n_sh;
+  d.scene_mag = s->b.scene_mag;
+  return d;
+}
+
+static ViewDev make_view(const gt_scene* s, const gt_uniforms& u, uint32_t w, uint32_t h, float4* out,
+                         uint32_t tile_begin) {
+  ViewDev v;
+  memset(&v, 0, sizeof v);
+  v.u = to_ray_uniforms(u);
+  v.s = scene_dev(s);
+  v.out = out;
+  v.w = w;
+  v.h = h;
+  v.tiles_x = (w + 7) / 8;
+  v.n_tiles = v.tiles_x * ((h + 3) / 4);
+  v.tile_begin = tile_begin;
+  v.n_particles = s->n;
+  return v;
+}
+
+static uint64_t ring_slot(gt_context* ctx) { return (ctx->ring_head++) % kEventRing; }
+
+static void fill_stats(const DevCounters& c, gt_render_stats* st) {
+  st->rays = c.rays;
+  st->rounds = c.rounds;
+  st->entries = c.entries;
+  st->contributing = c.contributing;
+  st->proxy_tests = c.proxy_tests;
+  st->node_visits = c.node_visits;
+  st->anyhits = c.anyhits;
+  st->status_flags = c.status;
+}
+
+static LaunchShape shape_for(gt_context* ctx, const gt_scene* s, uint32_t w, uint32_t h, uint32_t k) {
+  LaunchShape sh;
+  auto key = std::make_tuple((uint64_t)(s ? (uint64_t)log2((double)std::max<uint64_t>(s->b.n_kept, 1)) : 0),
+                             (uint32_t)log2((double)std::max<uint64_t>((uint64_t)w * h, 1)), kmax_for(k), 0u);
+  auto it = ctx->tune.find(key);
+  if (it != ctx->tune.end()) {
+    sh.blocks_per_sm = it->second.blocks_per_sm;
+  }
+  return sh;
+}
+
+// ============================================================== context
+extern "C" uint32_t gt_version(void) { return GT_ABI_VERSION; }
+
+extern "C" gt_status gt_context_create(int device, gt_context** out) {
+  if (!out) return fail(nullptr, GT_ERR_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0)
+    return fail(nullptr, GT_ERR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  if (device < 0 || device >= count) return fail(nullptr, GT_ERR_NO_DEVICE, "device ordinal out of range");
+  gt_context* ctx = new gt_context();
+  ctx->device = device;
+  memset(ctx->ring, 0, sizeof ctx->ring);
+#define CTX_TRY(expr)                                                           \
+  do {                                                                          \
+    cudaError_t e2 = (expr);                                                    \
+    if (e2 != cudaSuccess) {                                                    \
+      std::string m = std::string(#expr) + ": " + cudaGetErrorString(e2);      \
+      gt_context_destroy(ctx);                                                  \
+      return fail(nullptr, e2 == cudaErrorMemoryAllocation ? GT_ERR_OOM : GT_ERR_CUDA, m); \
+    }                                                                           \
+  } while (0)
+  CTX_TRY(cudaSetDevice(device));
+  CTX_TRY(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
+  CTX_TRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  CTX_TRY(cudaMalloc(&ctx->d_ctr, sizeof(DevCounters)));
+  CTX_TRY(cudaHostAlloc((void**)&ctx->h_ctr, sizeof(DevCounters), cudaHostAllocDefault));
+  CTX_TRY(cudaEventCreate(&ctx->call0));
+  CTX_TRY(cudaEventCreate(&ctx->call1));
+  CTX_TRY(cudaEventCreate(&ctx->timer0));
+  CTX_TRY(cudaEventCreate(&ctx->timer1));
+  for (int i = 0; i < 2 * kEventRing; ++i) CTX_TRY(cudaEventCreate(&ctx->ring[i]));
+#undef CTX_TRY
+  make_face_table(&ctx->faces);
+  *out = ctx;
+  return GT_OK;
+}
+
+extern "C" gt_status gt_context_destroy(gt_context* ctx) {
+  if (!ctx) return GT_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  drop_graphs(ctx);
+  cudaFree(ctx->d_ctr);
+  cudaFreeHost(ctx->h_ctr);
+  cudaFree(ctx->d_views);
+  cudaFreeHost(ctx->h_views);
+  cudaFree(ctx->staging);
+  for (cudaEvent_t ev : {ctx->call0, ctx->call1, ctx->timer0, ctx->timer1})
+    if (ev) cudaEventDestroy(ev);
+  for (int i = 0; i < 2 * kEventRing; ++i)
+    if (ctx->ring[i]) cudaEventDestroy(ctx->ring[i]);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return GT_OK;
+}
+
+extern "C" gt_status gt_last_error(const gt_context* ctx, char* buf, size_t len) {
+  if (!buf || len == 0) return GT_ERR_INVALID_ARG;
+  const std::string& m = ctx ? ctx->err : g_last_error;
+  size_t n = std::min(len - 1, m.size());
+  memcpy(buf, m.data(), n);
+  buf[n] = 0;
+  return GT_OK;
+}
+
+// ================================================================ scene
+extern "C" gt_status gt_scene_create(gt_context* ctx, const void* packed, uint64_t n, uint32_t stride_bytes,
+                                     double alpha_min, uint32_t flags, gt_scene** out) {
+  if (!ctx) return fail(nullptr, GT_ERR_INVALID_ARG, "context is NULL");
+  if (!out) return fail(ctx, GT_ERR_INVALID_ARG, "out is NULL");
+  *out = nullptr;
+  if (n > 0 && !packed) return fail(ctx, GT_ERR_INVALID_ARG, "packed buffer is NULL");
+  if (stride_bytes < 64 || stride_bytes % 4 != 0)
+    return fail(ctx, GT_ERR_INVALID_ARG, "stride_bytes must be a multiple of 4 and at least 64");
+  if (!(alpha_min > 0.0) || !(alpha_min < 1.0))
+    return fail(ctx, GT_ERR_INVALID_ARG, "alpha_min must be in (0, 1)");
+  if (n >= (1ull << 31)) return fail(ctx, GT_ERR_INVALID_ARG, "at most 2^31 - 1 particles");
+  API_CUDA(ctx, cudaSetDevice(ctx->device));
+  const void* dev = packed;
+  void* tmp = nullptr;
+  if (n > 0 && !(flags & GT_FLAG_INPUT_DEVICE)) {
+    API_CUDA(ctx, cudaMalloc(&tmp, n * (uint64_t)stride_bytes));
+    cudaError_t e = cudaMemcpyAsync(tmp, packed, n * (uint64_t)stride_bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) {
+      cudaFree(tmp);
+      return fail(ctx, GT_ERR_CUDA, std::string("upload of the packed buffer: ") + cudaGetErrorString(e));
+    }
+    dev = tmp;
+  }
+  gt_scene* s = new gt_scene();
+  s->ctx = ctx;
+  s->n = n;
+  s->stride = stride_bytes;
+  s->alpha_min = alpha_min;
+  cudaEventRecord(ctx->call0, ctx->stream);
+  Err e = build_scene(dev, n, stride_bytes, alpha_min, ctx->stream, &s->b, &ctx->launches);
+  cudaEventRecord(ctx->call1, ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
+  if (tmp) cudaFree(tmp);
+  if (e.code != GT_OK) {
+    free_scene(&s->b);
+    delete s;
+    return fail(ctx, e);
+  }
+  cudaEventElapsedTime(&s->build_ms, ctx->call0, ctx->call1);
+  *out = s;
+  return GT_OK;
+}
+
+extern "C" gt_status gt_scene_destroy(gt_scene* s) {
+  if (!s) return GT_OK;
+  cudaSetDevice(s->ctx->device);
+  cudaStreamSynchronize(s->ctx->stream);
+  free_scene(&s->b);
+  delete s;
+  return GT_OK;
+}
+
+extern "C" gt_status gt_scene_get_info(const gt_scene* s, gt_scene_info* info) {
+  if (!s || !info) return GT_ERR_INVALID_ARG;
+  memset(info, 0, sizeof *info);
+  info->n_particles = s->n;
+  info->n_kept = s->b.n_kept;
+  info->device_bytes = s->b.bytes;
+  info->bvh_depth = s->b.depth;
+  info->build_ms = s->build_ms;
+  for (int a = 0; a < 6; ++a) info->bounds[a] = s->b.bounds[a];
+  return GT_OK;
+}
+
+// =============================================================== render
+static gt_status finish_call(gt_context* ctx, gt_render_stats* stats, uint64_t kslot) {
+  API_CUDA(ctx, cudaMemcpyAsync(ctx->h_ctr, ctx->d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, ctx->stream));
+  API_CUDA(ctx, cudaEventRecord(ctx->call1, ctx->stream));
+  API_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (stats) {
+    memset(stats, 0, sizeof *stats);
+    fill_stats(*ctx->h_ctr, stats);
+    cudaEventElapsedTime(&stats->kernel_ms, ctx->ring[2 * kslot], ctx->ring[2 * kslot + 1]);
+    cudaEventElapsedTime(&stats->total_ms, ctx->call0, ctx->call1);
+  }
+  return status_to_error(ctx, ctx->h_ctr->status);
+}
+
+extern "C" gt_status gt_render(gt_context* ctx, const gt_scene* scene, const gt_uniforms* u, uint32_t w, uint32_t h,
+                               float* out_rgba, uint32_t flags, gt_render_stats* stats) {
+  if (!ctx) return fail(nullptr, GT_ERR_INVALID_ARG, "context is NULL");
+  if (!scene || scene->ctx != ctx) return fail(ctx, GT_ERR_INVALID_ARG, "scene is NULL or from another context");
+  gt_status st = check_uniforms(ctx, u);
+  if (st != GT_OK) return st;
+  if (!out_rgba) return fail(ctx, GT_ERR_INVALID_ARG, "out_rgba is NULL");
+  if (w == 0 || h == 0 || (uint64_t)w * h > (1ull << 31)) return fail(ctx, GT_ERR_INVALID_ARG, "bad image size");
+  if ((flags & GT_FLAG_ASYNC) && !(flags & GT_FLAG_OUTPUT_DEVICE))
+    return fail(ctx, GT_ERR_INVALID_ARG, "GT_FLAG_ASYNC needs a device output buffer");
+  if ((flags & GT_FLAG_OUTPUT_DEVICE) && ((uintptr_t)out_rgba % 16) != 0)
+    return fail(ctx, GT_ERR_INVALID_ARG, "device out_rgba must be 16-byte aligned");
+  API_CUDA(ctx, cudaSetDevice(ctx->device));
+  size_t bytes = (size_t)w * h * sizeof(float4);
+  float4* out = reinterpret_cast<float4*>(out_rgba);
+  if (!(flags & GT_FLAG_OUTPUT_DEVICE)) {
+    st = ensure_staging(ctx, bytes);
+    if (st != GT_OK) return st;
+    out = ctx->staging;
+  }
+  st = ensure_views(ctx, 1);
+  if (st != GT_OK) return st;
+  ViewDev v = make_view(scene, *u, w, h, out, 0);
+  API_CUDA(ctx, cudaEventRecord(ctx->call0, ctx->stream));
+  API_CUDA(ctx, cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), ctx->stream));
+  uint64_t slot = ring_slot(ctx);
+  API_CUDA(ctx, cudaEventRecord(ctx->ring[2 * slot], ctx->stream));
+  LaunchShape shape = shape_for(ctx, scene, w, h, u->k);
+  Err e = launch_trace(&v, 1, v.n_tiles, ctx->d_ctr, ctx->faces, shape, ctx->num_sms, ctx->stream, &ctx->launches,
+                       ctx->d_views);
+  if (e.code != GT_OK) return fail(ctx, e);
+  API_CUDA(ctx, cudaEventRecord(ctx->ring[2 * slot + 1], ctx->stream));
+  if (!(flags & GT_FLAG_OUTPUT_DEVICE))
+    API_CUDA(ctx, cudaMemcpyAsync(out_rgba, out, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  if (flags & GT_FLAG_ASYNC) return GT_OK;
+  return finish_call(ctx, stats, slot);
+}
+
+extern "C" gt_status gt_render_hits(gt_context* ctx, const gt_scene* scene, const gt_uniforms* u, uint32_t w,
+                                    uint32_t h, const uint32_t* pixels, uint32_t n_pix, uint32_t max_entries,
+                                    uint32_t* out_pidx, float* out_t, float* out_alpha, uint32_t* out_count,
+                                    uint32_t* out_rounds, float* out_rgba) {
+  if (!ctx) return fail(nullptr, GT_ERR_INVALID_ARG, "context is NULL");
+  if (!scene || scene->ctx != ctx) return fail(ctx, GT_ERR_INVALID_ARG, "scene is NULL or from another context");
+  gt_status st = check_uniforms(ctx, u);
+  if (st != GT_OK) return st;
+  if (w == 0 || h == 0 || (uint64_t)w * h > (1ull << 31)) return fail(ctx, GT_ERR_INVALID_ARG, "bad image size");
+  if (n_pix == 0) return GT_OK;
+  if (!pixels || !out_count || !out_rounds || (max_entries > 0 && (!out_pidx || !out_t || !out_alpha)))
+    return fail(ctx, GT_ERR_INVALID_ARG, "NULL output buffer");
+  API_CUDA(ctx, cudaSetDevice(ctx->device));
+  size_t me = std::max<uint32_t>(max_entries, 1);
+  size_t bytes = (size_t)n_pix * (4 + me * 12 + 4 + 4 + 16);
+  uint8_t* buf = nullptr;
+  API_CUDA(ctx, cudaMalloc(&buf, bytes));
+  uint32_t* d_pix = reinterpret_cast<uint32_t*>(buf);
+  float4* d_rgba = reinterpret_cast<float4*>(buf + (size_t)n_pix * 4);
+  uint32_t* d_pidx = reinterpret_cast<uint32_t*>(buf + (size_t)n_pix * 20);
+  float* d_t = reinterpret_cast<float*>(buf + (size_t)n_pix * (20 + 4 * me));
+  float* d_alpha = reinterpret_cast<float*>(buf + (size_t)n_pix * (20 + 8 * me));
+  uint32_t* d_count = reinterpret_cast<uint32_t*>(buf + (size_t)n_pix * (20 + 12 * me));
+  uint32_t* d_rounds = reinterpret_cast<uint32_t*>(buf + (size_t)n_pix * (24 + 12 * me));
+  ViewDev v = make_view(scene, *u, w, h, nullptr, 0);
+  gt_status rc = GT_OK;
+  do {
+    cudaError_t ce = cudaMemcpyAsync(d_pix, pixels, (size_t)n_pix * 4, cudaMemcpyHostToDevice, ctx->stream);
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), ctx->stream);
+    if (ce != cudaSuccess) {
+      rc = fail(ctx, GT_ERR_CUDA, cudaGetErrorString(ce));
+      break;
+    }
+    Err e = launch_trace_hits(v, d_pix, n_pix, (uint32_t)me, d_pidx, d_t, d_alpha, d_count, d_rounds,
+                              out_rgba ? d_rgba : nullptr, ctx->d_ctr, ctx->faces, ctx->stream, &ctx->launches);
+    if (e.code != GT_OK) {
+      rc = fail(ctx, e);
+      break;
+    }
+    ce = cudaMemcpyAsync(out_count, d_count, (size_t)n_pix * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(out_rounds, d_rounds, (size_t)n_pix * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (ce == cudaSuccess && out_rgba)
+      ce = cudaMemcpyAsync(out_rgba, d_rgba, (size_t)n_pix * 16, cudaMemcpyDeviceToHost, ctx->stream);
+    if (ce == cudaSuccess && max_entries > 0) {
+      // copy row by row: device rows have `me` entries, host rows `max_entries`
+      ce = cudaMemcpyAsync(out_pidx, d_pidx, (size_t)n_pix * me * 4, cudaMemcpyDeviceToHost, ctx->stream);
+      if (ce == cudaSuccess) ce = cudaMemcpyAsync(out_t, d_t, (size_t)n_pix * me * 4, cudaMemcpyDeviceToHost, ctx->stream);
+      if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(out_alpha, d_alpha, (size_t)n_pix * me * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(ctx->h_ctr, ctx->d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, ctx->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(ctx->stream);
+    if (ce != cudaSuccess) {
+      rc = fail(ctx, GT_ERR_CUDA, cudaGetErrorString(ce));
+      break;
+    }
+    rc = status_to_error(ctx, ctx->h_ctr->status);
+  } while (0);
+  cudaFree(buf);
+  return rc;
+}
+
+// ============================================================== batches
+extern "C" gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items, uint32_t count, uint32_t flags,
+                                     gt_render_stats* stats) {
+  if (!ctx) return fail(nullptr, GT_ERR_INVALID_ARG, "context is NULL");
+  if (count == 0) return GT_OK;
+  if (!items) return fail(ctx, GT_ERR_INVALID_ARG, "items is NULL");
+  if ((flags & GT_FLAG_ASYNC) && !(flags & GT_FLAG_OUTPUT_DEVICE))
+    return fail(ctx, GT_ERR_INVALID_ARG, "GT_FLAG_ASYNC needs device output buffers");
+  API_CUDA(ctx, cudaSetDevice(ctx->device));
+  size_t staging = 0;
+  uint32_t kmax = 8, total_tiles = 0;
+  for (uint32_t i = 0; i < count; ++i) {
+    const gt_batch_item& it = items[i];
+    if (!it.scene || it.scene->ctx != ctx) return fail(ctx, GT_ERR_INVALID_ARG, "batch item scene invalid");
+    gt_status st = check_uniforms(ctx, &it.u);
+    if (st != GT_OK) return st;
+    if (!it.out_rgba || it.w == 0 || it.h == 0 || (uint64_t)it.w * it.h > (1ull << 31))
+      return fail(ctx, GT_ERR_INVALID_ARG, "batch item image invalid");
+    if ((flags & GT_FLAG_OUTPUT_DEVICE) && ((uintptr_t)it.out_rgba % 16) != 0)
+      return fail(ctx, GT_ERR_INVALID_ARG, "device out_rgba must be 16-byte aligned");
+    staging += (size_t)it.w * it.h;
+    kmax = std::max(kmax, kmax_for(it.u.k));
+  }
+  gt_status st = ensure_views(ctx, count);
+  if (st != GT_OK) return st;
+  if (!(flags & GT_FLAG_OUTPUT_DEVICE)) {
+    st = ensure_staging(ctx, staging * sizeof(float4));
+    if (st != GT_OK) return st;
+  }
+  size_t off = 0;
+  for (uint32_t i = 0; i < count; ++i) {
+    const gt_batch_item& it = items[i];
+    float4* out = (flags & GT_FLAG_OUTPUT_DEVICE) ? reinterpret_cast<float4*>(it.out_rgba) : ctx->staging + off;
+    ctx->h_views[i] = make_view(it.scene, it.u, it.w, it.h, out, total_tiles);
+    total_tiles += ctx->h_views[i].n_tiles;
+    off += (size_t)it.w * it.h;
+  }
+  API_CUDA(ctx, cudaEventRecord(ctx->call0, ctx->stream));
+  uint64_t slot = ring_slot(ctx);
+  API_CUDA(ctx, cudaEventRecord(ctx->ring[2 * slot], ctx->stream));
+  // One graph per batch shape: counter reset + the persistent kernel.
+  LaunchShape shape = shape_for(ctx, items[0].scene, items[0].w, items[0].h, items[0].u.k);
+  auto key = std::make_tuple(count, total_tiles, kmax, shape.blocks_per_sm);
+  auto it = ctx->graphs.find(key);
+  if (it == ctx->graphs.end()) {
+    GraphEntry g;
+    cudaStream_t cs = ctx->stream;
+    API_CUDA(ctx, cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), cs);
+    // launch_trace re-uploads the view table; inside the graph it copies from
+    // the pinned staging table, which is refreshed before every replay.
+    Err e = launch_trace(ctx->h_views, count, total_tiles, ctx->d_ctr, ctx->faces, shape, ctx->num_sms, cs,
+                         &ctx->launches, ctx->d_views);
+    cudaError_t ce = cudaStreamEndCapture(cs, &g.graph);
+    if (e.code != GT_OK) return fail(ctx, e);
+    if (ce != cudaSuccess) return fail(ctx, GT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+    API_CUDA(ctx, cudaGraphInstantiate(&g.exec, g.graph, 0));
+    it = ctx->graphs.emplace(key, g).first;
+  }
+  API_CUDA(ctx, cudaGraphLaunch(it->second.exec, ctx->stream));
+  ++ctx->launches;
+  API_CUDA(ctx, cudaEventRecord(ctx->ring[2 * slot + 1], ctx->stream));
+  if (!(flags & GT_FLAG_OUTPUT_DEVICE)) {
+    size_t o2 = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+      size_t px = (size_t)items[i].w * items[i].h;
+      API_CUDA(ctx, cudaMemcpyAsync(items[i].out_rgba, ctx->staging + o2, px * sizeof(float4), cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+      o2 += px;
+    }
+  }
+  if (flags & GT_FLAG_ASYNC) return GT_OK;
+  return finish_call(ctx, stats, slot);
+}
+
+// =============================================================== tuning
+extern "C" gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const gt_uniforms* u, uint32_t w,
+                                 uint32_t h, gt_tune_result* result) {
+  if (!ctx) return fail(nullptr, GT_ERR_INVALID_ARG, "context is NULL");
+  if (!scene || scene->ctx != ctx) return fail(ctx, GT_ERR_INVALID_ARG, "scene is NULL or from another context");
+  gt_status st = check_uniforms(ctx, u);
+  if (st != GT_OK) return st;
+  if (w == 0 || h == 0) return fail(ctx, GT_ERR_INVALID_ARG, "bad image size");
+  API_CUDA(ctx, cudaSetDevice(ctx->device));
+  size_t bytes = (size_t)w * h * sizeof(float4);
+  st = ensure_staging(ctx, bytes);
+  if (st != GT_OK) return st;
+  st = ensure_views(ctx, 1);
+  if (st != GT_OK) return st;
+  ViewDev v = make_view(scene, *u, w, h, ctx->staging, 0);
+  const uint32_t cands[] = {1, 2, 3, 4, 6, 8, 12, 16};
+  float best = 1e30f, def = 0.0f;
+  uint32_t best_b = 4;
+  for (uint32_t b : cands) {
+    LaunchShape sh;
+    sh.blocks_per_sm = b;
+    float ms_min = 1e30f;
+    for (int rep = 0; rep < 3; ++rep) {
+      API_CUDA(ctx, cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), ctx->stream));
+      API_CUDA(ctx, cudaEventRecord(ctx->timer0, ctx->stream));
+      Err e = launch_trace(&v, 1, v.n_tiles, ctx->d_ctr, ctx->faces, sh, ctx->num_sms, ctx->stream, &ctx->launches,
+                           ctx->d_views);
+      if (e.code != GT_OK) return fail(ctx, e);
+      API_CUDA(ctx, cudaEventRecord(ctx->timer1, ctx->stream));
+      API_CUDA(ctx, cudaEventSynchronize(ctx->timer1));
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, ctx->timer0, ctx->timer1);
+      ms_min = std::min(ms_min, ms);
+    }
+    if (b == LaunchShape().blocks_per_sm) def = ms_min;
+    if (ms_min < best) {
+      best = ms_min;
+      best_b = b;
+    }
+  }
+  gt_tune_result r;
+  memset(&r, 0, sizeof r);
+  r.block_threads = 128;
+  r.blocks_per_sm = best_b;
+  r.tile_w = 8;
+  r.tile_h = 4;
+  r.best_ms = best;
+  r.default_ms = def;
+  auto key = std::make_tuple((uint64_t)log2((double)std::max<uint64_t>(scene->b.n_kept, 1)),
+                             (uint32_t)log2((double)std::max<uint64_t>((uint64_t)w * h, 1)), kmax_for(u->k), 0u);
+  ctx->tune[key] = r;
+  if (result) *result = r;
+  return GT_OK;
+}
+
+extern "C" gt_status gt_autotune_reset(gt_context* ctx) {
+  if (!ctx) return GT_ERR_INVALID_ARG;
+  ctx->tune.clear();
+  return GT_OK;
+}
+
+// ======================================================= device helpers
+extern "C" gt_status gt_device_alloc(gt_context* ctx, uint64_t bytes, void** out) {
+  if (!ctx || !out) return fail(ctx, GT_ERR_INVALID_ARG, "NULL argument");
+  API_CUDA(ctx, cudaSetDevice(ctx->device));
+  API_CUDA(ctx, cudaMalloc(out, bytes ? bytes : 1));
+  return GT_OK;
+}
+extern "C" gt_status gt_device_free(gt_context* ctx, void* ptr) {
+  if (!ctx) return GT_ERR_INVALID_ARG;
+  API_CUDA(ctx, cudaSetDevice(ctx->device));
+  API_CUDA(ctx, cudaFree(ptr));
+  return GT_OK;
+}
+extern "C" gt_status gt_host_alloc(gt_context* ctx, uint64_t bytes, void** out) {
+  if (!ctx || !out) return fail(ctx, GT_ERR_INVALID_ARG, "NULL argument");
+  API_CUDA(ctx, cudaSetDevice(ctx->device));
+  API_CUDA(ctx, cudaHostAlloc(out, bytes ? bytes : 1, cudaHostAllocDefault));
+  return GT_OK;
+}
+extern "C" gt_status gt_host_free(gt_context* ctx, void* ptr) {
+  if (!ctx) return GT_ERR_INVALID_ARG;
+  API_CUDA(ctx, cudaFreeHost(ptr));
+  return GT_OK;
+}
+extern "C" gt_status gt_memcpy(gt_context* ctx, void* dst, const void* src, uint64_t bytes, int kind) {
+  if (!ctx || (!dst && bytes) || (!src && bytes) || kind < 0 || kind > 2)
+    return fail(ctx, GT_ERR_INVALID_ARG, "bad gt_memcpy argument");
+  cudaMemcpyKind k = kind == 0 ? cudaMemcpyHostToDevice : (kind == 1 ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice);
+  API_CUDA(ctx, cudaSetDevice(ctx->device));
+  API_CUDA(ctx, cudaMemcpyAsync(dst, src, bytes, k, ctx->stream));
+  API_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return GT_OK;
+}
+extern "C" gt_status gt_synchronize(gt_context* ctx) {
+  if (!ctx) return GT_ERR_INVALID_ARG;
+  API_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return GT_OK;
+}
+extern "C" gt_status gt_timer_start(gt_context* ctx) {
+  if (!ctx) return GT_ERR_INVALID_ARG;
+  API_CUDA(ctx, cudaEventRecord(ctx->timer0, ctx->stream));
+  return GT_OK;
+}
+extern "C" gt_status gt_timer_stop(gt_context* ctx, float* ms) {
+  if (!ctx || !ms) return GT_ERR_INVALID_ARG;
+  API_CUDA(ctx, cudaEventRecord(ctx->timer1, ctx->stream));
+  API_CUDA(ctx, cudaEventSynchronize(ctx->timer1));
+  API_CUDA(ctx, cudaEventElapsedTime(ms, ctx->timer0, ctx->timer1));
+  return GT_OK;
+}
+extern "C" gt_status gt_kernel_times(gt_context* ctx, float* out_ms, uint32_t max, uint32_t* n) {
+  if (!ctx || !n || (max && !out_ms)) return GT_ERR_INVALID_ARG;
+  API_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  uint64_t avail = ctx->ring_head - ctx->ring_tail;
+  if (avail > kEventRing) {
+    ctx->ring_tail = ctx->ring_head - kEventRing;
+    avail = kEventRing;
+  }
+  uint32_t m = 0;
+  while (ctx->ring_tail < ctx->ring_head && m < max) {
+    uint64_t s = ctx->ring_tail % kEventRing;
+    float ms = 0.0f;
+    API_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ring[2 * s], ctx->ring[2 * s + 1]));
+    out_ms[m++] = ms;
+    ++ctx->ring_tail;
+  }
+  ctx->ring_tail = ctx->ring_head;
+  *n = m;
+  return GT_OK;
+}
+extern "C" gt_status gt_launch_count(const gt_context* ctx, uint64_t* n) {
+  if (!ctx || !n) return GT_ERR_INVALID_ARG;
+  *n = ctx->launches;
+  return GT_OK;
+}

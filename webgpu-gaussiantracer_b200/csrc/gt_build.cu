@@ -1,0 +1,669 @@
+// gt_build.cu — GPU scene build: proxies, LBVH, shading records.
+//
+// Replaces the reference's host-side acceleration-structure build
+// (gaussianSceneToBvh, src/main.ts:30-111; Tlas.build,
+// webrtx/src/wasm_bvh_builder.ts:260-377; build_blas/build_tlas,
+// webrtx/bvh/src/lib.rs:254-347, 512-603) with a linear BVH built on the GPU:
+//
+//   1. keep flags (opacity > alpha_min) and an exclusive scan  -> kept list
+//   2. per kept particle: proxy matrix M = T R diag(s*scale), world AABB of
+//      the 12 transformed icosahedron vertices, box centre, scene bounds
+//   3. 30-bit Morton codes of the box centres
+//   4. LSD radix sort of (code, kept slot), 4 passes of 8 bits, hand-written
+//      (per-tile histograms, one scan, stable warp-ranked scatter)
+//   5. Karras (2012) hierarchy over the sorted codes, ties broken by index
+//   6. bottom-up refit with one atomic arrival counter per internal node
+//   7. leaf records in leaf order (world-to-object map, particle index) and
+//      shading records in particle order (mean, opacity, precision matrix, SH)
+//
+// Node layout (4 x float4 per internal node; children's boxes in the parent):
+//   f0 = (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y)
+//   f1 = (c1.lo.x, c1.hi.x, c1.lo.y, c1.hi.y)
+//   f2 = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)
+//   f3 = (child0, child1, 0, 0) as uint bits; kLeafBit | j marks leaf j.
+#include <math.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "gt_device.cuh"
+#include "gt_internal.cuh"
+
+namespace gt {
+
+// ---------------------------------------------------------------- faces
+// Icosahedron with inradius 1 (src/main.ts:12-25).
+static const int kIcoIdx[60] = {0, 11, 5,  0, 5,  1,  0,  1,  7,  0,  7,  10, 0, 10, 11,
+                                1, 5,  9,  5, 11, 4,  11, 10, 2,  10, 7,  6,  7, 1,  8,
+                                3, 9,  4,  3, 4,  2,  3,  2,  6,  3,  6,  8,  3, 8,  9,
+                                4, 9,  5,  2, 4,  11, 6,  2,  10, 8,  6,  7,  9, 8,  1};
+
+static void ico_vertices(float v[36]) {
+  double rr = (3.0 + sqrt(5.0)) / (2.0 * sqrt(3.0));
+  double ss = 1.0 / rr;
+  double tt = (1.0 + sqrt(5.0)) / (2.0 * rr);
+  double t[36] = {-ss, tt, 0, ss,  tt, 0,  -ss, -tt, 0,   ss,  -tt, 0,   0,   -ss, tt,  0, ss,  tt,
+                  0,   -ss, -tt, 0, ss, -tt, tt,  0,   -ss, tt,  0,   ss,  -tt, 0,   -ss, -tt, 0, ss};
+  for (int i = 0; i < 36; ++i) v[i] = (float)t[i];
+}
+
+void make_face_table(FaceTable* F) {
+  // Host code is compiled with -ffp-contract=off: each expression below is
+  // rounded exactly as the device and the oracle round it.
+  float v[36];
+  ico_vertices(v);
+  float nmax = 0.0f;
+  for (int f = 0; f < 20; ++f) {
+    const float* p0 = v + 3 * kIcoIdx[3 * f];
+    const float* p1 = v + 3 * kIcoIdx[3 * f + 1];
+    const float* p2 = v + 3 * kIcoIdx[3 * f + 2];
+    float e0[3], e1[3];
+    for (int a = 0; a < 3; ++a) {
+      e0[a] = p1[a] - p0[a];
+      e1[a] = p0[a] - p2[a];
+      F->p0[f][a] = p0[a];
+      F->e0[f][a] = e0[a];
+      F->e1[f][a] = e1[a];
+    }
+    // n = cross(e1, e0)
+    F->n[f][0] = e1[1] * e0[2] - e1[2] * e0[1];
+    F->n[f][1] = e1[2] * e0[0] - e1[0] * e0[2];
+    F->n[f][2] = e1[0] * e0[1] - e1[1] * e0[0];
+    for (int a = 0; a < 3; ++a) nmax = fmaxf(nmax, fabsf(F->n[f][a]));
+  }
+  F->nmax = nmax;
+  float r = 0.0f;
+  for (int i = 0; i < 12; ++i)
+    r = fmaxf(r, sqrtf(v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]));
+  F->r_circ = r;
+}
+static_assert(sizeof(kIcoIdx) == 60 * sizeof(int), "table size");
+
+struct IcoVerts {
+  float v[36];
+};
+
+// ---------------------------------------------------------------- proxies
+// src/main.ts:79-94: s = sqrt(2 ln(o / alpha_min)); M = T(mu) R diag(s*scale)
+// with R = wgpu-matrix mat3.fromQuat([x, y, z, w]) evaluated in double and
+// rounded to binary32 (Float32Array), s*scale rounded to binary32, and each
+// column entry the binary32 product of the two.
+__device__ __forceinline__ void proxy_o2w(const float* rec, double alpha_min, float M[12]) {
+  double o = (double)rec[12];
+  double s = __dsqrt_rn(__dmul_rn(2.0, det_log(__ddiv_rn(o, alpha_min))));
+  double w = rec[8], x = rec[9], y = rec[10], z = rec[11];
+  double x2 = x + x, y2 = y + y, z2 = z + z;
+  double xx = x * x2, yx = y * x2, yy = y * y2;
+  double zx = z * x2, zy = z * y2, zz = z * z2;
+  double wx = w * x2, wy = w * y2, wz = w * z2;
+  double R[9] = {1.0 - yy - zz, yx + wz, zx - wy, yx - wz, 1.0 - xx - zz, zy + wx, zx + wy, zy - wx, 1.0 - xx - yy};
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    float Sc = __double2float_rn(__dmul_rn(s, (double)rec[4 + c]));
+#pragma unroll
+    for (int r = 0; r < 3; ++r) M[3 * c + r] = __double2float_rn(R[3 * c + r]) * Sc;
+  }
+  M[9] = rec[0];
+  M[10] = rec[1];
+  M[11] = rec[2];
+}
+
+// Affine inverse (replaces glam Affine3A::inverse, webrtx/bvh/src/lib.rs:501-505):
+// adjugate from cross products of the columns a, b, c; det = dot(c, cross(a, b)).
+__device__ __forceinline__ void affine_inverse(const float M[12], float W[12]) {
+  V3 a = mk(M[0], M[1], M[2]), b = mk(M[3], M[4], M[5]), c = mk(M[6], M[7], M[8]);
+  V3 p = mk(M[9], M[10], M[11]);
+  V3 t0 = vcross(b, c), t1 = vcross(c, a), t2 = vcross(a, b);
+  float det = vdot(c, t2);
+  float inv = __fdiv_rn(1.0f, det);
+  W[0] = t0.x * inv; W[1] = t1.x * inv; W[2] = t2.x * inv;
+  W[3] = t0.y * inv; W[4] = t1.y * inv; W[5] = t2.y * inv;
+  W[6] = t0.z * inv; W[7] = t1.z * inv; W[8] = t2.z * inv;
+  W[9] = -((W[0] * p.x + W[3] * p.y) + W[6] * p.z);
+  W[10] = -((W[1] * p.x + W[4] * p.y) + W[7] * p.z);
+  W[11] = -((W[2] * p.x + W[5] * p.y) + W[8] * p.z);
+}
+
+__device__ __forceinline__ const float* record(const uint8_t* packed, uint64_t i, uint32_t stride) {
+  return reinterpret_cast<const float*>(packed + i * (uint64_t)stride);
+}
+
+__global__ void k_keep_flags(const uint8_t* packed, uint64_t n, uint32_t stride, double alpha_min,
+                             uint32_t* flags) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  flags[i] = ((double)record(packed, i, stride)[12] > alpha_min) ? 1u : 0u;
+}
+
+// float min/max through order-preserving integer maps (for atomics)
+__device__ __forceinline__ uint32_t f2ord(float f) {
+  uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord2f(uint32_t u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
+}
+
+__global__ void k_proxy_boxes(const uint8_t* packed, uint64_t n, uint32_t stride, double alpha_min,
+                              const uint32_t* flags, const uint32_t* slots, const IcoVerts iv, float* box,
+                              uint32_t* kept_pidx, uint32_t* bounds_ord) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  float cmin[3] = {CUDART_INF_F, CUDART_INF_F, CUDART_INF_F}, cmax[3] = {-CUDART_INF_F, -CUDART_INF_F, -CUDART_INF_F};
+  float bmag = 0.0f;
+  if (i < n && flags[i]) {
+    const float* rec = record(packed, i, stride);
+    float M[12];
+    proxy_o2w(rec, alpha_min, M);
+    Affine A;
+#pragma unroll
+    for (int q = 0; q < 12; ++q) A.m[q] = M[q];
+    float lo[3] = {CUDART_INF_F, CUDART_INF_F, CUDART_INF_F}, hi[3] = {-CUDART_INF_F, -CUDART_INF_F, -CUDART_INF_F};
+#pragma unroll
+    for (int v = 0; v < 12; ++v) {
+      V3 w = xpoint(A, mk(iv.v[3 * v], iv.v[3 * v + 1], iv.v[3 * v + 2]));
+      lo[0] = fminf(lo[0], w.x); lo[1] = fminf(lo[1], w.y); lo[2] = fminf(lo[2], w.z);
+      hi[0] = fmaxf(hi[0], w.x); hi[1] = fmaxf(hi[1], w.y); hi[2] = fmaxf(hi[2], w.z);
+    }
+    float ext = fmaxf(fmaxf(hi[0] - lo[0], hi[1] - lo[1]), hi[2] - lo[2]);
+    float mag = 0.0f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) mag = fmaxf(mag, fmaxf(fabsf(lo[a]), fabsf(hi[a])));
+    // conservative padding for the rounding of the vertex transform
+    float pad = __fmaf_rn(1e-5f, ext, 2e-6f * (mag + 1.0f));
+    uint32_t s = slots[i];
+    float* b = box + 6 * (size_t)s;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      b[a] = lo[a] - pad;
+      b[3 + a] = hi[a] + pad;
+      float c = 0.5f * (b[a] + b[3 + a]);
+      cmin[a] = c;
+      cmax[a] = c;
+      bmag = fmaxf(bmag, fmaxf(fabsf(b[a]), fabsf(b[3 + a])));
+    }
+    kept_pidx[s] = (uint32_t)i;
+  }
+  // warp-reduce the centre bounds, then one atomic per warp
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      cmin[a] = fminf(cmin[a], __shfl_xor_sync(0xFFFFFFFFu, cmin[a], off));
+      cmax[a] = fmaxf(cmax[a], __shfl_xor_sync(0xFFFFFFFFu, cmax[a], off));
+    }
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) bmag = fmaxf(bmag, __shfl_xor_sync(0xFFFFFFFFu, bmag, off));
+  if ((threadIdx.x & 31) == 0 && cmin[0] <= cmax[0]) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      atomicMin(&bounds_ord[a], f2ord(cmin[a]));
+      atomicMax(&bounds_ord[3 + a], f2ord(cmax[a]));
+    }
+    atomicMax(&bounds_ord[6], f2ord(bmag));
+  }
+}
+
+__device__ __forceinline__ uint32_t spread10(uint32_t v) {
+  v &= 0x3FFu;
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+__global__ void k_morton(const float* box, uint32_t m, const uint32_t* bounds_ord, uint32_t* keys,
+                         uint32_t* vals) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  uint32_t code = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float lo = ord2f(bounds_ord[a]), hi = ord2f(bounds_ord[3 + a]);
+    float c = 0.5f * (box[6 * (size_t)j + a] + box[6 * (size_t)j + 3 + a]);
+    float e = hi - lo;
+    float u = e > 0.0f ? (c - lo) / e : 0.0f;
+    u = fminf(fmaxf(u, 0.0f), 1.0f);
+    uint32_t q = (uint32_t)(u * 1023.0f);
+    code |= spread10(q) << (2 - a);
+  }
+  keys[j] = code;
+  vals[j] = j;
+}
+
+// ------------------------------------------------------------------ scan
+constexpr int kScanBlock = 512;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanBlock * kScanItems;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total) {
+  __shared__ uint32_t warp_sums[32];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, off);
+    if (lane >= off) x += y;
+  }
+  if (lane == 31) warp_sums[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int nw = blockDim.x >> 5;
+    uint32_t s = lane < nw ? warp_sums[lane] : 0u;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      uint32_t y = __shfl_up_sync(0xFFFFFFFFu, s, off);
+      if (lane >= off) s += y;
+    }
+    warp_sums[lane] = s;
+  }
+  __syncthreads();
+  uint32_t base = warp ? warp_sums[warp - 1] : 0u;
+  if (total) *total = warp_sums[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return base + x - v;
+}
+
+__global__ void k_scan_tiles(const uint32_t* in, uint32_t* out, uint64_t n, uint32_t* tile_sums) {
+  uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+  uint32_t v[kScanItems];
+  uint32_t sum = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    v[i] = (base + i < n) ? in[base + i] : 0u;
+    sum += v[i];
+  }
+  uint32_t total;
+  uint32_t pre = block_exclusive_scan(sum, &total);
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    if (base + i < n) out[base + i] = pre;
+    pre += v[i];
+  }
+  if (threadIdx.x == 0 && tile_sums) tile_sums[blockIdx.x] = total;
+}
+
+__global__ void k_scan_add(uint32_t* out, uint64_t n, const uint32_t* tile_offsets) {
+  uint64_t base = (uint64_t)blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+  uint32_t add = tile_offsets[blockIdx.x];
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i)
+    if (base + i < n) out[base + i] += add;
+}
+
+// Exclusive scan of n uint32 values (in may equal out).  Temporaries are
+// stream-ordered allocations.
+static Err scan_exclusive(const uint32_t* in, uint32_t* out, uint64_t n, cudaStream_t st, uint64_t* launches) {
+  if (n == 0) return Err{};
+  uint64_t tiles = (n + kScanTile - 1) / kScanTile;
+  if (tiles == 1) {
+    k_scan_tiles<<<1, kScanBlock, 0, st>>>(in, out, n, nullptr);
+    ++*launches;
+    GT_CUDA_TRY(cudaGetLastError());
+    return Err{};
+  }
+  uint32_t* sums = nullptr;
+  GT_CUDA_TRY(cudaMallocAsync(&sums, tiles * sizeof(uint32_t), st));
+  k_scan_tiles<<<(unsigned)tiles, kScanBlock, 0, st>>>(in, out, n, sums);
+  ++*launches;
+  Err e = scan_exclusive(sums, sums, tiles, st, launches);
+  if (e.code == GT_OK) {
+    k_scan_add<<<(unsigned)tiles, kScanBlock, 0, st>>>(out, n, sums);
+    ++*launches;
+  }
+  cudaFreeAsync(sums, st);
+  if (e.code != GT_OK) return e;
+  GT_CUDA_TRY(cudaGetLastError());
+  return Err{};
+}
+
+// ------------------------------------------------------------ radix sort
+constexpr int kRsBlock = 256;
+constexpr int kRsItems = 8;
+constexpr int kRsTile = kRsBlock * kRsItems;
+
+__global__ void k_rs_hist(const uint32_t* keys, uint32_t n, int shift, uint32_t* hist, uint32_t n_tiles) {
+  __shared__ uint32_t cnt[256];
+  cnt[threadIdx.x] = 0;
+  __syncthreads();
+  uint32_t base = blockIdx.x * kRsTile;
+#pragma unroll
+  for (int r = 0; r < kRsItems; ++r) {
+    uint32_t i = base + r * kRsBlock + threadIdx.x;
+    if (i < n) atomicAdd(&cnt[(keys[i] >> shift) & 255u], 1u);
+  }
+  __syncthreads();
+  hist[threadIdx.x * n_tiles + blockIdx.x] = cnt[threadIdx.x];
+}
+
+// Stable scatter: items of a tile are ranked in index order, warp by warp.
+__global__ void k_rs_scatter(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, uint32_t n,
+                             int shift, const uint32_t* offsets, uint32_t n_tiles) {
+  __shared__ uint32_t running[256];
+  __shared__ uint32_t whist[kRsBlock / 32][257];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  running[threadIdx.x] = offsets[threadIdx.x * n_tiles + blockIdx.x];
+  uint32_t base = blockIdx.x * kRsTile;
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  for (int r = 0; r < kRsItems; ++r) {
+    for (int q = threadIdx.x; q < (kRsBlock / 32) * 257; q += kRsBlock) (&whist[0][0])[q] = 0;
+    __syncthreads();
+    uint32_t i = base + r * kRsBlock + threadIdx.x;
+    uint32_t key = 0, val = 0, digit = 256;
+    if (i < n) {
+      key = kin[i];
+      val = vin[i];
+      digit = (key >> shift) & 255u;
+    }
+    uint32_t peers = __match_any_sync(0xFFFFFFFFu, digit);
+    uint32_t rank = __popc(peers & lt_mask);
+    if (rank == 0 && digit < 256) whist[warp][digit] = __popc(peers);
+    __syncthreads();
+    {
+      uint32_t d = threadIdx.x;  // kRsBlock == 256 digits
+      uint32_t acc = running[d];
+#pragma unroll
+      for (int w = 0; w < kRsBlock / 32; ++w) {
+        uint32_t c = whist[w][d];
+        whist[w][d] = acc;
+        acc += c;
+      }
+      running[d] = acc;
+    }
+    __syncthreads();
+    if (digit < 256) {
+      uint32_t pos = whist[warp][digit] + rank;
+      kout[pos] = key;
+      vout[pos] = val;
+    }
+    __syncthreads();
+  }
+}
+
+static Err radix_sort(uint32_t* keys, uint32_t* vals, uint32_t n, cudaStream_t st, uint64_t* launches) {
+  if (n <= 1) return Err{};
+  uint32_t n_tiles = (n + kRsTile - 1) / kRsTile;
+  uint32_t *k2 = nullptr, *v2 = nullptr, *hist = nullptr;
+  GT_CUDA_TRY(cudaMallocAsync(&k2, (size_t)n * 4, st));
+  GT_CUDA_TRY(cudaMallocAsync(&v2, (size_t)n * 4, st));
+  GT_CUDA_TRY(cudaMallocAsync(&hist, (size_t)256 * n_tiles * 4, st));
+  uint32_t *ka = keys, *va = vals, *kb = k2, *vb = v2;
+  Err e;
+  for (int shift = 0; shift < 32; shift += 8) {
+    k_rs_hist<<<n_tiles, kRsBlock, 0, st>>>(ka, n, shift, hist, n_tiles);
+    ++*launches;
+    e = scan_exclusive(hist, hist, (uint64_t)256 * n_tiles, st, launches);
+    if (e.code != GT_OK) break;
+    k_rs_scatter<<<n_tiles, kRsBlock, 0, st>>>(ka, va, kb, vb, n, shift, hist, n_tiles);
+    ++*launches;
+    std::swap(ka, kb);
+    std::swap(va, vb);
+  }
+  // four passes: the sorted data is back in keys/vals
+  cudaFreeAsync(k2, st);
+  cudaFreeAsync(v2, st);
+  cudaFreeAsync(hist, st);
+  if (e.code != GT_OK) return e;
+  GT_CUDA_TRY(cudaGetLastError());
+  return Err{};
+}
+
+// -------------------------------------------------------------- hierarchy
+__device__ __forceinline__ int kdelta(const uint32_t* k, int n, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  uint32_t a = k[i], b = k[j];
+  if (a == b) return 32 + __clz((uint32_t)i ^ (uint32_t)j);
+  return __clz(a ^ b);
+}
+
+// Karras 2012, "Maximizing parallelism in the construction of BVHs, octrees
+// and k-d trees": internal node i covers a key range found by one exponential
+// and two binary searches on the longest common prefix.
+__global__ void k_karras(const uint32_t* keys, int n, float4* nodes, uint32_t* parent_int, uint32_t* parent_leaf) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  int d = (kdelta(keys, n, i, i + 1) - kdelta(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+  int dmin = kdelta(keys, n, i, i - d);
+  int lmax = 2;
+  while (kdelta(keys, n, i, i + lmax * d) > dmin) lmax *= 2;
+  int l = 0;
+  for (int t = lmax / 2; t >= 1; t /= 2)
+    if (kdelta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+  int j = i + l * d;
+  int dnode = kdelta(keys, n, i, j);
+  int s = 0, t = l;
+  do {
+    t = (t + 1) / 2;
+    if (kdelta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+  } while (t > 1);
+  int gamma = i + s * d + min(d, 0);
+  int lo = min(i, j), hi = max(i, j);
+  uint32_t c0 = (lo == gamma) ? (kLeafBit | (uint32_t)gamma) : (uint32_t)gamma;
+  uint32_t c1 = (hi == gamma + 1) ? (kLeafBit | (uint32_t)(gamma + 1)) : (uint32_t)(gamma + 1);
+  nodes[4 * (size_t)i + 3] = make_float4(__uint_as_float(c0), __uint_as_float(c1), 0.f, 0.f);
+  if (c0 & kLeafBit) parent_leaf[gamma] = (uint32_t)i; else parent_int[gamma] = (uint32_t)i;
+  if (c1 & kLeafBit) parent_leaf[gamma + 1] = (uint32_t)i; else parent_int[gamma + 1] = (uint32_t)i;
+  if (i == 0) parent_int[0] = kInvalid;
+}
+
+// Leaf records in leaf order: world-to-object map, particle index, box.
+__global__ void k_leaves(const uint8_t* packed, uint32_t stride, double alpha_min, const uint32_t* sorted_slots,
+                         uint32_t m, const uint32_t* kept_pidx, const float* box_by_slot, float4* w2o,
+                         uint32_t* leaf_pidx, float* leaf_box) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  uint32_t slot = sorted_slots[j];
+  uint32_t p = kept_pidx[slot];
+  float M[12], W[12];
+  proxy_o2w(record(packed, p, stride), alpha_min, M);
+  affine_inverse(M, W);
+  w2o[3 * (size_t)j] = make_float4(W[0], W[1], W[2], W[3]);
+  w2o[3 * (size_t)j + 1] = make_float4(W[4], W[5], W[6], W[7]);
+  w2o[3 * (size_t)j + 2] = make_float4(W[8], W[9], W[10], W[11]);
+  leaf_pidx[j] = p;
+#pragma unroll
+  for (int a = 0; a < 6; ++a) leaf_box[6 * (size_t)j + a] = box_by_slot[6 * (size_t)slot + a];
+}
+
+__device__ __forceinline__ void child_box(uint32_t ref, const float* leaf_box, const float* ibox, float b[6]) {
+  const float* src = (ref & kLeafBit) ? leaf_box + 6 * (size_t)(ref & ~kLeafBit) : ibox + 6 * (size_t)ref;
+#pragma unroll
+  for (int a = 0; a < 6; ++a) b[a] = __ldcg(src + a);
+}
+
+// Bottom-up refit: the second child to arrive at a node writes its boxes.
+__global__ void k_refit(uint32_t m, const float* leaf_box, float* ibox, float4* nodes, const uint32_t* parent_int,
+                        const uint32_t* parent_leaf, uint32_t* arrive) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  uint32_t node = parent_leaf[j];
+  uint32_t guard = 0;
+  while (node != kInvalid && guard++ < 4096u) {
+    __threadfence();
+    if (atomicAdd(&arrive[node], 1u) == 0u) return;
+    float4 f3 = __ldcg(nodes + 4 * (size_t)node + 3);
+    uint32_t c0 = __float_as_uint(f3.x), c1 = __float_as_uint(f3.y);
+    float b0[6], b1[6];
+    child_box(c0, leaf_box, ibox, b0);
+    child_box(c1, leaf_box, ibox, b1);
+    nodes[4 * (size_t)node + 0] = make_float4(b0[0], b0[3], b0[1], b0[4]);
+    nodes[4 * (size_t)node + 1] = make_float4(b1[0], b1[3], b1[1], b1[4]);
+    nodes[4 * (size_t)node + 2] = make_float4(b0[2], b0[5], b1[2], b1[5]);
+    float* ib = ibox + 6 * (size_t)node;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      ib[a] = fminf(b0[a], b1[a]);
+      ib[3 + a] = fmaxf(b0[3 + a], b1[3 + a]);
+    }
+    node = parent_int[node];
+  }
+}
+
+__global__ void k_depth(uint32_t m, const uint32_t* parent_int, const uint32_t* parent_leaf, uint32_t* depth) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  uint32_t d = 0, node = parent_leaf[j];
+  while (node != kInvalid && d < 100000u) {
+    ++d;
+    node = parent_int[node];
+  }
+  atomicMax(depth, d);
+}
+
+// Shading records in particle order: (mu, opacity), precision matrix A of
+// computeResponse (6 unique entries), and the 48 SH floats made tight.
+__global__ void k_shade(const uint8_t* packed, uint64_t n, uint32_t stride, uint32_t n_sh, const uint32_t* flags,
+                        float4* shade, float4* sh) {
+  uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (p >= n || !flags[p]) return;
+  const float* rec = record(packed, p, stride);
+  float q[4] = {rec[8], rec[9], rec[10], rec[11]};
+  float sc[3] = {rec[4], rec[5], rec[6]};
+  float A[3][3];
+  precision_matrix(q, sc, A);
+  shade[3 * p] = make_float4(rec[0], rec[1], rec[2], rec[12]);
+  shade[3 * p + 1] = make_float4(A[0][0], A[1][0], A[2][0], A[1][1]);
+  shade[3 * p + 2] = make_float4(A[2][1], A[2][2], 0.f, 0.f);
+  float v[48];
+#pragma unroll
+  for (int k = 0; k < 16; ++k)
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) v[3 * k + ch] = (uint32_t)k < n_sh ? rec[16 + 4 * k + ch] : 0.0f;
+#pragma unroll
+  for (int i = 0; i < 12; ++i) sh[12 * p + i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+}
+
+// -------------------------------------------------------------- driver
+void free_scene(SceneBuffers* b) {
+  cudaFree(b->nodes);
+  cudaFree(b->w2o);
+  cudaFree(b->leaf_pidx);
+  cudaFree(b->shade);
+  cudaFree(b->sh);
+  *b = SceneBuffers{};
+}
+
+static inline unsigned grid_for(uint64_t n, unsigned block) { return (unsigned)((n + block - 1) / block); }
+
+Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride, double alpha_min, cudaStream_t st,
+                SceneBuffers* out, uint64_t* launches) {
+  SceneBuffers b;
+  b.n_sh = std::min<uint32_t>(16u, (stride - 64u) / 16u);
+  const uint8_t* packed = static_cast<const uint8_t*>(packed_dev);
+  if (n == 0) {
+    *out = b;
+    return Err{};
+  }
+  if (n >= (1ull << 31)) return Err{GT_ERR_INVALID_ARG, "scene larger than 2^31 particles"};
+  // shading records (every particle slot; only kept ones are written/read)
+  GT_CUDA_TRY(cudaMalloc(&b.shade, n * 3 * sizeof(float4)));
+  GT_CUDA_TRY(cudaMalloc(&b.sh, n * 12 * sizeof(float4)));
+  b.bytes += n * 15 * sizeof(float4);
+  uint32_t *flags = nullptr, *slots = nullptr, *bounds = nullptr;
+  GT_CUDA_TRY(cudaMallocAsync(&flags, n * 4, st));
+  GT_CUDA_TRY(cudaMallocAsync(&slots, n * 4, st));
+  GT_CUDA_TRY(cudaMallocAsync(&bounds, 8 * 4, st));
+  const unsigned B = 256;
+  k_keep_flags<<<grid_for(n, B), B, 0, st>>>(packed, n, stride, alpha_min, flags);
+  ++*launches;
+  GT_CUDA_TRY(cudaGetLastError());
+  Err e = scan_exclusive(flags, slots, n, st, launches);
+  if (e.code != GT_OK) return e;
+  uint32_t last_flag = 0, last_slot = 0;
+  GT_CUDA_TRY(cudaMemcpyAsync(&last_flag, flags + (n - 1), 4, cudaMemcpyDeviceToHost, st));
+  GT_CUDA_TRY(cudaMemcpyAsync(&last_slot, slots + (n - 1), 4, cudaMemcpyDeviceToHost, st));
+  GT_CUDA_TRY(cudaStreamSynchronize(st));
+  uint32_t m = last_slot + last_flag;
+  b.n_kept = m;
+  k_shade<<<grid_for(n, 128), 128, 0, st>>>(packed, n, stride, b.n_sh, flags, b.shade, b.sh);
+  ++*launches;
+  if (m == 0) {
+    cudaFreeAsync(flags, st);
+    cudaFreeAsync(slots, st);
+    cudaFreeAsync(bounds, st);
+    GT_CUDA_TRY(cudaStreamSynchronize(st));
+    *out = b;
+    return Err{};
+  }
+  float* box = nullptr;
+  uint32_t *kept_pidx = nullptr, *keys = nullptr, *vals = nullptr;
+  GT_CUDA_TRY(cudaMallocAsync(&box, (size_t)m * 6 * 4, st));
+  GT_CUDA_TRY(cudaMallocAsync(&kept_pidx, (size_t)m * 4, st));
+  GT_CUDA_TRY(cudaMallocAsync(&keys, (size_t)m * 4, st));
+  GT_CUDA_TRY(cudaMallocAsync(&vals, (size_t)m * 4, st));
+  {
+    uint32_t init[8] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u, 0u, 0u};
+    GT_CUDA_TRY(cudaMemcpyAsync(bounds, init, sizeof init, cudaMemcpyHostToDevice, st));
+  }
+  IcoVerts iv;
+  ico_vertices(iv.v);
+  k_proxy_boxes<<<grid_for(n, B), B, 0, st>>>(packed, n, stride, alpha_min, flags, slots, iv, box, kept_pidx, bounds);
+  ++*launches;
+  k_morton<<<grid_for(m, B), B, 0, st>>>(box, m, bounds, keys, vals);
+  ++*launches;
+  GT_CUDA_TRY(cudaGetLastError());
+  e = radix_sort(keys, vals, m, st, launches);
+  if (e.code != GT_OK) return e;
+  // scene records
+  uint32_t n_int = m > 1 ? m - 1 : 0;
+  GT_CUDA_TRY(cudaMalloc(&b.w2o, (size_t)m * 3 * sizeof(float4)));
+  GT_CUDA_TRY(cudaMalloc(&b.leaf_pidx, (size_t)m * 4));
+  GT_CUDA_TRY(cudaMalloc(&b.nodes, (size_t)std::max<uint32_t>(n_int, 1) * 4 * sizeof(float4)));
+  b.bytes += (uint64_t)m * (3 * sizeof(float4) + 4) + (uint64_t)std::max<uint32_t>(n_int, 1) * 4 * sizeof(float4);
+  float *leaf_box = nullptr, *ibox = nullptr;
+  uint32_t *parent_int = nullptr, *parent_leaf = nullptr, *arrive = nullptr, *depth = nullptr;
+  GT_CUDA_TRY(cudaMallocAsync(&leaf_box, (size_t)m * 6 * 4, st));
+  GT_CUDA_TRY(cudaMallocAsync(&ibox, (size_t)std::max<uint32_t>(n_int, 1) * 6 * 4, st));
+  GT_CUDA_TRY(cudaMallocAsync(&parent_int, (size_t)std::max<uint32_t>(n_int, 1) * 4, st));
+  GT_CUDA_TRY(cudaMallocAsync(&parent_leaf, (size_t)m * 4, st));
+  GT_CUDA_TRY(cudaMallocAsync(&arrive, (size_t)std::max<uint32_t>(n_int, 1) * 4, st));
+  GT_CUDA_TRY(cudaMallocAsync(&depth, 4, st));
+  GT_CUDA_TRY(cudaMemsetAsync(arrive, 0, (size_t)std::max<uint32_t>(n_int, 1) * 4, st));
+  GT_CUDA_TRY(cudaMemsetAsync(depth, 0, 4, st));
+  k_leaves<<<grid_for(m, B), B, 0, st>>>(packed, stride, alpha_min, vals, m, kept_pidx, box, b.w2o, b.leaf_pidx,
+                                          leaf_box);
+  ++*launches;
+  if (m > 1) {
+    k_karras<<<grid_for(n_int, B), B, 0, st>>>(keys, (int)m, b.nodes, parent_int, parent_leaf);
+    k_refit<<<grid_for(m, B), B, 0, st>>>(m, leaf_box, ibox, b.nodes, parent_int, parent_leaf, arrive);
+    k_depth<<<grid_for(m, B), B, 0, st>>>(m, parent_int, parent_leaf, depth);
+    *launches += 3;
+    b.root = 0;
+  } else {
+    b.root = kLeafBit | 0u;
+  }
+  GT_CUDA_TRY(cudaGetLastError());
+  float rb[6];
+  uint32_t bo[8];
+  GT_CUDA_TRY(cudaMemcpyAsync(rb, m > 1 ? ibox : leaf_box, sizeof rb, cudaMemcpyDeviceToHost, st));
+  GT_CUDA_TRY(cudaMemcpyAsync(&b.depth, depth, 4, cudaMemcpyDeviceToHost, st));
+  GT_CUDA_TRY(cudaMemcpyAsync(bo, bounds, sizeof bo, cudaMemcpyDeviceToHost, st));
+  GT_CUDA_TRY(cudaStreamSynchronize(st));
+  for (int a = 0; a < 6; ++a) b.bounds[a] = rb[a];
+  float mag = 0.0f;
+  for (int a = 0; a < 6; ++a) mag = std::max(mag, std::fabs(rb[a]));
+  b.scene_mag = mag;
+  cudaFreeAsync(flags, st);
+  cudaFreeAsync(slots, st);
+  cudaFreeAsync(bounds, st);
+  cudaFreeAsync(box, st);
+  cudaFreeAsync(kept_pidx, st);
+  cudaFreeAsync(keys, st);
+  cudaFreeAsync(vals, st);
+  cudaFreeAsync(leaf_box, st);
+  cudaFreeAsync(ibox, st);
+  cudaFreeAsync(parent_int, st);
+  cudaFreeAsync(parent_leaf, st);
+  cudaFreeAsync(arrive, st);
+  cudaFreeAsync(depth, st);
+  GT_CUDA_TRY(cudaStreamSynchronize(st));
+  if (b.depth > kMaxDepth) {
+    free_scene(&b);
+    return Err{GT_ERR_UNSUPPORTED, "BVH deeper than the traversal stack allows"};
+  }
+  *out = b;
+  return Err{};
+}
+
+}  // namespace gt

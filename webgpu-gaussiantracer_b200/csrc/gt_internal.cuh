@@ -1,0 +1,173 @@
+// gt_internal.cuh — shared declarations of the CUDA tracer library.
+//
+// Numerics contract.  The tracer follows one fixed IEEE-754 binary32
+// operation order (the one the CPU oracle states in C): every product and
+// sum is rounded separately (the library is compiled with -fmad=false and
+// uses __f*_rn intrinsics where it matters), division and square root are
+// correctly rounded, and exp is the deterministic Cody-Waite routine below.
+// Hit t values, alphas and radiance are therefore bit-identical to the
+// oracle's float build on the same inputs.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/gtrace.h"
+
+namespace gt {
+
+// ------------------------------------------------------------------ limits
+constexpr int kStackSize = 128;            // traversal stack entries per ray
+constexpr uint32_t kMaxDepth = 120;        // deepest BVH the build accepts
+constexpr uint32_t kInvalid = 0xFFFFFFFFu; // empty k-buffer slot (uint(-1))
+constexpr uint32_t kLeafBit = 0x80000000u; // child reference: leaf flag
+constexpr uint32_t kMaxVisitsPerRound = 1u << 26;  // node-visit cap per round
+constexpr uint32_t kMaxRounds = 1u << 22;          // round cap per ray
+
+// device status word bits
+constexpr uint32_t kStatusStackOverflow = 1u;
+constexpr uint32_t kStatusVisitCap = 2u;
+constexpr uint32_t kStatusRoundCap = 4u;
+constexpr uint32_t kStatusCheckpointFull = 8u;
+
+// Unit icosahedron face constants (src/main.ts:12-25): p0, e0 = p1 - p0,
+// e1 = p0 - p2, n = cross(e1, e0), all in binary32 from the rounded
+// vertices (webrtx/src/glsl/intersect.glsl:73-92 uses exactly these).
+struct FaceTable {
+  float p0[20][3];
+  float e0[20][3];
+  float e1[20][3];
+  float n[20][3];
+  float nmax;      // max |n| component over all faces
+  float r_circ;    // circumradius of the vertex set
+};
+void make_face_table(FaceTable* ft);
+
+// Counters and status shared by the kernels of one call.
+struct DevCounters {
+  unsigned long long rays, rounds, entries, contributing, proxy_tests, node_visits, anyhits;
+  unsigned long long ckpt_rounds;
+  unsigned int status;
+  unsigned int work;  // work-stealing tile counter
+  unsigned int work2;
+  unsigned int pad;
+};
+
+// Scene as the kernels see it.  Records of kept proxies are in BVH leaf
+// order j; shading records are indexed by particle index p.
+struct SceneDev {
+  const float4* nodes;      // 4 float4 per internal node (see gt_build.cu)
+  const float4* w2o;        // 3 float4 per leaf: world-to-object 4x3 column-major
+  const uint32_t* leaf_pidx;// particle index of leaf j
+  const float4* shade;      // 3 float4 per particle: (mu, opacity), (a00,a01,a02,a11), (a12,a22,-,-)
+  const float4* sh;         // 12 float4 per particle: 16 RGB coefficients, tight
+  uint32_t root;            // root reference (kLeafBit | j for a one-proxy scene)
+  uint32_t n_kept;
+  uint32_t n_sh;            // coefficients present (16 for degree-3 data)
+  float scene_mag;          // max |coordinate| of the proxy boxes (padding scale)
+};
+
+// Uniform block fields the kernels use (a copy of gt_uniforms, widened).
+struct RayUniforms {
+  float tw[16];
+  float asp[2];
+  float t_min, t_max, T_min, alpha_min;
+  uint32_t k, deg, early_stop, debug;
+};
+
+inline RayUniforms to_ray_uniforms(const gt_uniforms& u) {
+  RayUniforms r;
+  for (int i = 0; i < 16; ++i) r.tw[i] = u.to_world[i];
+  r.asp[0] = u.camera_aspect[0];
+  r.asp[1] = u.camera_aspect[1];
+  r.t_min = u.t_min;
+  r.t_max = u.t_max;
+  r.T_min = u.T_min;
+  r.alpha_min = u.alpha_min;
+  r.k = u.k;
+  r.deg = u.sh_degree_max;
+  r.early_stop = u.early_stop;
+  r.debug = u.debug_mode;
+  return r;
+}
+
+// One view of a launch: image, output and work-tile range.
+struct ViewDev {
+  RayUniforms u;
+  SceneDev s;
+  float4* out;          // w*h pixels
+  uint32_t w, h;
+  uint32_t tiles_x;     // tiles per row
+  uint32_t tile_begin;  // first global tile index of this view
+  uint32_t n_tiles;
+  const float4* dL;     // backward: dL/drgba (w*h)
+  float* grad;          // backward: 59 x n parameter-major gradient
+  uint64_t n_particles;
+};
+
+// Launch shape of the persistent trace kernel.
+struct LaunchShape {
+  uint32_t block_threads = 128;
+  uint32_t blocks_per_sm = 4;
+  uint32_t tile_w = 8, tile_h = 4;  // a warp's pixel tile (tile_w*tile_h == 32)
+};
+
+// ----------------------------------------------------------- host helpers
+struct Err {
+  gt_status code = GT_OK;
+  std::string msg;
+};
+
+#define GT_CUDA_TRY(expr)                                                         \
+  do {                                                                            \
+    cudaError_t e_ = (expr);                                                      \
+    if (e_ != cudaSuccess) {                                                      \
+      return ::gt::Err{e_ == cudaErrorMemoryAllocation ? GT_ERR_OOM : GT_ERR_CUDA, \
+                       std::string(#expr) + ": " + cudaGetErrorString(e_)};        \
+    }                                                                             \
+  } while (0)
+
+// Scene build (gt_build.cu).
+struct SceneBuffers {
+  float4* nodes = nullptr;
+  float4* w2o = nullptr;
+  uint32_t* leaf_pidx = nullptr;
+  float4* shade = nullptr;
+  float4* sh = nullptr;
+  uint32_t root = 0;
+  uint64_t n_kept = 0;
+  uint32_t depth = 0;
+  uint32_t n_sh = 0;
+  float bounds[6] = {0, 0, 0, 0, 0, 0};
+  float scene_mag = 0;
+  uint64_t bytes = 0;
+};
+Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride_bytes, double alpha_min,
+                cudaStream_t stream, SceneBuffers* out, uint64_t* launches);
+void free_scene(SceneBuffers* b);
+
+// Trace launches (gt_trace.cu).
+Err launch_trace(const ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
+                 const FaceTable& faces, const LaunchShape& shape, int num_sms, cudaStream_t stream,
+                 uint64_t* launches, ViewDev* d_views_scratch);
+Err launch_trace_hits(const ViewDev& view, const uint32_t* pixels, uint32_t n_pix, uint32_t max_entries,
+                      uint32_t* out_pidx, float* out_t, float* out_alpha, uint32_t* out_count,
+                      uint32_t* out_rounds, float4* out_rgba, DevCounters* counters, const FaceTable& faces,
+                      cudaStream_t stream, uint64_t* launches);
+uint32_t kmax_for(uint32_t k);
+
+// Backward (gt_backward.cu).
+struct BwdConfig {
+  uint32_t mode;         // 1 checkpoint, 2 replay
+  uint32_t max_rounds;
+  uint32_t* ckpt_pidx;   // [rays][max_rounds][k] (checkpoint mode)
+  float* ckpt_round;     // [rays][max_rounds][2]: t_curr at round start, T at round start
+  uint32_t* ckpt_nrounds;// [rays]
+};
+Err launch_backward(const ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
+                    const FaceTable& faces, const BwdConfig& cfg, int num_sms, cudaStream_t stream,
+                    uint64_t* launches, ViewDev* d_views_scratch, cudaEvent_t mid_event);
+
+}  // namespace gt

@@ -1,0 +1,262 @@
+"""Host API of the tracer: the drop-in for the reference's render path.
+
+The reference drives its WebGPU pipeline like this (src/main.ts:469-577)::
+
+    const tlas = await gaussianSceneToBvh(device, gsData, alpha_min, GaussianIndices);
+    const rtPipeline = await createRayTracingPipeline(device, tlas, hit_array_size);
+    const sbt = createShaderBindingTable(device, rtPipeline, GaussianIndices);
+    ...
+    passEncoder.traceRays(device, sbt, width, height);
+
+Here the same steps are::
+
+    ctx = Context(0)                                   # adapter + device
+    scene = gaussian_scene_to_bvh(ctx, gs_data, alpha_min, gaussian_indices)
+    rgba = ctx.trace_rays(scene, uniforms, width, height)   # (H, W, 4) float32
+
+The acceleration structure, pipeline and shader binding table collapse into
+one scene handle built on the GPU; ``trace_rays`` takes the reference's
+112-byte uniform block and returns its RGBA-f32 pixel buffer.  Errors are
+raised as ``GTraceError`` (the reference throws strings).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+from .ply import PackedGaussians
+
+
+def _uniforms(u) -> L.Uniforms:
+    if isinstance(u, L.Uniforms):
+        return u
+    b = bytes(np.asarray(u, dtype=np.uint8).tobytes() if not isinstance(u, (bytes, bytearray)) else u)
+    if len(b) != 112:
+        raise ValueError("the uniform block is 112 bytes")
+    return L.Uniforms.from_buffer_copy(b)
+
+
+class Context:
+    """A CUDA device, its stream and the library state (one per GPU)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = L.load()
+        h = C.c_void_p()
+        L.check(self._lib.gt_context_create(device, C.byref(h)), None)
+        self._h = h
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.gt_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def check(self, status: int):
+        L.check(status, self._h)
+
+    # ------------------------------------------------------------- render
+    def render(self, scene: "Scene", uniforms, width: int, height: int, out: np.ndarray | None = None,
+               stats: bool = False):
+        """Renders one view to a host array of shape (height, width, 4)."""
+        u = _uniforms(uniforms)
+        if out is None:
+            out = np.empty((height, width, 4), dtype=np.float32)
+        if out.dtype != np.float32 or not out.flags.c_contiguous or out.size != width * height * 4:
+            raise ValueError("out must be a C-contiguous float32 array of width*height*4 values")
+        st = L.RenderStats()
+        self.check(self._lib.gt_render(self._h, scene.handle, C.byref(u), width, height,
+                                       out.ctypes.data_as(C.c_void_p), 0, C.byref(st)))
+        return (out, st.as_dict()) if stats else out
+
+    trace_rays = render
+
+    def render_device(self, scene: "Scene", uniforms, width: int, height: int, out_dev: int, asynchronous=False):
+        """Renders into a device buffer (pointer from ``device_alloc``)."""
+        u = _uniforms(uniforms)
+        flags = L.GT_FLAG_OUTPUT_DEVICE | (L.GT_FLAG_ASYNC if asynchronous else 0)
+        st = L.RenderStats()
+        self.check(self._lib.gt_render(self._h, scene.handle, C.byref(u), width, height, C.c_void_p(out_dev), flags,
+                                       None if asynchronous else C.byref(st)))
+        return None if asynchronous else st.as_dict()
+
+    def render_hits(self, scene: "Scene", uniforms, width: int, height: int, pixels, max_entries: int = 64):
+        """Composited hit sequences of the listed pixels (see gt_render_hits)."""
+        u = _uniforms(uniforms)
+        pix = np.ascontiguousarray(pixels, dtype=np.uint32)
+        n = pix.shape[0]
+        me = max(int(max_entries), 1)
+        rec = {"pidx": np.zeros((n, me), np.uint32), "t": np.zeros((n, me), np.float32),
+               "alpha": np.zeros((n, me), np.float32), "count": np.zeros(n, np.uint32),
+               "rounds": np.zeros(n, np.uint32), "rgba": np.zeros((n, 4), np.float32)}
+        vp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+        self.check(self._lib.gt_render_hits(self._h, scene.handle, C.byref(u), width, height, vp(pix), n, me,
+                                            vp(rec["pidx"]), vp(rec["t"]), vp(rec["alpha"]), vp(rec["count"]),
+                                            vp(rec["rounds"]), vp(rec["rgba"])))
+        return rec
+
+    def backward(self, scene: "Scene", uniforms, width: int, height: int, dL_drgba: np.ndarray, mode: int = 0,
+                 max_rounds: int = 0, mem_budget: int = 0, out: np.ndarray | None = None, accumulate=False):
+        """dLoss/dparams (59 x n, parameter-major) from dLoss/drgba (h, w, 4)."""
+        u = _uniforms(uniforms)
+        g = np.ascontiguousarray(dL_drgba, dtype=np.float32)
+        if g.size != width * height * 4:
+            raise ValueError("dL_drgba must hold width*height*4 values")
+        if out is None:
+            out = np.zeros((59, scene.n), dtype=np.float32)
+        opts = L.BwdOpts(mode, max_rounds, mem_budget, 0, 0, 0.0, 0.0)
+        st = L.RenderStats()
+        flags = L.GT_FLAG_ACCUMULATE if accumulate else 0
+        self.check(self._lib.gt_backward(self._h, scene.handle, C.byref(u), width, height,
+                                         g.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p), flags,
+                                         C.byref(opts), C.byref(st)))
+        info = st.as_dict()
+        info.update(used_mode=opts.used_mode, fwd_ms=opts.fwd_ms, bwd_ms=opts.bwd_ms)
+        return out, info
+
+    def render_batch(self, views, outs=None, device_outputs=False, asynchronous=False):
+        """views: list of (scene, uniforms, width, height[, out]) -> list of outputs, stats."""
+        items = (L.BatchItem * len(views))()
+        results = []
+        for i, v in enumerate(views):
+            scene, uniforms, w, h = v[:4]
+            if device_outputs:
+                ptr = v[4]
+                results.append(ptr)
+            else:
+                arr = outs[i] if outs is not None else np.empty((h, w, 4), dtype=np.float32)
+                results.append(arr)
+                ptr = arr.ctypes.data
+            items[i].scene = scene.handle
+            items[i].u = _uniforms(uniforms)
+            items[i].w = w
+            items[i].h = h
+            items[i].out_rgba = ptr
+            items[i].dL_drgba = None
+        flags = (L.GT_FLAG_OUTPUT_DEVICE if device_outputs else 0) | (L.GT_FLAG_ASYNC if asynchronous else 0)
+        st = L.RenderStats()
+        self.check(self._lib.gt_render_batch(self._h, items, len(views), flags, None if asynchronous else C.byref(st)))
+        return results, st.as_dict()
+
+    def autotune(self, scene: "Scene", uniforms, width: int, height: int):
+        r = L.TuneResult()
+        self.check(self._lib.gt_autotune(self._h, scene.handle, C.byref(_uniforms(uniforms)), width, height,
+                                         C.byref(r)))
+        return {name: getattr(r, name) for name, _ in r._fields_}
+
+    # ----------------------------------------------------------- helpers
+    def device_alloc(self, nbytes: int) -> int:
+        p = C.c_void_p()
+        self.check(self._lib.gt_device_alloc(self._h, nbytes, C.byref(p)))
+        return p.value
+
+    def device_free(self, ptr: int):
+        self.check(self._lib.gt_device_free(self._h, C.c_void_p(ptr)))
+
+    def host_alloc(self, nbytes: int, dtype=np.float32, shape=None) -> np.ndarray:
+        """Page-locked host array (freed with host_free)."""
+        p = C.c_void_p()
+        self.check(self._lib.gt_host_alloc(self._h, nbytes, C.byref(p)))
+        buf = (C.c_uint8 * nbytes).from_address(p.value)
+        arr = np.frombuffer(buf, dtype=dtype)
+        return arr.reshape(shape) if shape is not None else arr
+
+    def host_free(self, arr: np.ndarray):
+        self.check(self._lib.gt_host_free(self._h, C.c_void_p(arr.ctypes.data)))
+
+    def memcpy(self, dst: int, src: int, nbytes: int, kind: int):
+        self.check(self._lib.gt_memcpy(self._h, C.c_void_p(dst), C.c_void_p(src), nbytes, kind))
+
+    def synchronize(self):
+        self.check(self._lib.gt_synchronize(self._h))
+
+    def timer_start(self):
+        self.check(self._lib.gt_timer_start(self._h))
+
+    def timer_stop(self) -> float:
+        ms = C.c_float()
+        self.check(self._lib.gt_timer_stop(self._h, C.byref(ms)))
+        return ms.value
+
+    def kernel_times(self, max_n: int = 256):
+        buf = (C.c_float * max_n)()
+        n = C.c_uint32()
+        self.check(self._lib.gt_kernel_times(self._h, buf, max_n, C.byref(n)))
+        return [buf[i] for i in range(n.value)]
+
+    def launch_count(self) -> int:
+        n = C.c_uint64()
+        self.check(self._lib.gt_launch_count(self._h, C.byref(n)))
+        return n.value
+
+
+class Scene:
+    """Proxies + BVH + shading records of one packed particle buffer, on the GPU."""
+
+    def __init__(self, ctx: Context, packed: np.ndarray, alpha_min: float, device_ptr: int | None = None,
+                 n: int | None = None, stride: int | None = None):
+        self.ctx = ctx
+        self._lib = ctx._lib
+        h = C.c_void_p()
+        if device_ptr is not None:
+            self.n = int(n)
+            ctx.check(self._lib.gt_scene_create(ctx.handle, C.c_void_p(device_ptr), self.n, int(stride),
+                                                float(alpha_min), L.GT_FLAG_INPUT_DEVICE, C.byref(h)))
+        else:
+            arr = np.ascontiguousarray(packed, dtype=np.float32)
+            self.n = arr.shape[0]
+            stride = arr.shape[1] * 4 if arr.ndim == 2 and self.n else 320
+            ctx.check(self._lib.gt_scene_create(ctx.handle, arr.ctypes.data_as(C.c_void_p) if self.n else None,
+                                                self.n, stride, float(alpha_min), 0, C.byref(h)))
+        self._h = h
+        self.alpha_min = alpha_min
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self) -> dict:
+        i = L.SceneInfo()
+        self.ctx.check(self._lib.gt_scene_get_info(self._h, C.byref(i)))
+        d = {name: getattr(i, name) for name, _ in i._fields_ if not name.startswith("_")}
+        d["bounds"] = list(i.bounds)
+        return d
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.gt_scene_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def gaussian_scene_to_bvh(ctx: Context, gs_data: PackedGaussians, alpha_min: float,
+                          gaussian_indices: list | None = None) -> Scene:
+    """gaussianSceneToBvh (src/main.ts:30-111): one proxy per Gaussian with
+    opacity > alpha_min; fills ``gaussian_indices`` with the kept particle
+    indices in order, as the reference does for its shader binding table."""
+    if gaussian_indices is not None:
+        op = gs_data.gaussianData["opacity"]
+        gaussian_indices.extend(np.nonzero(op > alpha_min)[0].tolist())
+    return Scene(ctx, gs_data.gaussiansBuffer, alpha_min)
