@@ -122,6 +122,8 @@ uint32_t gt_version(void);
 /* Creates a context on CUDA device `device`.  Replaces the adapter/device
  * request of src/main.ts:396-427. */
 gt_status gt_context_create(int device, gt_context** out);
+/* Destroys the context and every scene still alive on it (their handles
+ * become invalid). */
 gt_status gt_context_destroy(gt_context* ctx);
 
 /* Copies the last error message of `ctx` (NUL-terminated, truncated to

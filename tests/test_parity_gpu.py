@@ -52,7 +52,7 @@ def test_hit_sequences_bit_exact(ctx, k):
     got = ctx.render_hits(g, v.uniforms, w, h, pix, max_entries=256)
     _, ref = o.render(v.uniforms, w, h, pixels=pix, max_entries=256)
     _assert_hits_equal(got, ref, 256)
-    assert got["count"].max() > k  # several rounds happened
+    assert got["rounds"].max() >= 2  # several rounds happened
 
 
 def test_small_config_full_image(ctx):

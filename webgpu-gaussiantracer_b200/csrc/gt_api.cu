@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <map>
 #include <mutex>
+#include <set>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -45,6 +46,7 @@ struct gt_context {
   uint64_t launches = 0;
   std::map<std::tuple<uint64_t, uint32_t, uint32_t, uint32_t>, gt_tune_result> tune;
   std::map<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t>, GraphEntry> graphs;
+  std::set<gt_scene*> scenes;  // live scenes; destroyed with the context
 };
 
 struct gt_scene {
@@ -230,6 +232,11 @@ extern "C" gt_status gt_context_destroy(gt_context* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   drop_graphs(ctx);
+  for (gt_scene* s : ctx->scenes) {
+    free_scene(&s->b);
+    delete s;
+  }
+  ctx->scenes.clear();
   cudaFree(ctx->d_ctr);
   cudaFreeHost(ctx->h_ctr);
   cudaFree(ctx->d_views);
@@ -293,14 +300,18 @@ extern "C" gt_status gt_scene_create(gt_context* ctx, const void* packed, uint64
     return fail(ctx, e);
   }
   cudaEventElapsedTime(&s->build_ms, ctx->call0, ctx->call1);
+  ctx->scenes.insert(s);
   *out = s;
   return GT_OK;
 }
 
 extern "C" gt_status gt_scene_destroy(gt_scene* s) {
   if (!s) return GT_OK;
-  cudaSetDevice(s->ctx->device);
-  cudaStreamSynchronize(s->ctx->stream);
+  gt_context* ctx = s->ctx;
+  if (!ctx->scenes.count(s)) return fail(ctx, GT_ERR_INVALID_ARG, "scene already destroyed");
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  ctx->scenes.erase(s);
   free_scene(&s->b);
   delete s;
   return GT_OK;

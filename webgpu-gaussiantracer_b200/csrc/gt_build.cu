@@ -500,6 +500,31 @@ __global__ void k_refit(uint32_t m, const float* leaf_box, float* ibox, float4* 
   }
 }
 
+// Tree check before any traversal: every child reference in range and every
+// node reached by exactly one parent (the root by none).
+__global__ void k_check_children(uint32_t m, const float4* nodes, uint32_t* refcount, uint32_t* bad) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i + 1 >= m) return;
+  float4 f3 = nodes[4 * (size_t)i + 3];
+  uint32_t c[2] = {__float_as_uint(f3.x), __float_as_uint(f3.y)};
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    uint32_t r = c[q];
+    if (r & kLeafBit) {
+      uint32_t j = r & ~kLeafBit;
+      if (j >= m) atomicOr(bad, 1u); else atomicAdd(&refcount[(m - 1) + j], 1u);
+    } else {
+      if (r >= m - 1 || r == 0) atomicOr(bad, 2u); else atomicAdd(&refcount[r], 1u);
+    }
+  }
+}
+__global__ void k_check_counts(uint32_t total, const uint32_t* refcount, uint32_t* bad) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  uint32_t expect = i == 0 ? 0u : 1u;
+  if (refcount[i] != expect) atomicOr(bad, 4u);
+}
+
 __global__ void k_depth(uint32_t m, const uint32_t* parent_int, const uint32_t* parent_leaf, uint32_t* depth) {
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= m) return;
@@ -629,6 +654,15 @@ Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride, double alph
     k_refit<<<grid_for(m, B), B, 0, st>>>(m, leaf_box, ibox, b.nodes, parent_int, parent_leaf, arrive);
     k_depth<<<grid_for(m, B), B, 0, st>>>(m, parent_int, parent_leaf, depth);
     *launches += 3;
+    // structural check: refcount over [internal 0..m-2 | leaves 0..m-1]
+    uint32_t* refc = nullptr;
+    GT_CUDA_TRY(cudaMallocAsync(&refc, (size_t)(2 * m - 1) * 4, st));
+    GT_CUDA_TRY(cudaMemsetAsync(refc, 0, (size_t)(2 * m - 1) * 4, st));
+    GT_CUDA_TRY(cudaMemsetAsync(bounds + 7, 0, 4, st));
+    k_check_children<<<grid_for(n_int, B), B, 0, st>>>(m, b.nodes, refc, bounds + 7);
+    k_check_counts<<<grid_for(2 * m - 1, B), B, 0, st>>>(2 * m - 1, refc, bounds + 7);
+    *launches += 2;
+    cudaFreeAsync(refc, st);
     b.root = 0;
   } else {
     b.root = kLeafBit | 0u;
@@ -658,6 +692,10 @@ Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride, double alph
   cudaFreeAsync(arrive, st);
   cudaFreeAsync(depth, st);
   GT_CUDA_TRY(cudaStreamSynchronize(st));
+  if (bo[7] != 0) {
+    free_scene(&b);
+    return Err{GT_ERR_CUDA, "internal error: the built hierarchy is not a tree"};
+  }
   if (b.depth > kMaxDepth) {
     free_scene(&b);
     return Err{GT_ERR_UNSUPPORTED, "BVH deeper than the traversal stack allows"};

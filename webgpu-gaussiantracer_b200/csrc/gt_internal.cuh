@@ -23,7 +23,6 @@ constexpr int kStackSize = 128;            // traversal stack entries per ray
 constexpr uint32_t kMaxDepth = 120;        // deepest BVH the build accepts
 constexpr uint32_t kInvalid = 0xFFFFFFFFu; // empty k-buffer slot (uint(-1))
 constexpr uint32_t kLeafBit = 0x80000000u; // child reference: leaf flag
-constexpr uint32_t kMaxVisitsPerRound = 1u << 26;  // node-visit cap per round
 constexpr uint32_t kMaxRounds = 1u << 22;          // round cap per ray
 
 // device status word bits

@@ -141,13 +141,15 @@ __device__ __forceinline__ void traverse(const SceneDev& S, const BoxRay& br, fl
   int sp = 0;
   uint32_t cur = S.root;
   uint32_t visits = 0;
+  // a tree walk pops every internal node at most once
+  const uint32_t max_visits = S.n_kept + 64u;
   while (true) {
     if (cur & kLeafBit) {
       ++st.proxy_tests;
       leaf(cur & ~kLeafBit, thi());
     } else {
       ++st.node_visits;
-      if (++visits > kMaxVisitsPerRound) {
+      if (++visits > max_visits) {
         status |= kStatusVisitCap;
         return;
       }

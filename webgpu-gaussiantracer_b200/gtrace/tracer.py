@@ -22,6 +22,7 @@ raised as ``GTraceError`` (the reference throws strings).
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -47,13 +48,17 @@ class Context:
         L.check(self._lib.gt_context_create(device, C.byref(h)), None)
         self._h = h
         self.device = device
+        self._scenes = weakref.WeakSet()
 
     @property
     def handle(self):
         return self._h
 
     def close(self):
+        """Destroys the context; scenes built on it are released with it."""
         if getattr(self, "_h", None):
+            for s in list(self._scenes):
+                s._h = None  # freed by gt_context_destroy
             self._lib.gt_context_destroy(self._h)
             self._h = None
 
@@ -227,9 +232,12 @@ class Scene:
                                                 self.n, stride, float(alpha_min), 0, C.byref(h)))
         self._h = h
         self.alpha_min = alpha_min
+        ctx._scenes.add(self)
 
     @property
     def handle(self):
+        if not self._h:
+            raise ValueError("scene is closed (or its context was closed)")
         return self._h
 
     def info(self) -> dict:
@@ -240,9 +248,9 @@ class Scene:
         return d
 
     def close(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and getattr(self.ctx, "_h", None):
             self._lib.gt_scene_destroy(self._h)
-            self._h = None
+        self._h = None
 
     def __del__(self):
         try:
