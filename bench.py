@@ -111,6 +111,10 @@ def make_workload(name: str):
     if name == "clusters-1m-1080p":
         pg, amin, v = synth.clusters_1m_config()
         desc = "1M Gaussians (64 clusters), 1920x1080, k=16, alpha_min=0.01, T_min=0.01, SH3, camera radius 12"
+    elif name == "clusters-1m-480x270":
+        pg, amin, v = synth.clusters_1m_config()
+        v = synth.view(480, 270, (0.0, 0.0, 12.0), k=16)
+        desc = "1M Gaussians (64 clusters), 480x270 (profiling size), k=16, alpha_min=0.01, T_min=0.01, SH3"
     elif name == "small-256":
         pg, amin, v = synth.small_config()
         desc = "16,384 Gaussians (uniform), 256x256, k=6, alpha_min=0.01, T_min=0.01, SH3, camera at distance 4"
