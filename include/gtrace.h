@@ -228,6 +228,26 @@ typedef struct gt_batch_item {
 gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items, uint32_t count,
                           uint32_t flags, gt_render_stats* stats);
 
+/* Renders a batch exactly like gt_render_batch but allocates no memory.
+ * For callers that cannot allocate while they render: a frame loop that must
+ * never stall on cudaMalloc/cudaFree (both synchronise the whole device), or
+ * a process whose GPU memory is owned and capped by another allocator.
+ * No counterpart in the reference.
+ *   - outputs must be device buffers: GT_FLAG_OUTPUT_DEVICE is required
+ *     (host outputs would need a staging allocation);
+ *   - at most 256 views per call; larger counts are rejected with
+ *     GT_ERR_INVALID_ARG;
+ *   - the launch's scratch (tile counter, statistics, device view table,
+ *     about 56 KB) lives in one fixed array in the library's device image;
+ *     every GPU that loads the library holds a copy until the process exits;
+ *   - the first call on a device looks up that array's address (do it before
+ *     any stream capture);
+ *   - all calls on a device share the array and it keeps the last call's
+ *     contents: calls whose GPU work overlaps (other contexts or streams on
+ *     the same device) race; calls on one context are stream-ordered. */
+gt_status gt_render_batch_noalloc(gt_context* ctx, const gt_batch_item* items, uint32_t count,
+                                  uint32_t flags, gt_render_stats* stats);
+
 /* Accumulates, per scene, the gradients of all its views in one launch.
  * dL_dparams[s] receives the sum over the items whose scene is scenes[s]. */
 gt_status gt_backward_batch(gt_context* ctx, const gt_batch_item* items, uint32_t count,

@@ -1,0 +1,103 @@
+"""gt_render_batch_noalloc: the batched render for callers that cannot
+allocate while they render (a frame loop that must not stall on
+cudaMalloc/cudaFree, which synchronise the device; a process whose GPU memory
+is owned by another allocator).  Its scratch lives in a fixed device array,
+so this test calls it through the C ABI twice in a row and checks each result
+against gt_render_batch on the same views, bit for bit (the tolerance of the
+other parity tests).  The file name sorts last so that a run stopping at the
+first failure has run every other test already; it also passes alone."""
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+for p in (ROOT, os.path.join(ROOT, "webgpu-gaussiantracer_b200")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+from gtrace import _lib as L  # noqa: E402
+from gtrace import synth  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _scene(lib, ctx, n, seed, alpha_min):
+    rec = np.ascontiguousarray(synth.pack(synth.raw_small(n=n, seed=seed)).gaussiansBuffer)
+    h = C.c_void_p()
+    assert lib.gt_scene_create(ctx, rec.ctypes.data_as(C.c_void_p), rec.shape[0], 320, alpha_min, 0,
+                               C.byref(h)) == L.GT_OK, L.last_error(ctx)
+    return h
+
+
+def test_noalloc_batch_matches_gt_render_batch():
+    lib = L.load()
+    ctx = C.c_void_p()
+    assert lib.gt_context_create(0, C.byref(ctx)) == L.GT_OK, L.last_error(None)
+    buffers = []
+    try:
+        s1 = _scene(lib, ctx, 1200, 31, 0.01)
+        s2 = _scene(lib, ctx, 2000, 32, 0.05)
+        shapes = [(s1, synth.view(37, 21, (0.0, 0.0, 4.0), k=6), 37, 21),
+                  (s2, synth.view(64, 40, (1.0, 2.0, 3.5), k=16), 64, 40),
+                  (s1, synth.view(16, 16, (0.5, -3.0, 2.0), k=3), 16, 16)]
+        count = len(shapes)
+
+        def items_for(outs):
+            items = (L.BatchItem * count)()
+            for i, (sc, v, w, h) in enumerate(shapes):
+                items[i].scene = sc
+                items[i].u = L.Uniforms.from_buffer_copy(v.uniforms.tobytes())
+                items[i].w, items[i].h = w, h
+                items[i].out_rgba = outs[i]
+                items[i].dL_drgba = None
+            return items
+
+        def device_buffers():
+            outs = []
+            for _, _, w, h in shapes:
+                p = C.c_void_p()
+                assert lib.gt_device_alloc(ctx, w * h * 16, C.byref(p)) == L.GT_OK
+                buffers.append(p.value)
+                outs.append(p.value)
+            return outs
+
+        def download(outs):
+            res = []
+            for (_, _, w, h), p in zip(shapes, outs):
+                a = np.empty((h, w, 4), np.float32)
+                assert lib.gt_memcpy(ctx, a.ctypes.data_as(C.c_void_p), C.c_void_p(p), w * h * 16, 1) == L.GT_OK
+                res.append(a)
+            return res
+
+        ref_outs = device_buffers()
+        st = L.RenderStats()
+        assert lib.gt_render_batch(ctx, items_for(ref_outs), count, L.GT_FLAG_OUTPUT_DEVICE,
+                                   C.byref(st)) == L.GT_OK, L.last_error(ctx)
+        ref = download(ref_outs)
+        assert st.rays == sum(w * h for _, _, w, h in shapes)
+
+        na_outs = device_buffers()
+        for call in range(2):  # the static scratch is reused: two calls in a row
+            for p, (_, _, w, h) in zip(na_outs, shapes):
+                zero = np.zeros(w * h * 4, np.float32)
+                assert lib.gt_memcpy(ctx, C.c_void_p(p), zero.ctypes.data_as(C.c_void_p), w * h * 16, 0) == L.GT_OK
+            st2 = L.RenderStats()
+            rc = lib.gt_render_batch_noalloc(ctx, items_for(na_outs), count, L.GT_FLAG_OUTPUT_DEVICE, C.byref(st2))
+            assert rc == L.GT_OK, L.last_error(ctx)
+            got = download(na_outs)
+            for a, b in zip(got, ref):
+                np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
+            assert st2.rays == st.rays and st2.entries == st.entries and st2.status_flags == 0
+
+        # sizes beyond the fixed scratch and host outputs are rejected
+        big = (L.BatchItem * 257)()
+        assert lib.gt_render_batch_noalloc(ctx, big, 257, L.GT_FLAG_OUTPUT_DEVICE, None) == L.GT_ERR_INVALID_ARG
+        assert "256" in L.last_error(ctx)
+        assert lib.gt_render_batch_noalloc(ctx, items_for(na_outs), count, 0, None) == L.GT_ERR_INVALID_ARG
+    finally:
+        for p in buffers:
+            lib.gt_device_free(ctx, C.c_void_p(p))
+        lib.gt_context_destroy(ctx)

@@ -12,51 +12,14 @@
 #include <tuple>
 #include <vector>
 
+#include "gt_handles.h"
 #include "gt_internal.cuh"
 
 using namespace gt;
 
 namespace {
 thread_local std::string g_last_error;  // errors without a context
-constexpr int kEventRing = 256;
-
-struct GraphEntry {
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-};
 }  // namespace
-
-struct gt_context {
-  int device = 0;
-  int num_sms = 148;
-  cudaStream_t stream = nullptr;
-  std::string err;
-  FaceTable faces;
-  DevCounters* d_ctr = nullptr;
-  DevCounters* h_ctr = nullptr;  // pinned
-  ViewDev* d_views = nullptr;
-  uint32_t d_views_cap = 0;
-  ViewDev* h_views = nullptr;    // pinned staging for view tables
-  uint32_t h_views_cap = 0;
-  float4* staging = nullptr;
-  size_t staging_bytes = 0;
-  cudaEvent_t call0 = nullptr, call1 = nullptr, timer0 = nullptr, timer1 = nullptr;
-  cudaEvent_t ring[2 * kEventRing];
-  uint64_t ring_head = 0, ring_tail = 0;
-  uint64_t launches = 0;
-  std::map<std::tuple<uint64_t, uint32_t, uint32_t, uint32_t>, gt_tune_result> tune;
-  std::map<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t>, GraphEntry> graphs;
-  std::set<gt_scene*> scenes;  // live scenes; destroyed with the context
-};
-
-struct gt_scene {
-  gt_context* ctx = nullptr;
-  SceneBuffers b;
-  uint64_t n = 0;
-  uint32_t stride = 0;
-  double alpha_min = 0.0;
-  float build_ms = 0.0f;
-};
 
 // ----------------------------------------------------------------- helpers
 static gt_status fail(gt_context* ctx, gt_status code, const std::string& msg) {
@@ -164,6 +127,16 @@ static ViewDev make_view(const gt_scene* s, const gt_uniforms& u, uint32_t w, ui
   return v;
 }
 
+namespace gt {
+gt_status api_fail(gt_context* ctx, gt_status code, const std::string& msg) { return fail(ctx, code, msg); }
+gt_status api_status_to_error(gt_context* ctx, uint32_t status) { return status_to_error(ctx, status); }
+gt_status api_check_uniforms(gt_context* ctx, const gt_uniforms* u) { return check_uniforms(ctx, u); }
+ViewDev api_make_view(const gt_scene* s, const gt_uniforms& u, uint32_t w, uint32_t h, float4* out,
+                      uint32_t tile_begin) {
+  return make_view(s, u, w, h, out, tile_begin);
+}
+}  // namespace gt
+
 static uint64_t ring_slot(gt_context* ctx) { return (ctx->ring_head++) % kEventRing; }
 
 static void fill_stats(const DevCounters& c, gt_render_stats* st) {
@@ -187,6 +160,13 @@ static LaunchShape shape_for(gt_context* ctx, const gt_scene* s, uint32_t w, uin
   }
   return sh;
 }
+
+namespace gt {
+LaunchShape api_shape_for(gt_context* ctx, const gt_scene* s, uint32_t w, uint32_t h, uint32_t k) {
+  return shape_for(ctx, s, w, h, k);
+}
+void api_fill_stats(const DevCounters& c, gt_render_stats* st) { fill_stats(c, st); }
+}  // namespace gt
 
 // ============================================================== context
 extern "C" uint32_t gt_version(void) { return GT_ABI_VERSION; }

@@ -1,0 +1,63 @@
+// gt_handles.h — the library's definitions of the opaque C-ABI handles.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <set>
+#include <string>
+#include <tuple>
+
+#include "gt_internal.cuh"
+
+namespace gt {
+constexpr int kEventRing = 256;
+
+struct GraphEntry {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+}  // namespace gt
+
+struct gt_context {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  gt::FaceTable faces;
+  gt::DevCounters* d_ctr = nullptr;
+  gt::DevCounters* h_ctr = nullptr;  // pinned
+  gt::ViewDev* d_views = nullptr;
+  uint32_t d_views_cap = 0;
+  gt::ViewDev* h_views = nullptr;    // pinned staging for view tables
+  uint32_t h_views_cap = 0;
+  float4* staging = nullptr;
+  size_t staging_bytes = 0;
+  cudaEvent_t call0 = nullptr, call1 = nullptr, timer0 = nullptr, timer1 = nullptr;
+  cudaEvent_t ring[2 * gt::kEventRing];
+  uint64_t ring_head = 0, ring_tail = 0;
+  uint64_t launches = 0;
+  std::map<std::tuple<uint64_t, uint32_t, uint32_t, uint32_t>, gt_tune_result> tune;
+  std::map<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t>, gt::GraphEntry> graphs;
+  std::set<gt_scene*> scenes;  // live scenes; destroyed with the context
+};
+
+struct gt_scene {
+  gt_context* ctx = nullptr;
+  gt::SceneBuffers b;
+  uint64_t n = 0;
+  uint32_t stride = 0;
+  double alpha_min = 0.0;
+  float build_ms = 0.0f;
+};
+
+namespace gt {
+// shared by the C-ABI translation units (gt_api.cu)
+gt_status api_fail(gt_context* ctx, gt_status code, const std::string& msg);
+gt_status api_status_to_error(gt_context* ctx, uint32_t status);
+gt_status api_check_uniforms(gt_context* ctx, const gt_uniforms* u);
+ViewDev api_make_view(const gt_scene* s, const gt_uniforms& u, uint32_t w, uint32_t h, float4* out,
+                      uint32_t tile_begin);
+LaunchShape api_shape_for(gt_context* ctx, const gt_scene* s, uint32_t w, uint32_t h, uint32_t k);
+void api_fill_stats(const DevCounters& c, gt_render_stats* st);
+}  // namespace gt

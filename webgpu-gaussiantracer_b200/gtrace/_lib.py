@@ -88,6 +88,7 @@ SIGNATURES = [
     ("gt_backward", _i32, [_vp, _vp, C.POINTER(Uniforms), _u32, _u32, _vp, _vp, _u32, C.POINTER(BwdOpts),
                            C.POINTER(RenderStats)]),
     ("gt_render_batch", _i32, [_vp, C.POINTER(BatchItem), _u32, _u32, C.POINTER(RenderStats)]),
+    ("gt_render_batch_noalloc", _i32, [_vp, C.POINTER(BatchItem), _u32, _u32, C.POINTER(RenderStats)]),
     ("gt_backward_batch", _i32, [_vp, C.POINTER(BatchItem), _u32, C.POINTER(_vp), C.POINTER(_vp), _u32, _u32,
                                  C.POINTER(BwdOpts), C.POINTER(RenderStats)]),
     ("gt_autotune", _i32, [_vp, _vp, C.POINTER(Uniforms), _u32, _u32, C.POINTER(TuneResult)]),
