@@ -119,7 +119,9 @@ __device__ __forceinline__ void proxy_test(const FaceTable& F, const float4* w2o
               fabsf(d.z) * (fabsf(m[6]) + fabsf(m[7]) + fabsf(m[8]));
     tau = 1e-5f * F.nmax * s;
   }
-#pragma unroll
+  // rolled on purpose: one copy of the triangle test and of the caller's
+  // k-buffer insertion keeps the kernel small enough for the instruction cache
+#pragma unroll 1
   for (int f = 0; f < 20; ++f) {
     float dn = vdot(mk(F.n[f][0], F.n[f][1], F.n[f][2]), od);
     if (CULL && dn > tau) continue;
@@ -252,63 +254,88 @@ struct HitRecord {
   }
 };
 
-// tracePath (src/GS_shader.ts:192-273) for one pixel.
+// Per-lane state of one primary ray between rounds.
+struct RayState {
+  V3 o, d;
+  BoxRay br;
+  float L0, L1, L2, T, t_curr;
+  uint32_t step, n_entries;
+};
+
+__device__ __forceinline__ void ray_init(const ViewDev& V, uint32_t px, uint32_t py, RayState& R) {
+  ray_gen(V.u, V.w, V.h, px, py, R.o, R.d);
+  R.br = make_boxray(R.o, R.d, V.s.scene_mag);
+  R.L0 = R.L1 = R.L2 = 0.0f;
+  R.T = 1.0f;
+  R.t_curr = V.u.t_min;
+  R.step = 0;
+  R.n_entries = 0;
+}
+
+// The loop condition of tracePath (src/GS_shader.ts:231-234): another round
+// starts while T_min < T and t_curr < t_max, unless earlyStop == step.
+__device__ __forceinline__ bool ray_more(const ViewDev& V, const RayState& R) {
+  return V.u.T_min < R.T && R.t_curr < V.u.t_max && V.u.early_stop != R.step;
+}
+
+// One round of tracePath (src/GS_shader.ts:235-269): collect the k closest
+// front-face hits beyond t_curr, advance t_curr, composite the entries.
+template <int KMAX, class Rec>
+__device__ __forceinline__ void ray_round(const ViewDev& V, const FaceTable& F, RayState& R, RayStats& st,
+                                          uint32_t& status, Rec& rec) {
+  const float t_max = V.u.t_max;
+  const int first = KMAX - (int)V.u.k;
+  ++R.step;
+  float bt[KMAX];
+  uint32_t bp[KMAX];
+#pragma unroll
+  for (int i = 0; i < KMAX; ++i) {
+    bt[i] = i < first ? -CUDART_INF_F : t_max;
+    bp[i] = i < first ? 0u : kInvalid;
+  }
+  collect_round<KMAX>(V.s, F, R.o, R.d, R.br, R.t_curr, t_max, bt, bp, st, status);
+  ++st.rounds;
+  R.t_curr = bt[KMAX - 1] + 1e-4f;
+#pragma unroll
+  for (int i = 0; i < KMAX; ++i) {
+    if (i < first) continue;
+    if (bp[i] == kInvalid) {
+      R.t_curr = t_max;
+      break;
+    }
+    uint32_t p = bp[i];
+    Shade sd = load_shade(V.s.shade, p);
+    float alpha = response(sd, R.o, R.d) * sd.opacity;
+    rec.entry(R.n_entries, p, bt[i], alpha);
+    ++R.n_entries;
+    ++st.entries;
+    if (V.u.alpha_min < alpha) {
+      ++st.contributing;
+      V3 dir = vnorm(vsub(sd.mu, R.o));
+      float c[3];
+      sh_radiance(V.s.sh, p, dir, V.u.deg, c);
+      float ta = R.T * alpha;
+      R.L0 = R.L0 + ta * (c[0] > 0.0f ? c[0] : 0.0f);
+      R.L1 = R.L1 + ta * (c[1] > 0.0f ? c[1] : 0.0f);
+      R.L2 = R.L2 + ta * (c[2] > 0.0f ? c[2] : 0.0f);
+      R.T = R.T * (1.0f - alpha);
+    }
+  }
+  if (R.step >= kMaxRounds && ray_more(V, R)) {
+    status |= kStatusRoundCap;
+    R.t_curr = t_max;
+  }
+}
+
+// tracePath (src/GS_shader.ts:192-273) for one pixel, all rounds.
 template <int KMAX, class Rec>
 __device__ __forceinline__ float4 trace_pixel(const ViewDev& V, const FaceTable& F, uint32_t px, uint32_t py,
                                               RayStats& st, uint32_t& status, Rec& rec, uint32_t* n_entries_out) {
-  V3 o, d;
-  ray_gen(V.u, V.w, V.h, px, py, o, d);
-  BoxRay br = make_boxray(o, d, V.s.scene_mag);
-  float L0 = 0.0f, L1 = 0.0f, L2 = 0.0f, T = 1.0f;
-  float t_curr = V.u.t_min;
-  const float t_max = V.u.t_max;
-  const int first = KMAX - (int)V.u.k;
-  uint32_t step = 0, n_entries = 0;
-  while (V.u.T_min < T && t_curr < t_max) {
-    if (V.u.early_stop == step) break;
-    ++step;
-    if (step > kMaxRounds) {
-      status |= kStatusRoundCap;
-      break;
-    }
-    float bt[KMAX];
-    uint32_t bp[KMAX];
-#pragma unroll
-    for (int i = 0; i < KMAX; ++i) {
-      bt[i] = i < first ? -CUDART_INF_F : t_max;
-      bp[i] = i < first ? 0u : kInvalid;
-    }
-    collect_round<KMAX>(V.s, F, o, d, br, t_curr, t_max, bt, bp, st, status);
-    ++st.rounds;
-    t_curr = bt[KMAX - 1] + 1e-4f;
-#pragma unroll
-    for (int i = 0; i < KMAX; ++i) {
-      if (i < first) continue;
-      if (bp[i] == kInvalid) {
-        t_curr = t_max;
-        break;
-      }
-      uint32_t p = bp[i];
-      Shade sd = load_shade(V.s.shade, p);
-      float alpha = response(sd, o, d) * sd.opacity;
-      rec.entry(n_entries, p, bt[i], alpha);
-      ++n_entries;
-      ++st.entries;
-      if (V.u.alpha_min < alpha) {
-        ++st.contributing;
-        V3 dir = vnorm(vsub(sd.mu, o));
-        float c[3];
-        sh_radiance(V.s.sh, p, dir, V.u.deg, c);
-        float ta = T * alpha;
-        L0 = L0 + ta * (c[0] > 0.0f ? c[0] : 0.0f);
-        L1 = L1 + ta * (c[1] > 0.0f ? c[1] : 0.0f);
-        L2 = L2 + ta * (c[2] > 0.0f ? c[2] : 0.0f);
-        T = T * (1.0f - alpha);
-      }
-    }
-  }
-  if (n_entries_out) *n_entries_out = n_entries;
-  return make_float4(L0, L1, L2, 1.0f);
+  RayState R;
+  ray_init(V, px, py, R);
+  while (ray_more(V, R)) ray_round<KMAX>(V, F, R, st, status, rec);
+  if (n_entries_out) *n_entries_out = R.n_entries;
+  return make_float4(R.L0, R.L1, R.L2, 1.0f);
 }
 
 // Debug views (src/GS_shader.ts:201-228, 289-296, 312-321).
@@ -393,29 +420,71 @@ __device__ __forceinline__ uint32_t find_view(const ViewDev* views, uint32_t n_v
   return lo;
 }
 
-// Persistent trace kernel over the tiles of all views.
+// Persistent trace kernel over all pixels of all views.  Work items are
+// pixel slots: slot = 32 * tile + lane-in-tile, tiles of 8x4 pixels in
+// row-major order per view, views back to back.  A lane whose ray is done
+// takes the next slot at once (warp-aggregated atomic), so rays of very
+// different length do not hold whole warps idle.
 template <int KMAX>
 __global__ void __launch_bounds__(128) k_trace(const ViewDev* __restrict__ views, uint32_t n_views,
                                                uint32_t total_tiles, DevCounters* ctr,
                                                const __grid_constant__ FaceTable F) {
   const uint32_t lane = threadIdx.x & 31;
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  const uint32_t total_slots = total_tiles * 32u;
   RayStats st = {0, 0, 0, 0, 0, 0};
   uint32_t status = 0, rays = 0;
   NoRecord rec;
+  bool active = false, exhausted = false;
+  uint32_t vi = 0, px = 0, py = 0;
+  RayState R;
   while (true) {
-    uint32_t tile = 0;
-    if (lane == 0) tile = atomicAdd(&ctr->work, 1u);
-    tile = __shfl_sync(0xFFFFFFFFu, tile, 0);
-    if (tile >= total_tiles) break;
-    const ViewDev& V = views[n_views == 1 ? 0 : find_view(views, n_views, tile)];
-    uint32_t lt = tile - V.tile_begin;
-    uint32_t px = (lt % V.tiles_x) * kTileW + (lane % kTileW);
-    uint32_t py = (lt / V.tiles_x) * kTileH + (lane / kTileW);
-    if (px < V.w && py < V.h) {
-      float4 r = V.u.debug == 0 ? trace_pixel<KMAX>(V, F, px, py, st, status, rec, nullptr)
-                                : trace_debug(V, F, px, py, st, status, nullptr);
-      V.out[(size_t)py * V.w + px] = r;
-      ++rays;
+    bool want = !active && !exhausted;
+    uint32_t need = __ballot_sync(0xFFFFFFFFu, want);
+    while (need) {
+      int leader = __ffs(need) - 1;
+      uint32_t base = 0;
+      if ((int)lane == leader) base = atomicAdd(&ctr->work, (uint32_t)__popc(need));
+      base = __shfl_sync(0xFFFFFFFFu, base, leader);
+      if (want) {
+        uint32_t slot = base + __popc(need & lt_mask);
+        if (slot >= total_slots || slot < base) {
+          exhausted = true;
+          want = false;
+        } else {
+          uint32_t tile = slot >> 5, s = slot & 31u;
+          vi = n_views == 1 ? 0u : find_view(views, n_views, tile);
+          const ViewDev& V = views[vi];
+          uint32_t lt = tile - V.tile_begin;
+          px = (lt % V.tiles_x) * kTileW + (s % kTileW);
+          py = (lt / V.tiles_x) * kTileH + (s / kTileW);
+          if (px < V.w && py < V.h) {
+            want = false;
+            if (V.u.debug == 0) {
+              ray_init(V, px, py, R);
+              active = ray_more(V, R);
+              if (!active) {  // no round at all: black pixel
+                V.out[(size_t)py * V.w + px] = make_float4(0.f, 0.f, 0.f, 1.f);
+                ++rays;
+              }
+            } else {
+              V.out[(size_t)py * V.w + px] = trace_debug(V, F, px, py, st, status, nullptr);
+              ++rays;
+            }
+          }
+        }
+      }
+      need = __ballot_sync(0xFFFFFFFFu, want);
+    }
+    if (!__any_sync(0xFFFFFFFFu, active)) break;
+    if (active) {
+      const ViewDev& V = views[vi];
+      ray_round<KMAX>(V, F, R, st, status, rec);
+      if (!ray_more(V, R)) {
+        V.out[(size_t)py * V.w + px] = make_float4(R.L0, R.L1, R.L2, 1.0f);
+        ++rays;
+        active = false;
+      }
     }
   }
   flush_stats(ctr, st, rays, status);
