@@ -203,6 +203,10 @@ extern "C" gt_status gt_context_create(int device, gt_context** out) {
   for (int i = 0; i < 2 * kEventRing; ++i) CTX_TRY(cudaEventCreate(&ctx->ring[i]));
 #undef CTX_TRY
   make_face_table(&ctx->faces);
+  if (ctx->faces.npairs != 10) {
+    gt_context_destroy(ctx);
+    return fail(nullptr, GT_ERR_CUDA, "internal error: icosahedron face table has no antipodal pairing");
+  }
   *out = ctx;
   return GT_OK;
 }

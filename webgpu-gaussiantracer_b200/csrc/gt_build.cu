@@ -76,6 +76,38 @@ void make_face_table(FaceTable* F) {
   for (int i = 0; i < 12; ++i)
     r = fmaxf(r, sqrtf(v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]));
   F->r_circ = r;
+  float em = 0.0f;
+  for (int f = 0; f < 20; ++f) {
+    em = fmaxf(em, fabsf(F->e0[f][0]) + fabsf(F->e0[f][1]) + fabsf(F->e0[f][2]));
+    em = fmaxf(em, fabsf(F->e1[f][0]) + fabsf(F->e1[f][1]) + fabsf(F->e1[f][2]));
+  }
+  F->emax = em;
+  for (int f = 0; f < 20; ++f)
+    F->c[f] = F->n[f][0] * F->p0[f][0] + F->n[f][1] * F->p0[f][1] + F->n[f][2] * F->p0[f][2];
+  // antipodal pairs: the face whose vertices are the negated vertices of f
+  int q = 0;
+  bool used[20] = {false};
+  for (int f = 0; f < 20 && q < 10; ++f) {
+    if (used[f]) continue;
+    for (int g = f + 1; g < 20; ++g) {
+      int match = 0;
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          const float* va = v + 3 * kIcoIdx[3 * f + a];
+          const float* vb = v + 3 * kIcoIdx[3 * g + b];
+          if (va[0] == -vb[0] && va[1] == -vb[1] && va[2] == -vb[2]) ++match;
+        }
+      bool neg = F->n[g][0] == -F->n[f][0] && F->n[g][1] == -F->n[f][1] && F->n[g][2] == -F->n[f][2];
+      if (match == 3 && neg) {
+        F->pa[q] = f;
+        F->pb[q] = g;
+        used[f] = used[g] = true;
+        ++q;
+        break;
+      }
+    }
+  }
+  F->npairs = q;
 }
 static_assert(sizeof(kIcoIdx) == 60 * sizeof(int), "table size");
 

@@ -41,6 +41,10 @@ struct FaceTable {
   float n[20][3];
   float nmax;      // max |n| component over all faces
   float r_circ;    // circumradius of the vertex set
+  float emax;      // max L1 norm of the edge vectors e0, e1
+  float c[20];     // plane offsets n . p0 (pre-check only)
+  int pa[10], pb[10];  // antipodal face pairs: n[pb[q]] == -n[pa[q]] bit for bit
+  int npairs;          // 10 (checked when the context is created)
 };
 void make_face_table(FaceTable* ft);
 

@@ -87,47 +87,80 @@ __device__ __forceinline__ void node_test(const float4& f0, const float4& f1, co
 
 // Ray/proxy test.  Calls on_hit(t, face) for every face hit by the reference
 // triangle test with t in (tlo, thi) that is front-facing (CULL) or any
-// (!CULL).  Two exact filters run first:
+// (!CULL).  Three exact filters run before that test; each skips only work
+// whose outcome is already known:
 //   * bounding sphere: every triangle lies inside the circumsphere, and the
 //     triangle test cannot report a point farther than its rounding error
 //     (covered by the 1e-3 + 1e-5 |o_obj| margin) from its triangle;
 //   * facing: dot(n, d_obj) and the reference's world-space facing product
-//     both approximate n^T W2O d within 1e-5 * nmax * sum(|W2O||d|), so a
-//     face whose dot(n, d_obj) exceeds that bound is back-facing.
+//     both approximate n^T W2O d within tau = 1e-5 * nmax * sum(|W2O||d|), so
+//     a face whose dot(n, d_obj) exceeds tau is back-facing.  Faces come in
+//     antipodal pairs with n_b == -n_a bit for bit, so dot(n_b, d) ==
+//     -dot(n_a, d) exactly and one dot product serves both;
+//   * t range: the triangle test's t times dn lies within
+//     E = 10 u nmax (|p0|_1 + |o|_1) of num = n.p0 - n.o (u = 2^-24), so a
+//     face with num >= tlo*dn + M or num <= thi*dn - M (dn < 0) has its t
+//     outside (tlo, thi); M = 3e-5 nmax (|o|_1 + 2) + 1e-6 (|tlo|+|thi|)|dn|
+//     is ~50x that error.
 template <bool CULL, class OnHit>
 __device__ __forceinline__ void proxy_test(const FaceTable& F, const float4* w2o, uint32_t j, V3 o, V3 d, float tlo,
                                            float thi, OnHit&& on_hit) {
   Affine W = load_affine(w2o + 3 * (size_t)j);
   V3 oo = xpoint(W, o), od = xdir(W, d);
+  float l1o = fabsf(oo.x) + fabsf(oo.y) + fabsf(oo.z);
   {
     float dd = __fmaf_rn(od.x, od.x, __fmaf_rn(od.y, od.y, od.z * od.z));
     float ox = __fmaf_rn(oo.x, od.x, __fmaf_rn(oo.y, od.y, oo.z * od.z));
     float tc = -__fdividef(ox, dd);
     float cx = __fmaf_rn(tc, od.x, oo.x), cy = __fmaf_rn(tc, od.y, oo.y), cz = __fmaf_rn(tc, od.z, oo.z);
     float r2 = __fmaf_rn(cx, cx, __fmaf_rn(cy, cy, cz * cz));
-    float l1 = fabsf(oo.x) + fabsf(oo.y) + fabsf(oo.z);
-    float rp = __fmaf_rn(1e-5f, l1, F.r_circ + 1e-3f);
+    float rp = __fmaf_rn(1e-5f, l1o, F.r_circ + 1e-3f);
     if (!(r2 <= rp * rp)) {
       if (dd == dd && r2 == r2) return;  // NaN falls through to the exact test
     }
   }
-  float tau = 0.0f;
-  if (CULL) {
-    const float* m = W.m;
-    float s = fabsf(d.x) * (fabsf(m[0]) + fabsf(m[1]) + fabsf(m[2])) +
-              fabsf(d.y) * (fabsf(m[3]) + fabsf(m[4]) + fabsf(m[5])) +
-              fabsf(d.z) * (fabsf(m[6]) + fabsf(m[7]) + fabsf(m[8]));
-    tau = 1e-5f * F.nmax * s;
+  if (!CULL) {
+#pragma unroll 1
+    for (int f = 0; f < 20; ++f) {
+      float dn = vdot(mk(F.n[f][0], F.n[f][1], F.n[f][2]), od);
+      float t;
+      if (tri_test(F, f, oo, tlo, od, thi, dn, t)) on_hit(t, f);
+    }
+    return;
   }
+  const float* m = W.m;
+  float s = fabsf(d.x) * (fabsf(m[0]) + fabsf(m[1]) + fabsf(m[2])) +
+            fabsf(d.y) * (fabsf(m[3]) + fabsf(m[4]) + fabsf(m[5])) +
+            fabsf(d.z) * (fabsf(m[6]) + fabsf(m[7]) + fabsf(m[8]));
+  const float tau = 1e-5f * F.nmax * s;
+  const float mbase = 3e-5f * F.nmax * (l1o + 2.0f);
+  const float trange = 1e-6f * (fabsf(tlo) + fminf(fabsf(thi), 1e30f));
   // rolled on purpose: one copy of the triangle test and of the caller's
   // k-buffer insertion keeps the kernel small enough for the instruction cache
 #pragma unroll 1
-  for (int f = 0; f < 20; ++f) {
-    float dn = vdot(mk(F.n[f][0], F.n[f][1], F.n[f][2]), od);
-    if (CULL && dn > tau) continue;
-    float t;
-    if (tri_test(F, f, oo, tlo, od, thi, dn, t)) {
-      if (!CULL || front_facing(F, f, W, d)) on_hit(t, f);
+  for (int pair = 0; pair < 10; ++pair) {
+    const int fa = F.pa[pair];
+    const V3 na = mk(F.n[fa][0], F.n[fa][1], F.n[fa][2]);
+    const float dna = vdot(na, od);
+    if (fabsf(dna) > tau) {
+      // exactly one face of the pair can face the ray
+      const int f = dna < 0.0f ? fa : F.pb[pair];
+      const float dn = dna < 0.0f ? dna : -dna;
+      const float no = __fmaf_rn(na.x, oo.x, __fmaf_rn(na.y, oo.y, na.z * oo.z));
+      const float num = F.c[f] - (dna < 0.0f ? no : -no);
+      const float mg = __fmaf_rn(trange, fabsf(dn), mbase);
+      if (num >= __fmaf_rn(tlo, dn, mg) || num <= __fmaf_rn(thi, dn, -mg)) continue;
+      float t;
+      if (tri_test(F, f, oo, tlo, od, thi, dn, t) && front_facing(F, f, W, d)) on_hit(t, f);
+    } else {
+      // grazing pair: both faces go to the exact test
+#pragma unroll 1
+      for (int c = 0; c < 2; ++c) {
+        const int f = c ? F.pb[pair] : fa;
+        const float dn = c ? -dna : dna;
+        float t;
+        if (tri_test(F, f, oo, tlo, od, thi, dn, t) && front_facing(F, f, W, d)) on_hit(t, f);
+      }
     }
   }
 }
