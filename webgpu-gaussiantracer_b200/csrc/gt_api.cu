@@ -44,6 +44,7 @@ static gt_status status_to_error(gt_context* ctx, uint32_t status) {
   if (status & (kStatusVisitCap | kStatusRoundCap))
     return fail(ctx, GT_ERR_DEVICE_TIMEOUT, "a device loop reached its iteration limit");
   if (status & kStatusCheckpointFull) return fail(ctx, GT_ERR_DEVICE_TIMEOUT, "checkpoint capacity exceeded");
+  if (status & kStatusHitOverflow) return fail(ctx, GT_ERR_CUDA, "internal error: too many hits on one proxy");
   return GT_OK;
 }
 
@@ -100,6 +101,7 @@ static gt_status ensure_staging(gt_context* ctx, size_t bytes) {
 static SceneDev scene_dev(const gt_scene* s) {
   SceneDev d;
   d.nodes = s->b.nodes;
+  d.nodes8 = s->b.nodes8;
   d.w2o = s->b.w2o;
   d.leaf_pidx = s->b.leaf_pidx;
   d.shade = s->b.shade;
@@ -390,7 +392,11 @@ extern "C" gt_status gt_render_hits(gt_context* ctx, const gt_scene* scene, cons
   uint32_t* d_count = reinterpret_cast<uint32_t*>(buf + (size_t)n_pix * (20 + 12 * me));
   uint32_t* d_rounds = reinterpret_cast<uint32_t*>(buf + (size_t)n_pix * (24 + 12 * me));
   ViewDev v = make_view(scene, *u, w, h, nullptr, 0);
-  gt_status rc = GT_OK;
+  gt_status rc = ensure_views(ctx, 1);
+  if (rc != GT_OK) {
+    cudaFree(buf);
+    return rc;
+  }
   do {
     cudaError_t ce = cudaMemcpyAsync(d_pix, pixels, (size_t)n_pix * 4, cudaMemcpyHostToDevice, ctx->stream);
     if (ce == cudaSuccess) ce = cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), ctx->stream);
@@ -398,7 +404,7 @@ extern "C" gt_status gt_render_hits(gt_context* ctx, const gt_scene* scene, cons
       rc = fail(ctx, GT_ERR_CUDA, cudaGetErrorString(ce));
       break;
     }
-    Err e = launch_trace_hits(v, d_pix, n_pix, (uint32_t)me, d_pidx, d_t, d_alpha, d_count, d_rounds,
+    Err e = launch_trace_hits(v, ctx->d_views, d_pix, n_pix, (uint32_t)me, d_pidx, d_t, d_alpha, d_count, d_rounds,
                               out_rgba ? d_rgba : nullptr, ctx->d_ctr, ctx->faces, ctx->stream, &ctx->launches);
     if (e.code != GT_OK) {
       rc = fail(ctx, e);

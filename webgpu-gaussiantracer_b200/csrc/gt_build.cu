@@ -22,6 +22,7 @@
 //   f2 = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)
 //   f3 = (child0, child1, 0, 0) as uint bits; kLeafBit | j marks leaf j.
 #include <math.h>
+#include <string.h>
 
 #include <algorithm>
 #include <vector>
@@ -591,9 +592,155 @@ __global__ void k_shade(const uint8_t* packed, uint64_t n, uint32_t stride, uint
   for (int i = 0; i < 12; ++i) sh[12 * p + i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
 }
 
+// ------------------------------------------------------------- BVH8 collapse
+// Greedy collapse of the binary hierarchy into 8-wide nodes: a node starts
+// with the two children of a binary node and repeatedly opens its internal
+// entry of largest surface area until it holds 8 entries or only leaves.
+// Each binary internal node ends up inside exactly one 8-wide node, and
+// every 8-wide node opens at least one binary node, so there are fewer
+// 8-wide nodes than binary internal nodes.
+//
+// 8-wide node layout: 8 child records of 32 bytes (2 float4):
+//   f0 = (lo.x, lo.y, lo.z, hi.x), f1 = (hi.y, hi.z, ref, 0)
+// ref = kLeafBit | j for leaf j, an 8-wide node index, or kInvalid (empty
+// slot, with an empty box).
+struct Entry8 {
+  float b[6];
+  uint32_t ref;  // binary reference: kLeafBit | j or internal index
+};
+
+__device__ __forceinline__ void binary_children(const float4* bn, uint32_t i, Entry8& c0, Entry8& c1) {
+  float4 f0 = bn[4 * (size_t)i], f1 = bn[4 * (size_t)i + 1], f2 = bn[4 * (size_t)i + 2], f3 = bn[4 * (size_t)i + 3];
+  c0.b[0] = f0.x; c0.b[3] = f0.y; c0.b[1] = f0.z; c0.b[4] = f0.w; c0.b[2] = f2.x; c0.b[5] = f2.y;
+  c1.b[0] = f1.x; c1.b[3] = f1.y; c1.b[1] = f1.z; c1.b[4] = f1.w; c1.b[2] = f2.z; c1.b[5] = f2.w;
+  c0.ref = __float_as_uint(f3.x);
+  c1.ref = __float_as_uint(f3.y);
+}
+
+__device__ __forceinline__ float half_area(const float b[6]) {
+  float x = b[3] - b[0], y = b[4] - b[1], z = b[5] - b[2];
+  return x * y + y * z + z * x;
+}
+
+__global__ void k_collapse8(const float4* bn, const uint32_t* front_bin, const uint32_t* front_n8, uint32_t n_front,
+                            float4* nodes8, uint32_t* next_bin, uint32_t* next_n8, uint32_t* counters,
+                            uint32_t max_nodes8) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_front) return;
+  uint32_t bi = front_bin[i], n8 = front_n8[i];
+  Entry8 e[8];
+  binary_children(bn, bi, e[0], e[1]);
+  int cnt = 2;
+  while (cnt < 8) {
+    int best = -1;
+    float ba = -1.0f;
+    for (int q = 0; q < cnt; ++q) {
+      if (e[q].ref & kLeafBit) continue;
+      float a = half_area(e[q].b);
+      if (a > ba) {
+        ba = a;
+        best = q;
+      }
+    }
+    if (best < 0) break;
+    Entry8 c0, c1;
+    binary_children(bn, e[best].ref, c0, c1);
+    e[best] = c0;
+    e[cnt++] = c1;
+  }
+  float4* out = nodes8 + 16 * (size_t)n8;
+  for (int q = 0; q < 8; ++q) {
+    if (q < cnt) {
+      uint32_t ref = e[q].ref;
+      if (!(ref & kLeafBit)) {
+        uint32_t child8 = atomicAdd(&counters[0], 1u);
+        if (child8 >= max_nodes8) {
+          atomicOr(&counters[2], 1u);
+          child8 = 0;
+        } else {
+          uint32_t slot = atomicAdd(&counters[1], 1u);
+          next_bin[slot] = ref;
+          next_n8[slot] = child8;
+        }
+        ref = child8;
+      }
+      out[2 * q] = make_float4(e[q].b[0], e[q].b[1], e[q].b[2], e[q].b[3]);
+      out[2 * q + 1] = make_float4(e[q].b[4], e[q].b[5], __uint_as_float(ref), 0.f);
+    } else {
+      out[2 * q] = make_float4(1e30f, 1e30f, 1e30f, -1e30f);
+      out[2 * q + 1] = make_float4(-1e30f, -1e30f, __uint_as_float(kInvalid), 0.f);
+    }
+  }
+}
+
+// Collapses the binary hierarchy (m leaves) into `*out8` (exactly sized).
+static Err collapse_bvh8(const float4* bn, const float* leaf_box, uint32_t m, cudaStream_t st, float4** out8,
+                         uint32_t* n_nodes8, uint64_t* launches) {
+  uint32_t cap = std::max<uint32_t>(m > 1 ? m - 1 : 1, 1);
+  float4* tmp = nullptr;
+  uint32_t *fb = nullptr, *fn = nullptr, *nb = nullptr, *nn = nullptr, *ctr = nullptr;
+  GT_CUDA_TRY(cudaMallocAsync(&tmp, (size_t)cap * 16 * sizeof(float4), st));
+  GT_CUDA_TRY(cudaMallocAsync(&fb, (size_t)cap * 4, st));
+  GT_CUDA_TRY(cudaMallocAsync(&fn, (size_t)cap * 4, st));
+  GT_CUDA_TRY(cudaMallocAsync(&nb, (size_t)cap * 4, st));
+  GT_CUDA_TRY(cudaMallocAsync(&nn, (size_t)cap * 4, st));
+  GT_CUDA_TRY(cudaMallocAsync(&ctr, 4 * 4, st));
+  uint32_t total = 1;
+  if (m == 1) {
+    float lb[6];
+    GT_CUDA_TRY(cudaMemcpyAsync(lb, leaf_box, sizeof lb, cudaMemcpyDeviceToHost, st));
+    GT_CUDA_TRY(cudaStreamSynchronize(st));
+    auto bits = [](uint32_t u) {
+      float f;
+      memcpy(&f, &u, 4);
+      return f;
+    };
+    float4 host[16];
+    host[0] = make_float4(lb[0], lb[1], lb[2], lb[3]);
+    host[1] = make_float4(lb[4], lb[5], bits(kLeafBit | 0u), 0.f);
+    for (int q = 1; q < 8; ++q) {
+      host[2 * q] = make_float4(1e30f, 1e30f, 1e30f, -1e30f);
+      host[2 * q + 1] = make_float4(-1e30f, -1e30f, bits(kInvalid), 0.f);
+    }
+    GT_CUDA_TRY(cudaMemcpyAsync(tmp, host, sizeof host, cudaMemcpyHostToDevice, st));
+  } else {
+    uint32_t init[4] = {1u, 0u, 0u, 0u};
+    uint32_t zero = 0u;
+    GT_CUDA_TRY(cudaMemcpyAsync(ctr, init, sizeof init, cudaMemcpyHostToDevice, st));
+    GT_CUDA_TRY(cudaMemcpyAsync(fb, &zero, 4, cudaMemcpyHostToDevice, st));
+    GT_CUDA_TRY(cudaMemcpyAsync(fn, &zero, 4, cudaMemcpyHostToDevice, st));
+    uint32_t n_front = 1;
+    for (int level = 0; n_front > 0 && level < 1000; ++level) {
+      GT_CUDA_TRY(cudaMemsetAsync(ctr + 1, 0, 4, st));
+      k_collapse8<<<(n_front + 127) / 128, 128, 0, st>>>(bn, fb, fn, n_front, tmp, nb, nn, ctr, cap);
+      ++*launches;
+      GT_CUDA_TRY(cudaGetLastError());
+      uint32_t c[4];
+      GT_CUDA_TRY(cudaMemcpyAsync(c, ctr, sizeof c, cudaMemcpyDeviceToHost, st));
+      GT_CUDA_TRY(cudaStreamSynchronize(st));
+      if (c[2]) return Err{GT_ERR_CUDA, "internal error: 8-wide collapse exceeded its node bound"};
+      total = c[0];
+      n_front = c[1];
+      std::swap(fb, nb);
+      std::swap(fn, nn);
+    }
+  }
+  GT_CUDA_TRY(cudaMalloc(out8, (size_t)total * 16 * sizeof(float4)));
+  GT_CUDA_TRY(cudaMemcpyAsync(*out8, tmp, (size_t)total * 16 * sizeof(float4), cudaMemcpyDeviceToDevice, st));
+  cudaFreeAsync(tmp, st);
+  cudaFreeAsync(fb, st);
+  cudaFreeAsync(fn, st);
+  cudaFreeAsync(nb, st);
+  cudaFreeAsync(nn, st);
+  cudaFreeAsync(ctr, st);
+  *n_nodes8 = total;
+  return Err{};
+}
+
 // -------------------------------------------------------------- driver
 void free_scene(SceneBuffers* b) {
   cudaFree(b->nodes);
+  cudaFree(b->nodes8);
   cudaFree(b->w2o);
   cudaFree(b->leaf_pidx);
   cudaFree(b->shade);
@@ -700,6 +847,11 @@ Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride, double alph
     b.root = kLeafBit | 0u;
   }
   GT_CUDA_TRY(cudaGetLastError());
+  {
+    Err ce = collapse_bvh8(b.nodes, leaf_box, m, st, &b.nodes8, &b.n_nodes8, launches);
+    if (ce.code != GT_OK) return ce;
+    b.bytes += (uint64_t)b.n_nodes8 * 16 * sizeof(float4);
+  }
   float rb[6];
   uint32_t bo[8];
   GT_CUDA_TRY(cudaMemcpyAsync(rb, m > 1 ? ibox : leaf_box, sizeof rb, cudaMemcpyDeviceToHost, st));

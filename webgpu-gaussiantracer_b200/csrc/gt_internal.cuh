@@ -30,6 +30,7 @@ constexpr uint32_t kStatusStackOverflow = 1u;
 constexpr uint32_t kStatusVisitCap = 2u;
 constexpr uint32_t kStatusRoundCap = 4u;
 constexpr uint32_t kStatusCheckpointFull = 8u;
+constexpr uint32_t kStatusHitOverflow = 16u;  // more hits on one proxy than a vertex allows
 
 // Unit icosahedron face constants (src/main.ts:12-25): p0, e0 = p1 - p0,
 // e1 = p0 - p2, n = cross(e1, e0), all in binary32 from the rounded
@@ -62,6 +63,7 @@ struct DevCounters {
 // order j; shading records are indexed by particle index p.
 struct SceneDev {
   const float4* nodes;      // 4 float4 per internal node (see gt_build.cu)
+  const float4* nodes8;     // 16 float4 per 8-wide node (see gt_build.cu)
   const float4* w2o;        // 3 float4 per leaf: world-to-object 4x3 column-major
   const uint32_t* leaf_pidx;// particle index of leaf j
   const float4* shade;      // 3 float4 per particle: (mu, opacity), (a00,a01,a02,a11), (a12,a22,-,-)
@@ -135,6 +137,8 @@ struct Err {
 // Scene build (gt_build.cu).
 struct SceneBuffers {
   float4* nodes = nullptr;
+  float4* nodes8 = nullptr;  // 8-wide nodes: 8 child records of 2 float4
+  uint32_t n_nodes8 = 0;
   float4* w2o = nullptr;
   uint32_t* leaf_pidx = nullptr;
   float4* shade = nullptr;
@@ -155,8 +159,8 @@ void free_scene(SceneBuffers* b);
 Err launch_trace(const ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
                  const FaceTable& faces, const LaunchShape& shape, int num_sms, cudaStream_t stream,
                  uint64_t* launches, ViewDev* d_views_scratch);
-Err launch_trace_hits(const ViewDev& view, const uint32_t* pixels, uint32_t n_pix, uint32_t max_entries,
-                      uint32_t* out_pidx, float* out_t, float* out_alpha, uint32_t* out_count,
+Err launch_trace_hits(const ViewDev& view, ViewDev* d_views, const uint32_t* pixels, uint32_t n_pix,
+                      uint32_t max_entries, uint32_t* out_pidx, float* out_t, float* out_alpha, uint32_t* out_count,
                       uint32_t* out_rounds, float4* out_rgba, DevCounters* counters, const FaceTable& faces,
                       cudaStream_t stream, uint64_t* launches);
 uint32_t kmax_for(uint32_t k);

@@ -1,550 +1,449 @@
-// gt_trace.cu — forward tracer: one persistent kernel for any number of views.
+// gt_trace.cu — forward tracer, one warp per ray, over the 8-wide BVH.
 //
 // Replaces the reference's per-pixel mega compute shader (raygen + tracePath
 // rounds, src/GS_shader.ts:192-309; traversal, webrtx/src/glsl/trace.glsl:42-245;
 // any-hit k-buffer, src/GS_shader.ts:323-367).
 //
-// Design:
-//   * Persistent warps.  A warp takes a tile of 32 pixels (8x4) from a global
-//     atomic counter, traces it, and takes the next; tiles of all views of a
-//     batch share one counter, so uneven views balance themselves.
-//   * One ray per lane.  Each round collects the k closest front-face proxy
-//     hits beyond t_curr into a sorted register k-buffer (fully unrolled,
-//     KMAX slots; the k active slots sit at the end, the others hold -inf and
-//     never move), then composites them in order.
-//   * Traversal of the binary LBVH with a per-lane stack in local memory,
-//     nearer child first, popped entries skipped once the k-th hit is closer.
-//     The far bound of every box test is the current k-th hit, so a round
-//     touches only the front of the ray.
-//   * A proxy is tested in object space: the ray goes through the leaf's
-//     world-to-object map, a conservative bounding-sphere test drops most
-//     candidates, and the reference's triangle test then runs on the faces
-//     that can be front-facing.
-//
-// Round semantics (equal to the reference's): the set of a round is the k
-// smallest front-face hits with t in (t_curr, t_max), ordered by (t, particle
-// index); the reference reaches the same set through its commit rule, which
-// never discards one of the k closest hits.  Ties in t are ordered by particle
-// index (the reference orders them by arrival).
+// Why a warp per ray: rays of a Gaussian scene differ wildly in the number of
+// rounds, nodes and proxies they touch, so one ray per lane leaves most lanes
+// idle (2.6 of 32 active in the thread-per-ray version).  Here the 32 lanes
+// of a warp cooperate on one ray and every control decision is warp-uniform:
+//   * traversal: up to 4 nodes are popped at once and their 32 children are
+//     box-tested by the 32 lanes; hit inner children are sorted by entry
+//     distance (warp bitonic sort) and pushed far-to-near onto a per-warp
+//     stack in shared memory; hit leaves go to a per-warp leaf queue;
+//   * leaves: 32 queued proxies are tested at a time, one per lane, with the
+//     exact object-space test of the reference (gt_trace_common.cuh);
+//   * k-buffer: lane i holds the i-th closest hit (t, particle) found so far;
+//     a hit is inserted with one ballot and one shuffle.  The buffer keeps the
+//     32 closest hits beyond t_curr, so a traversal can feed several rounds
+//     of k <= 16: a round's set (the k smallest hits with t > t_curr) is
+//     certain whenever it lies inside the buffer or the buffer is not full;
+//   * compositing: lanes evaluate the response and SH colour of one entry
+//     each; the front-to-back accumulation then runs in entry order on
+//     broadcast values, so the float operations are those of the reference
+//     loop (src/GS_shader.ts:250-269), in the same order.
 #include <math_constants.h>
 
 #include "gt_device.cuh"
 #include "gt_internal.cuh"
+#include "gt_trace_common.cuh"
 
 namespace gt {
 
-constexpr int kTileW = 8, kTileH = 4;
+constexpr int kWarpsPerBlock = 4;
+constexpr int kWarpStack = 256;  // stack entries per warp
+constexpr int kLeafQueue = 96;   // leaf queue entries per warp (<= 63 in use)
+constexpr int kMaxHitsPerProxy = 6;
+constexpr uint32_t kFull = 0xFFFFFFFFu;
 
-struct RayStats {
-  uint32_t rounds, entries, contributing, proxy_tests, node_visits, anyhits;
+struct WarpScratch {
+  uint32_t snode[kWarpStack];
+  float st[kWarpStack];
+  uint32_t leafq[kLeafQueue];
+  float leaft[kLeafQueue];
 };
 
-// Box-test state of a ray: inverse direction, origin times inverse direction
-// and, per axis, a padding of the slab planes that covers the rounding of
-// the object-space triangle test (hit points lie within ~1e-6 relative of
-// |origin| + scene size of the true surface).
-struct BoxRay {
-  float ix, iy, iz, ox, oy, oz, px, py, pz;
+struct HitOut {
+  uint32_t* pidx;   // [slot][max_entries]
+  float* t;
+  float* alpha;
+  uint32_t* count;  // [slot]
+  uint32_t* rounds; // [slot]
+  float4* rgba;     // [slot] or null
+  uint32_t max_entries;
 };
 
-__device__ __forceinline__ float safe_inv(float d) {
-  float a = fabsf(d) < 1e-30f ? copysignf(1e-30f, d) : d;
-  return __frcp_rn(a);
-}
-
-__device__ __forceinline__ BoxRay make_boxray(V3 o, V3 d, float scene_mag) {
-  BoxRay b;
-  b.ix = safe_inv(d.x);
-  b.iy = safe_inv(d.y);
-  b.iz = safe_inv(d.z);
-  b.ox = o.x * b.ix;
-  b.oy = o.y * b.iy;
-  b.oz = o.z * b.iz;
-  float m = fmaxf(fmaxf(fabsf(o.x), fabsf(o.y)), fabsf(o.z));
-  float pad = 4e-6f * (m + scene_mag) + 1e-7f;
-  b.px = pad * fabsf(b.ix);
-  b.py = pad * fabsf(b.iy);
-  b.pz = pad * fabsf(b.iz);
-  return b;
-}
-
-// Slab test of the two children of a node against [tlo, thi].
-__device__ __forceinline__ void node_test(const float4& f0, const float4& f1, const float4& f2, const BoxRay& r,
-                                          float tlo, float thi, float& n0, float& n1, bool& h0, bool& h1) {
-  float ax = __fmaf_rn(f0.x, r.ix, -r.ox), bx = __fmaf_rn(f0.y, r.ix, -r.ox);
-  float ay = __fmaf_rn(f0.z, r.iy, -r.oy), by = __fmaf_rn(f0.w, r.iy, -r.oy);
-  float az = __fmaf_rn(f2.x, r.iz, -r.oz), bz = __fmaf_rn(f2.y, r.iz, -r.oz);
-  n0 = fmaxf(fmaxf(fminf(ax, bx) - r.px, fminf(ay, by) - r.py), fmaxf(fminf(az, bz) - r.pz, tlo));
-  float x0 = fminf(fminf(fmaxf(ax, bx) + r.px, fmaxf(ay, by) + r.py), fminf(fmaxf(az, bz) + r.pz, thi));
-  h0 = n0 <= x0;
-  float cx = __fmaf_rn(f1.x, r.ix, -r.ox), dx = __fmaf_rn(f1.y, r.ix, -r.ox);
-  float cy = __fmaf_rn(f1.z, r.iy, -r.oy), dy = __fmaf_rn(f1.w, r.iy, -r.oy);
-  float cz = __fmaf_rn(f2.z, r.iz, -r.oz), dz = __fmaf_rn(f2.w, r.iz, -r.oz);
-  n1 = fmaxf(fmaxf(fminf(cx, dx) - r.px, fminf(cy, dy) - r.py), fmaxf(fminf(cz, dz) - r.pz, tlo));
-  float x1 = fminf(fminf(fmaxf(cx, dx) + r.px, fmaxf(cy, dy) + r.py), fminf(fmaxf(cz, dz) + r.pz, thi));
-  h1 = n1 <= x1;
-}
-
-// Ray/proxy test.  Calls on_hit(t, face) for every face hit by the reference
-// triangle test with t in (tlo, thi) that is front-facing (CULL) or any
-// (!CULL).  Three exact filters run before that test; each skips only work
-// whose outcome is already known:
-//   * bounding sphere: every triangle lies inside the circumsphere, and the
-//     triangle test cannot report a point farther than its rounding error
-//     (covered by the 1e-3 + 1e-5 |o_obj| margin) from its triangle;
-//   * facing: dot(n, d_obj) and the reference's world-space facing product
-//     both approximate n^T W2O d within tau = 1e-5 * nmax * sum(|W2O||d|), so
-//     a face whose dot(n, d_obj) exceeds tau is back-facing.  Faces come in
-//     antipodal pairs with n_b == -n_a bit for bit, so dot(n_b, d) ==
-//     -dot(n_a, d) exactly and one dot product serves both;
-//   * t range: the triangle test's t times dn lies within
-//     E = 10 u nmax (|p0|_1 + |o|_1) of num = n.p0 - n.o (u = 2^-24), so a
-//     face with num >= tlo*dn + M or num <= thi*dn - M (dn < 0) has its t
-//     outside (tlo, thi); M = 3e-5 nmax (|o|_1 + 2) + 1e-6 (|tlo|+|thi|)|dn|
-//     is ~50x that error.
-template <bool CULL, class OnHit>
-__device__ __forceinline__ void proxy_test(const FaceTable& F, const float4* w2o, uint32_t j, V3 o, V3 d, float tlo,
-                                           float thi, OnHit&& on_hit) {
-  Affine W = load_affine(w2o + 3 * (size_t)j);
-  V3 oo = xpoint(W, o), od = xdir(W, d);
-  float l1o = fabsf(oo.x) + fabsf(oo.y) + fabsf(oo.z);
-  {
-    float dd = __fmaf_rn(od.x, od.x, __fmaf_rn(od.y, od.y, od.z * od.z));
-    float ox = __fmaf_rn(oo.x, od.x, __fmaf_rn(oo.y, od.y, oo.z * od.z));
-    float tc = -__fdividef(ox, dd);
-    float cx = __fmaf_rn(tc, od.x, oo.x), cy = __fmaf_rn(tc, od.y, oo.y), cz = __fmaf_rn(tc, od.z, oo.z);
-    float r2 = __fmaf_rn(cx, cx, __fmaf_rn(cy, cy, cz * cz));
-    float rp = __fmaf_rn(1e-5f, l1o, F.r_circ + 1e-3f);
-    if (!(r2 <= rp * rp)) {
-      if (dd == dd && r2 == r2) return;  // NaN falls through to the exact test
-    }
-  }
-  if (!CULL) {
-#pragma unroll 1
-    for (int f = 0; f < 20; ++f) {
-      float dn = vdot(mk(F.n[f][0], F.n[f][1], F.n[f][2]), od);
-      float t;
-      if (tri_test(F, f, oo, tlo, od, thi, dn, t)) on_hit(t, f);
-    }
-    return;
-  }
-  const float* m = W.m;
-  float s = fabsf(d.x) * (fabsf(m[0]) + fabsf(m[1]) + fabsf(m[2])) +
-            fabsf(d.y) * (fabsf(m[3]) + fabsf(m[4]) + fabsf(m[5])) +
-            fabsf(d.z) * (fabsf(m[6]) + fabsf(m[7]) + fabsf(m[8]));
-  const float tau = 1e-5f * F.nmax * s;
-  const float mbase = 3e-5f * F.nmax * (l1o + 2.0f);
-  const float trange = 1e-6f * (fabsf(tlo) + fminf(fabsf(thi), 1e30f));
-  // rolled on purpose: one copy of the triangle test and of the caller's
-  // k-buffer insertion keeps the kernel small enough for the instruction cache
-#pragma unroll 1
-  for (int pair = 0; pair < 10; ++pair) {
-    const int fa = F.pa[pair];
-    const V3 na = mk(F.n[fa][0], F.n[fa][1], F.n[fa][2]);
-    const float dna = vdot(na, od);
-    if (fabsf(dna) > tau) {
-      // exactly one face of the pair can face the ray
-      const int f = dna < 0.0f ? fa : F.pb[pair];
-      const float dn = dna < 0.0f ? dna : -dna;
-      const float no = __fmaf_rn(na.x, oo.x, __fmaf_rn(na.y, oo.y, na.z * oo.z));
-      const float num = F.c[f] - (dna < 0.0f ? no : -no);
-      const float mg = __fmaf_rn(trange, fabsf(dn), mbase);
-      if (num >= __fmaf_rn(tlo, dn, mg) || num <= __fmaf_rn(thi, dn, -mg)) continue;
-      float t;
-      if (tri_test(F, f, oo, tlo, od, thi, dn, t) && front_facing(F, f, W, d)) on_hit(t, f);
-    } else {
-      // grazing pair: both faces go to the exact test
-#pragma unroll 1
-      for (int c = 0; c < 2; ++c) {
-        const int f = c ? F.pb[pair] : fa;
-        const float dn = c ? -dna : dna;
-        float t;
-        if (tri_test(F, f, oo, tlo, od, thi, dn, t) && front_facing(F, f, W, d)) on_hit(t, f);
+// Warp bitonic sort of (key, val), ascending by key over the 32 lanes.
+__device__ __forceinline__ void warp_sort(float& key, uint32_t& val, uint32_t lane) {
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      float ok = __shfl_xor_sync(kFull, key, j);
+      uint32_t ov = __shfl_xor_sync(kFull, val, j);
+      bool up = (lane & k) == 0;
+      bool lower = (lane & j) == 0;
+      bool take = (lower == up) ? (ok < key) : (ok > key);
+      if (take) {
+        key = ok;
+        val = ov;
       }
     }
   }
 }
 
-// Generic stack traversal.  thi() gives the current far bound; leaf(j, thi)
-// tests proxy j.  Returns false if a bound was exceeded (status set).
-template <class ThiFn, class LeafFn>
-__device__ __forceinline__ void traverse(const SceneDev& S, const BoxRay& br, float tlo, ThiFn&& thi, LeafFn&& leaf,
-                                         RayStats& st, uint32_t& status) {
+// Inserts (t, p) into the warp k-buffer (lane i = i-th closest, ascending in
+// (t, particle index)).  Entries greater than the hit form a suffix.
+__device__ __forceinline__ void warp_insert(float& bt, uint32_t& bp, float t, uint32_t p, uint32_t lane) {
+  bool after = t < bt || (t == bt && p < bp);
+  uint32_t m = __ballot_sync(kFull, after);
+  if (m) {
+    int pos = __ffs(m) - 1;
+    float ut = __shfl_up_sync(kFull, bt, 1);
+    uint32_t up = __shfl_up_sync(kFull, bp, 1);
+    if ((int)lane > pos) {
+      bt = ut;
+      bp = up;
+    }
+    if ((int)lane == pos) {
+      bt = t;
+      bp = p;
+    }
+  }
+}
+
+// Modes of one traversal.
+enum TraverseMode { kCollect = 0, kClosestAny = 1, kCountFront = 2 };
+
+// Warp-cooperative traversal from the root with interval (tlo, t_max).
+//   kCollect:    the 32 closest front-face hits go into (bt, bp)
+//   kClosestAny: the closest hit of any facing goes into lane 0 of (bt, bp)
+//   kCountFront: every front-face hit is counted into *count
+// Far bound of the box tests: the buffer's last entry (kCollect), its first
+// entry (kClosestAny) or t_max (kCountFront).
+template <int MODE>
+__device__ __forceinline__ void traverse8(const SceneDev& S, const FaceTable& F, WarpScratch& W, V3 o, V3 d,
+                                          const BoxRay& br, float tlo, float t_max, float& bt, uint32_t& bp,
+                                          uint32_t* count, RayStats& st, uint32_t& status, uint32_t lane) {
   if (S.n_kept == 0) return;
-  uint32_t stack_node[kStackSize];
-  float stack_t[kStackSize];
-  int sp = 0;
-  uint32_t cur = S.root;
-  uint32_t visits = 0;
-  // a tree walk pops every internal node at most once
-  const uint32_t max_visits = S.n_kept + 64u;
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  const int cull_lane = MODE == kClosestAny ? 0 : 31;
+  int sp = 0, nq = 0;
+  if (lane == 0) {
+    W.snode[0] = 0;
+    W.st[0] = -CUDART_INF_F;
+  }
+  sp = 1;
+  __syncwarp();
+  float thi = MODE == kCountFront ? t_max : __shfl_sync(kFull, bt, cull_lane);
+  uint32_t iters = 0;
+  const uint32_t max_iters = 4u * S.n_kept + 64u;
   while (true) {
-    if (cur & kLeafBit) {
-      ++st.proxy_tests;
-      leaf(cur & ~kLeafBit, thi());
-    } else {
-      ++st.node_visits;
-      if (++visits > max_visits) {
-        status |= kStatusVisitCap;
-        return;
+    if (++iters > max_iters) {
+      status |= kStatusVisitCap;
+      return;
+    }
+    // pop up to 4 nodes still in range
+    uint32_t pn[4] = {0, 0, 0, 0};
+    int np = 0;
+    while (np < 4 && sp > 0) {
+      --sp;
+      float t = W.st[sp];
+      uint32_t n = W.snode[sp];
+      if (t <= thi) pn[np++] = n;
+    }
+    __syncwarp();
+    if (np > 0) {
+      const int slot = (int)(lane >> 3);
+      const bool valid = slot < np;
+      uint32_t node = slot == 0 ? pn[0] : slot == 1 ? pn[1] : slot == 2 ? pn[2] : pn[3];
+      float tnear = CUDART_INF_F;
+      uint32_t ref = kInvalid;
+      bool hit = false;
+      if (valid) {
+        const float4* rec = S.nodes8 + 16 * (size_t)node + 2 * (lane & 7);
+        float4 a = __ldg(rec), b = __ldg(rec + 1);
+        ref = __float_as_uint(b.z);
+        float x0 = __fmaf_rn(a.x, br.ix, -br.ox), x1 = __fmaf_rn(a.w, br.ix, -br.ox);
+        float y0 = __fmaf_rn(a.y, br.iy, -br.oy), y1 = __fmaf_rn(b.x, br.iy, -br.oy);
+        float z0 = __fmaf_rn(a.z, br.iz, -br.oz), z1 = __fmaf_rn(b.y, br.iz, -br.oz);
+        float tn = fmaxf(fmaxf(fminf(x0, x1) - br.px, fminf(y0, y1) - br.py), fmaxf(fminf(z0, z1) - br.pz, tlo));
+        float tf = fminf(fminf(fmaxf(x0, x1) + br.px, fmaxf(y0, y1) + br.py), fminf(fmaxf(z0, z1) + br.pz, thi));
+        hit = ref != kInvalid && tn <= tf;
+        tnear = tn;
       }
-      const float4* nd = S.nodes + 4 * (size_t)cur;
-      float4 f0 = __ldg(nd), f1 = __ldg(nd + 1), f2 = __ldg(nd + 2), f3 = __ldg(nd + 3);
-      float n0, n1;
-      bool h0, h1;
-      node_test(f0, f1, f2, br, tlo, thi(), n0, n1, h0, h1);
-      uint32_t c0 = __float_as_uint(f3.x), c1 = __float_as_uint(f3.y);
-      if (h0 && h1) {
-        bool swap = n1 < n0;
-        uint32_t nearc = swap ? c1 : c0, farc = swap ? c0 : c1;
-        float fart = swap ? n0 : n1;
-        if (sp >= kStackSize) {
+      st.node_visits += (lane & 7) == 0 && valid ? 1u : 0u;
+      const bool leaf = (ref & kLeafBit) != 0;
+      const uint32_t lmask = __ballot_sync(kFull, hit && leaf);
+      const uint32_t imask = __ballot_sync(kFull, hit && !leaf);
+      if (lmask) {
+        if (hit && leaf) {
+          int q = nq + __popc(lmask & lt_mask);
+          W.leafq[q] = ref & ~kLeafBit;
+          W.leaft[q] = tnear;
+        }
+        nq += __popc(lmask);
+      }
+      if (imask) {
+        const int m = __popc(imask);
+        if (sp + m > kWarpStack) {
           status |= kStatusStackOverflow;
           return;
         }
-        stack_node[sp] = farc;
-        stack_t[sp] = fart;
-        ++sp;
-        cur = nearc;
-        continue;
-      } else if (h0) {
-        cur = c0;
-        continue;
-      } else if (h1) {
-        cur = c1;
-        continue;
+        float key = (hit && !leaf) ? tnear : CUDART_INF_F;
+        uint32_t val = ref;
+        if (m > 1) warp_sort(key, val, lane);
+        else if (imask) {
+          int src = __ffs(imask) - 1;
+          key = __shfl_sync(kFull, key, src);
+          val = __shfl_sync(kFull, val, src);
+        }
+        if ((int)lane < m) {
+          W.snode[sp + m - 1 - (int)lane] = val;
+          W.st[sp + m - 1 - (int)lane] = key;
+        }
+        sp += m;
       }
+      __syncwarp();
     }
-    // pop the next entry that is still in range
-    bool found = false;
-    while (sp > 0) {
-      --sp;
-      if (stack_t[sp] <= thi()) {
-        cur = stack_node[sp];
-        found = true;
-        break;
+    const bool drain = sp == 0;
+    if (nq >= 32 || (drain && nq > 0)) {
+      const int nb = nq < 32 ? nq : 32;
+      uint32_t j = 0;
+      bool have = (int)lane < nb;
+      if (have) {
+        j = W.leafq[lane];
+        have = W.leaft[lane] <= thi;
       }
-    }
-    if (!found) return;
-  }
-}
-
-// (t, p) < (bt, bp) in the round order
-__device__ __forceinline__ bool hit_less(float t, uint32_t p, float bt, uint32_t bp) {
-  return t < bt || (t == bt && p < bp);
-}
-
-template <int KMAX>
-__device__ __forceinline__ void kinsert(float (&bt)[KMAX], uint32_t (&bp)[KMAX], float t, uint32_t p) {
+      __syncwarp();
+      if (nq > nb) {  // keep the rest (at most 31 entries) at the front of the queue
+        uint32_t qj = 0;
+        float qt = 0.f;
+        bool mv = (int)lane < nq - nb;
+        if (mv) {
+          qj = W.leafq[nb + lane];
+          qt = W.leaft[nb + lane];
+        }
+        __syncwarp();
+        if (mv) {
+          W.leafq[lane] = qj;
+          W.leaft[lane] = qt;
+        }
+        __syncwarp();
+      }
+      nq -= nb;
+      // one proxy per lane
+      float ht[kMaxHitsPerProxy];
+      int nh = 0;
+      if (have) {
+        ++st.proxy_tests;
+        const float tb = MODE == kCountFront ? t_max : fminf(next_up(thi), t_max);
+        proxy_test<MODE != kClosestAny>(F, S.w2o, j, o, d, tlo, tb, [&](float t, int) {
+          if (nh < kMaxHitsPerProxy) ht[nh] = t;
+          ++nh;
+        });
+        if (nh > kMaxHitsPerProxy) {
+          status |= kStatusHitOverflow;
+          nh = kMaxHitsPerProxy;
+        }
+      }
+      if (MODE == kCountFront) {
+        st.anyhits += nh;
+      } else {
+        uint32_t p = nh ? __ldg(S.leaf_pidx + j) : 0u;
+        st.anyhits += nh;
+        int hi = 0;
+        while (true) {
+          uint32_t pend = __ballot_sync(kFull, hi < nh);
+          if (!pend) break;
+          int src = __ffs(pend) - 1;
+          float myt = 0.f;
 #pragma unroll
-  for (int i = 0; i < KMAX; ++i) {
-    bool lt = hit_less(t, p, bt[i], bp[i]);
-    float t2 = lt ? bt[i] : t;
-    uint32_t p2 = lt ? bp[i] : p;
-    bt[i] = lt ? t : bt[i];
-    bp[i] = lt ? p : bp[i];
-    t = t2;
-    p = p2;
-  }
-}
-
-// next float above x: the far bound of the triangle test that still admits
-// a tie with the k-th hit
-__device__ __forceinline__ float next_up(float x) { return nextafterf(x, CUDART_INF_F); }
-
-// One round: the k closest front-face hits with t in (t_lo, t_max).
-template <int KMAX>
-__device__ __forceinline__ void collect_round(const SceneDev& S, const FaceTable& F, V3 o, V3 d, const BoxRay& br,
-                                              float t_lo, float t_max, float (&bt)[KMAX], uint32_t (&bp)[KMAX],
-                                              RayStats& st, uint32_t& status) {
-  auto thi = [&]() { return bt[KMAX - 1]; };
-  auto leaf = [&](uint32_t j, float far) {
-    float tb = fminf(next_up(far), t_max);
-    proxy_test<true>(F, S.w2o, j, o, d, t_lo, tb, [&](float t, int) {
-      ++st.anyhits;
-      uint32_t p = __ldg(S.leaf_pidx + j);
-      if (hit_less(t, p, bt[KMAX - 1], bp[KMAX - 1])) kinsert<KMAX>(bt, bp, t, p);
-    });
-  };
-  traverse(S, br, t_lo, thi, leaf, st, status);
-}
-
-struct NoRecord {
-  __device__ __forceinline__ void entry(uint32_t, uint32_t, float, float) {}
-};
-
-struct HitRecord {
-  uint32_t* pidx;
-  float* t;
-  float* alpha;
-  uint32_t max_entries;
-  __device__ __forceinline__ void entry(uint32_t n, uint32_t p, float tt, float a) {
-    if (n < max_entries) {
-      pidx[n] = p;
-      t[n] = tt;
-      alpha[n] = a;
+          for (int q = 0; q < kMaxHitsPerProxy; ++q)
+            if (q == hi) myt = ht[q];
+          float t = __shfl_sync(kFull, myt, src);
+          uint32_t pp = __shfl_sync(kFull, p, src);
+          if ((int)lane == src) ++hi;
+          warp_insert(bt, bp, t, pp, lane);
+        }
+        thi = __shfl_sync(kFull, bt, cull_lane);
+      }
     }
+    if (sp == 0 && nq == 0) break;
   }
-};
+}
 
-// Per-lane state of one primary ray between rounds.
-struct RayState {
+// Per-ray state (identical in all lanes).
+struct WRay {
   V3 o, d;
   BoxRay br;
   float L0, L1, L2, T, t_curr;
   uint32_t step, n_entries;
 };
 
-__device__ __forceinline__ void ray_init(const ViewDev& V, uint32_t px, uint32_t py, RayState& R) {
-  ray_gen(V.u, V.w, V.h, px, py, R.o, R.d);
-  R.br = make_boxray(R.o, R.d, V.s.scene_mag);
-  R.L0 = R.L1 = R.L2 = 0.0f;
-  R.T = 1.0f;
-  R.t_curr = V.u.t_min;
-  R.step = 0;
-  R.n_entries = 0;
-}
-
-// The loop condition of tracePath (src/GS_shader.ts:231-234): another round
-// starts while T_min < T and t_curr < t_max, unless earlyStop == step.
-__device__ __forceinline__ bool ray_more(const ViewDev& V, const RayState& R) {
+__device__ __forceinline__ bool wray_more(const ViewDev& V, const WRay& R) {
   return V.u.T_min < R.T && R.t_curr < V.u.t_max && V.u.early_stop != R.step;
 }
 
-// One round of tracePath (src/GS_shader.ts:235-269): collect the k closest
-// front-face hits beyond t_curr, advance t_curr, composite the entries.
-template <int KMAX, class Rec>
-__device__ __forceinline__ void ray_round(const ViewDev& V, const FaceTable& F, RayState& R, RayStats& st,
-                                          uint32_t& status, Rec& rec) {
+// tracePath (src/GS_shader.ts:192-273) for one pixel, by one warp.
+template <bool RECORD>
+__device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTable& F, WarpScratch& W, uint32_t px,
+                                                 uint32_t py, RayStats& st, uint32_t& status, uint32_t lane,
+                                                 const HitOut& ho, uint32_t slot) {
+  WRay R;
+  ray_gen(V.u, V.w, V.h, px, py, R.o, R.d);
+  R.br = make_boxray(R.o, R.d, V.s.scene_mag);
   const float t_max = V.u.t_max;
-  const int first = KMAX - (int)V.u.k;
-  ++R.step;
-  float bt[KMAX];
-  uint32_t bp[KMAX];
-#pragma unroll
-  for (int i = 0; i < KMAX; ++i) {
-    bt[i] = i < first ? -CUDART_INF_F : t_max;
-    bp[i] = i < first ? 0u : kInvalid;
-  }
-  collect_round<KMAX>(V.s, F, R.o, R.d, R.br, R.t_curr, t_max, bt, bp, st, status);
-  ++st.rounds;
-  R.t_curr = bt[KMAX - 1] + 1e-4f;
-#pragma unroll
-  for (int i = 0; i < KMAX; ++i) {
-    if (i < first) continue;
-    if (bp[i] == kInvalid) {
-      R.t_curr = t_max;
-      break;
-    }
-    uint32_t p = bp[i];
-    Shade sd = load_shade(V.s.shade, p);
-    float alpha = response(sd, R.o, R.d) * sd.opacity;
-    rec.entry(R.n_entries, p, bt[i], alpha);
-    ++R.n_entries;
-    ++st.entries;
-    if (V.u.alpha_min < alpha) {
-      ++st.contributing;
-      V3 dir = vnorm(vsub(sd.mu, R.o));
-      float c[3];
-      sh_radiance(V.s.sh, p, dir, V.u.deg, c);
-      float ta = R.T * alpha;
-      R.L0 = R.L0 + ta * (c[0] > 0.0f ? c[0] : 0.0f);
-      R.L1 = R.L1 + ta * (c[1] > 0.0f ? c[1] : 0.0f);
-      R.L2 = R.L2 + ta * (c[2] > 0.0f ? c[2] : 0.0f);
-      R.T = R.T * (1.0f - alpha);
-    }
-  }
-  if (R.step >= kMaxRounds && ray_more(V, R)) {
-    status |= kStatusRoundCap;
-    R.t_curr = t_max;
-  }
-}
-
-// tracePath (src/GS_shader.ts:192-273) for one pixel, all rounds.
-template <int KMAX, class Rec>
-__device__ __forceinline__ float4 trace_pixel(const ViewDev& V, const FaceTable& F, uint32_t px, uint32_t py,
-                                              RayStats& st, uint32_t& status, Rec& rec, uint32_t* n_entries_out) {
-  RayState R;
-  ray_init(V, px, py, R);
-  while (ray_more(V, R)) ray_round<KMAX>(V, F, R, st, status, rec);
-  if (n_entries_out) *n_entries_out = R.n_entries;
-  return make_float4(R.L0, R.L1, R.L2, 1.0f);
-}
-
-// Debug views (src/GS_shader.ts:201-228, 289-296, 312-321).
-//   mode 1: closest proxy hit of any facing, coloured by max(0, SH(ray dir));
-//   mode 2: number of front-face proxy hits in (t_min, t_max), bucketed.
-__device__ __forceinline__ float4 trace_debug(const ViewDev& V, const FaceTable& F, uint32_t px, uint32_t py,
-                                              RayStats& st, uint32_t& status, uint32_t* count_out) {
-  V3 o, d;
-  ray_gen(V.u, V.w, V.h, px, py, o, d);
-  BoxRay br = make_boxray(o, d, V.s.scene_mag);
-  const float t_max = V.u.t_max;
-  if (V.u.debug == 1) {
+  if (V.u.debug != 0) {
     float bt = t_max;
     uint32_t bp = kInvalid;
-    auto thi = [&]() { return bt; };
-    auto leaf = [&](uint32_t j, float far) {
-      float tb = bp == kInvalid ? t_max : fminf(next_up(far), t_max);
-      proxy_test<false>(F, V.s.w2o, j, o, d, V.u.t_min, tb, [&](float t, int) {
-        ++st.anyhits;
-        uint32_t p = __ldg(V.s.leaf_pidx + j);
-        if (hit_less(t, p, bt, bp)) {
-          bt = t;
-          bp = p;
+    uint32_t cnt = 0;
+    if (V.u.debug == 1) {
+      traverse8<kClosestAny>(V.s, F, W, R.o, R.d, R.br, V.u.t_min, t_max, bt, bp, nullptr, st, status, lane);
+      float4 out = make_float4(0.f, 0.f, 0.f, 1.f);
+      uint32_t p0 = __shfl_sync(kFull, bp, 0);
+      if (p0 != kInvalid) {
+        float c[3];
+        sh_radiance(V.s.sh, p0, R.d, V.u.deg, c);
+        out = make_float4(c[0] > 0.f ? c[0] : 0.f, c[1] > 0.f ? c[1] : 0.f, c[2] > 0.f ? c[2] : 0.f, 1.f);
+        cnt = 1;
+      }
+      if (RECORD && lane == 0) {
+        ho.count[slot] = cnt;
+        ho.rounds[slot] = 0;
+      }
+      return out;
+    }
+    // kCountFront: per-lane counts, reduced
+    uint32_t before = st.anyhits;
+    traverse8<kCountFront>(V.s, F, W, R.o, R.d, R.br, V.u.t_min, t_max, bt, bp, nullptr, st, status, lane);
+    cnt = __reduce_add_sync(kFull, st.anyhits - before);
+    float r = 0.f, g = 0.f, b = 0.f;
+    if (cnt == 0) {
+    } else if (cnt < 20) { r = 0.5f; g = 0.5f; }
+    else if (cnt < 40) { r = 0.5f; b = 0.5f; }
+    else if (cnt < 60) { g = 0.5f; b = 0.5f; }
+    else if (cnt < 80) { r = 0.5f; }
+    else if (cnt < 100) { g = 0.5f; }
+    else if (cnt < 150) { b = 0.5f; }
+    else { r = 0.5f; g = 0.5f; b = 0.5f; }
+    if (RECORD && lane == 0) {
+      ho.count[slot] = cnt;
+      ho.rounds[slot] = 0;
+    }
+    return make_float4(r, g, b, 1.f);
+  }
+  R.L0 = R.L1 = R.L2 = 0.f;
+  R.T = 1.f;
+  R.t_curr = V.u.t_min;
+  R.step = 0;
+  R.n_entries = 0;
+  const uint32_t k = V.u.k;
+  while (wray_more(V, R)) {
+    // one traversal: the 32 closest front-face hits with t > t_curr
+    float bt = t_max;
+    uint32_t bp = kInvalid;
+    traverse8<kCollect>(V.s, F, W, R.o, R.d, R.br, R.t_curr, t_max, bt, bp, nullptr, st, status, lane);
+    if (status & (kStatusStackOverflow | kStatusVisitCap | kStatusHitOverflow)) {
+      status = __reduce_or_sync(kFull, status);
+      break;
+    }
+    const uint32_t cnt = __popc(__ballot_sync(kFull, bp != kInvalid));
+    const bool complete = cnt < 32u;
+    // rounds served from this buffer
+    while (wray_more(V, R)) {
+      const uint32_t skip = __popc(__ballot_sync(kFull, bp != kInvalid && !(bt > R.t_curr)));
+      const uint32_t avail = cnt - skip;
+      if (!complete && avail < k) break;  // the next round reaches past the buffer
+      ++R.step;
+      st.rounds += lane == 0 ? 1u : 0u;
+      const uint32_t n = avail < k ? avail : k;
+      float new_t = n == k ? __shfl_sync(kFull, bt, (int)(skip + k - 1)) + 1e-4f : t_max;
+      // lanes skip..skip+n-1 hold this round's entries
+      const bool mine = lane >= skip && lane < skip + n;
+      float alpha = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
+      bool contrib = false;
+      if (mine) {
+        Shade sd = load_shade(V.s.shade, bp);
+        alpha = response(sd, R.o, R.d) * sd.opacity;
+        contrib = V.u.alpha_min < alpha;
+        if (contrib) {
+          V3 dir = vnorm(vsub(sd.mu, R.o));
+          float c[3];
+          sh_radiance(V.s.sh, bp, dir, V.u.deg, c);
+          c0 = c[0] > 0.f ? c[0] : 0.f;
+          c1 = c[1] > 0.f ? c[1] : 0.f;
+          c2 = c[2] > 0.f ? c[2] : 0.f;
         }
-      });
-    };
-    traverse(V.s, br, V.u.t_min, thi, leaf, st, status);
-    if (count_out) *count_out = bp == kInvalid ? 0u : 1u;
-    if (bp == kInvalid) return make_float4(0.f, 0.f, 0.f, 1.f);
-    float c[3];
-    sh_radiance(V.s.sh, bp, d, V.u.deg, c);
-    return make_float4(c[0] > 0.f ? c[0] : 0.f, c[1] > 0.f ? c[1] : 0.f, c[2] > 0.f ? c[2] : 0.f, 1.f);
-  }
-  uint32_t count = 0;
-  auto thi = [&]() { return t_max; };
-  auto leaf = [&](uint32_t j, float) {
-    proxy_test<true>(F, V.s.w2o, j, o, d, V.u.t_min, t_max, [&](float, int) { ++count; });
-  };
-  traverse(V.s, br, V.u.t_min, thi, leaf, st, status);
-  st.anyhits += count;
-  if (count_out) *count_out = count;
-  float r = 0.f, g = 0.f, b = 0.f;
-  if (count == 0) {
-  } else if (count < 20) { r = 0.5f; g = 0.5f; }
-  else if (count < 40) { r = 0.5f; b = 0.5f; }
-  else if (count < 60) { g = 0.5f; b = 0.5f; }
-  else if (count < 80) { r = 0.5f; }
-  else if (count < 100) { g = 0.5f; }
-  else if (count < 150) { b = 0.5f; }
-  else { r = 0.5f; g = 0.5f; b = 0.5f; }
-  return make_float4(r, g, b, 1.f);
-}
-
-__device__ __forceinline__ void flush_stats(DevCounters* ctr, RayStats& st, uint32_t rays, uint32_t status) {
-  unsigned long long v[7] = {rays, st.rounds, st.entries, st.contributing, st.proxy_tests, st.node_visits, st.anyhits};
-#pragma unroll
-  for (int i = 0; i < 7; ++i) {
-    unsigned long long x = v[i];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xFFFFFFFFu, x, off);
-    v[i] = x;
-  }
-  uint32_t s = __reduce_or_sync(0xFFFFFFFFu, status);
-  if ((threadIdx.x & 31) == 0) {
-    atomicAdd(&ctr->rays, v[0]);
-    atomicAdd(&ctr->rounds, v[1]);
-    atomicAdd(&ctr->entries, v[2]);
-    atomicAdd(&ctr->contributing, v[3]);
-    atomicAdd(&ctr->proxy_tests, v[4]);
-    atomicAdd(&ctr->node_visits, v[5]);
-    atomicAdd(&ctr->anyhits, v[6]);
-    if (s) atomicOr(&ctr->status, s);
-  }
-}
-
-__device__ __forceinline__ uint32_t find_view(const ViewDev* views, uint32_t n_views, uint32_t tile) {
-  uint32_t lo = 0, hi = n_views - 1;
-  while (lo < hi) {
-    uint32_t mid = (lo + hi + 1) >> 1;
-    if (views[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
-
-// Persistent trace kernel over all pixels of all views.  Work items are
-// pixel slots: slot = 32 * tile + lane-in-tile, tiles of 8x4 pixels in
-// row-major order per view, views back to back.  A lane whose ray is done
-// takes the next slot at once (warp-aggregated atomic), so rays of very
-// different length do not hold whole warps idle.
-template <int KMAX>
-__global__ void __launch_bounds__(128) k_trace(const ViewDev* __restrict__ views, uint32_t n_views,
-                                               uint32_t total_tiles, DevCounters* ctr,
-                                               const __grid_constant__ FaceTable F) {
-  const uint32_t lane = threadIdx.x & 31;
-  const uint32_t lt_mask = (1u << lane) - 1u;
-  const uint32_t total_slots = total_tiles * 32u;
-  RayStats st = {0, 0, 0, 0, 0, 0};
-  uint32_t status = 0, rays = 0;
-  NoRecord rec;
-  bool active = false, exhausted = false;
-  uint32_t vi = 0, px = 0, py = 0;
-  RayState R;
-  while (true) {
-    bool want = !active && !exhausted;
-    uint32_t need = __ballot_sync(0xFFFFFFFFu, want);
-    while (need) {
-      int leader = __ffs(need) - 1;
-      uint32_t base = 0;
-      if ((int)lane == leader) base = atomicAdd(&ctr->work, (uint32_t)__popc(need));
-      base = __shfl_sync(0xFFFFFFFFu, base, leader);
-      if (want) {
-        uint32_t slot = base + __popc(need & lt_mask);
-        if (slot >= total_slots || slot < base) {
-          exhausted = true;
-          want = false;
-        } else {
-          uint32_t tile = slot >> 5, s = slot & 31u;
-          vi = n_views == 1 ? 0u : find_view(views, n_views, tile);
-          const ViewDev& V = views[vi];
-          uint32_t lt = tile - V.tile_begin;
-          px = (lt % V.tiles_x) * kTileW + (s % kTileW);
-          py = (lt / V.tiles_x) * kTileH + (s / kTileW);
-          if (px < V.w && py < V.h) {
-            want = false;
-            if (V.u.debug == 0) {
-              ray_init(V, px, py, R);
-              active = ray_more(V, R);
-              if (!active) {  // no round at all: black pixel
-                V.out[(size_t)py * V.w + px] = make_float4(0.f, 0.f, 0.f, 1.f);
-                ++rays;
-              }
-            } else {
-              V.out[(size_t)py * V.w + px] = trace_debug(V, F, px, py, st, status, nullptr);
-              ++rays;
-            }
+        if (RECORD) {
+          uint32_t e = R.n_entries + (lane - skip);
+          if (e < ho.max_entries) {
+            size_t at = (size_t)slot * ho.max_entries + e;
+            ho.pidx[at] = bp;
+            ho.t[at] = bt;
+            ho.alpha[at] = alpha;
           }
         }
       }
-      need = __ballot_sync(0xFFFFFFFFu, want);
-    }
-    if (!__any_sync(0xFFFFFFFFu, active)) break;
-    if (active) {
-      const ViewDev& V = views[vi];
-      ray_round<KMAX>(V, F, R, st, status, rec);
-      if (!ray_more(V, R)) {
-        V.out[(size_t)py * V.w + px] = make_float4(R.L0, R.L1, R.L2, 1.0f);
-        ++rays;
-        active = false;
+      const uint32_t cmask = __ballot_sync(kFull, contrib);
+      st.entries += lane == 0 ? n : 0u;
+      st.contributing += lane == 0 ? __popc(cmask) : 0u;
+      // front-to-back accumulation in entry order
+      for (uint32_t e = 0; e < n; ++e) {
+        const int src = (int)(skip + e);
+        float a = __shfl_sync(kFull, alpha, src);
+        float x0 = __shfl_sync(kFull, c0, src);
+        float x1 = __shfl_sync(kFull, c1, src);
+        float x2 = __shfl_sync(kFull, c2, src);
+        if ((cmask >> src) & 1u) {
+          float ta = R.T * a;
+          R.L0 = R.L0 + ta * x0;
+          R.L1 = R.L1 + ta * x1;
+          R.L2 = R.L2 + ta * x2;
+          R.T = R.T * (1.0f - a);
+        }
+      }
+      R.n_entries += n;
+      R.t_curr = new_t;
+      if (R.step >= kMaxRounds && wray_more(V, R)) {
+        status |= kStatusRoundCap;
+        R.t_curr = t_max;
       }
     }
   }
-  flush_stats(ctr, st, rays, status);
+  if (RECORD && lane == 0) {
+    ho.count[slot] = R.n_entries;
+    ho.rounds[slot] = R.step;
+  }
+  return make_float4(R.L0, R.L1, R.L2, 1.0f);
 }
 
-// Hit-list recording for listed pixels (parity and inspection).
-template <int KMAX>
-__global__ void __launch_bounds__(128) k_trace_hits(const ViewDev V, const uint32_t* pixels, uint32_t n_pix,
-                                                    uint32_t max_entries, uint32_t* out_pidx, float* out_t,
-                                                    float* out_alpha, uint32_t* out_count, uint32_t* out_rounds,
-                                                    float4* out_rgba, DevCounters* ctr,
-                                                    const __grid_constant__ FaceTable F) {
-  uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+// Persistent kernel: each warp takes one pixel slot at a time from a global
+// counter (slot = 32 * tile + position in the 8x4 tile, views back to back),
+// so neighbouring pixels run on neighbouring warps at the same time.
+template <bool RECORD>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_trace8(const ViewDev* __restrict__ views, uint32_t n_views,
+                                                                  uint32_t total_tiles, DevCounters* ctr,
+                                                                  const __grid_constant__ FaceTable F,
+                                                                  const uint32_t* pixels, uint32_t n_pix,
+                                                                  const HitOut ho) {
+  __shared__ WarpScratch scratch[kWarpsPerBlock];
+  const uint32_t lane = threadIdx.x & 31;
+  WarpScratch& W = scratch[threadIdx.x >> 5];
   RayStats st = {0, 0, 0, 0, 0, 0};
   uint32_t status = 0, rays = 0;
-  if (q < n_pix) {
-    uint32_t pix = pixels[q];
-    if (pix < V.w * V.h) {
-      HitRecord rec{out_pidx + (size_t)q * max_entries, out_t + (size_t)q * max_entries,
-                    out_alpha + (size_t)q * max_entries, max_entries};
-      uint32_t n = 0;
-      float4 r = V.u.debug == 0 ? trace_pixel<KMAX>(V, F, pix % V.w, pix / V.w, st, status, rec, &n)
-                                : trace_debug(V, F, pix % V.w, pix / V.w, st, status, &n);
-      out_count[q] = n;
-      out_rounds[q] = st.rounds;
-      if (out_rgba) out_rgba[q] = r;
-      rays = 1;
+  const uint32_t total = RECORD ? n_pix : total_tiles * 32u;
+  while (true) {
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(&ctr->work, 1u);
+    item = __shfl_sync(kFull, item, 0);
+    if (item >= total) break;
+    uint32_t vi = 0, px, py;
+    if (RECORD) {
+      uint32_t pix = pixels[item];
+      const ViewDev& V = views[0];
+      if (pix >= V.w * V.h) continue;
+      px = pix % V.w;
+      py = pix / V.w;
+    } else {
+      uint32_t tile = item >> 5, s = item & 31u;
+      vi = n_views == 1 ? 0u : find_view(views, n_views, tile);
+      const ViewDev& V = views[vi];
+      uint32_t lt = tile - V.tile_begin;
+      px = (lt % V.tiles_x) * kTileW + (s % kTileW);
+      py = (lt / V.tiles_x) * kTileH + (s / kTileW);
+      if (px >= V.w || py >= V.h) continue;
+    }
+    const ViewDev& V = views[vi];
+    float4 r = trace_ray_warp<RECORD>(V, F, W, px, py, st, status, lane, ho, item);
+    if (lane == 0) {
+      if (RECORD) {
+        if (ho.rgba) ho.rgba[item] = r;
+      } else {
+        V.out[(size_t)py * V.w + px] = r;
+      }
+      ++rays;
     }
   }
   flush_stats(ctr, st, rays, status);
@@ -553,43 +452,30 @@ __global__ void __launch_bounds__(128) k_trace_hits(const ViewDev V, const uint3
 uint32_t kmax_for(uint32_t k) { return k <= 8 ? 8u : (k <= 16 ? 16u : 32u); }
 
 Err launch_trace(const ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
-                 const FaceTable& faces, const LaunchShape& shape, int num_sms, cudaStream_t stream, uint64_t* launches,
-                 ViewDev* d_views) {
-  uint32_t kmax = 8;
-  for (uint32_t v = 0; v < n_views; ++v) kmax = kmax_for(std::max(kmax, views[v].u.k));
+                  const FaceTable& faces, const LaunchShape& shape, int num_sms, cudaStream_t stream,
+                  uint64_t* launches, ViewDev* d_views) {
   GT_CUDA_TRY(cudaMemcpyAsync(d_views, views, sizeof(ViewDev) * n_views, cudaMemcpyHostToDevice, stream));
-  uint32_t warps_needed = total_tiles;
-  uint32_t block = 128;
+  uint32_t block = kWarpsPerBlock * 32;
   uint32_t grid = (uint32_t)num_sms * std::max(1u, shape.blocks_per_sm);
-  uint32_t max_grid = (warps_needed + (block / 32) - 1) / (block / 32);
-  if (grid > max_grid) grid = std::max(1u, max_grid);
-  if (kmax == 8)
-    k_trace<8><<<grid, block, 0, stream>>>(d_views, n_views, total_tiles, counters, faces);
-  else if (kmax == 16)
-    k_trace<16><<<grid, block, 0, stream>>>(d_views, n_views, total_tiles, counters, faces);
-  else
-    k_trace<32><<<grid, block, 0, stream>>>(d_views, n_views, total_tiles, counters, faces);
+  uint64_t warps_needed = (uint64_t)total_tiles * 32u;
+  uint64_t max_grid = (warps_needed + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  if (grid > max_grid) grid = (uint32_t)std::max<uint64_t>(1, max_grid);
+  HitOut ho{};
+  k_trace8<false><<<grid, block, 0, stream>>>(d_views, n_views, total_tiles, counters, faces, nullptr, 0u, ho);
   ++*launches;
   GT_CUDA_TRY(cudaGetLastError());
   return Err{};
 }
 
-Err launch_trace_hits(const ViewDev& view, const uint32_t* pixels, uint32_t n_pix, uint32_t max_entries,
-                      uint32_t* out_pidx, float* out_t, float* out_alpha, uint32_t* out_count, uint32_t* out_rounds,
-                      float4* out_rgba, DevCounters* counters, const FaceTable& faces, cudaStream_t stream,
-                      uint64_t* launches) {
-  uint32_t kmax = kmax_for(view.u.k);
-  uint32_t grid = (n_pix + 127) / 128;
-  if (grid == 0) return Err{};
-  if (kmax == 8)
-    k_trace_hits<8><<<grid, 128, 0, stream>>>(view, pixels, n_pix, max_entries, out_pidx, out_t, out_alpha, out_count,
-                                              out_rounds, out_rgba, counters, faces);
-  else if (kmax == 16)
-    k_trace_hits<16><<<grid, 128, 0, stream>>>(view, pixels, n_pix, max_entries, out_pidx, out_t, out_alpha,
-                                               out_count, out_rounds, out_rgba, counters, faces);
-  else
-    k_trace_hits<32><<<grid, 128, 0, stream>>>(view, pixels, n_pix, max_entries, out_pidx, out_t, out_alpha,
-                                               out_count, out_rounds, out_rgba, counters, faces);
+Err launch_trace_hits(const ViewDev& view, ViewDev* d_views, const uint32_t* pixels, uint32_t n_pix,
+                      uint32_t max_entries, uint32_t* out_pidx, float* out_t, float* out_alpha, uint32_t* out_count,
+                      uint32_t* out_rounds, float4* out_rgba, DevCounters* counters, const FaceTable& faces,
+                      cudaStream_t stream, uint64_t* launches) {
+  if (n_pix == 0) return Err{};
+  GT_CUDA_TRY(cudaMemcpyAsync(d_views, &view, sizeof(ViewDev), cudaMemcpyHostToDevice, stream));
+  HitOut ho{out_pidx, out_t, out_alpha, out_count, out_rounds, out_rgba, max_entries};
+  uint32_t grid = std::min<uint32_t>((n_pix + kWarpsPerBlock - 1) / kWarpsPerBlock, 148u * 8u);
+  k_trace8<true><<<grid, kWarpsPerBlock * 32, 0, stream>>>(d_views, 1, 0, counters, faces, pixels, n_pix, ho);
   ++*launches;
   GT_CUDA_TRY(cudaGetLastError());
   return Err{};

@@ -1,0 +1,179 @@
+// gt_trace_common.cuh — pieces shared by the trace kernels: per-ray
+// statistics, the box-test ray, the exact ray/proxy test and work helpers.
+#pragma once
+
+#include <math_constants.h>
+
+#include "gt_device.cuh"
+#include "gt_internal.cuh"
+
+namespace gt {
+
+constexpr int kTileW = 8, kTileH = 4;
+
+struct RayStats {
+  uint32_t rounds, entries, contributing, proxy_tests, node_visits, anyhits;
+};
+
+// Box-test state of a ray: inverse direction, origin times inverse direction
+// and, per axis, a padding of the slab planes that covers the rounding of
+// the object-space triangle test (hit points lie within ~1e-6 relative of
+// |origin| + scene size of the true surface).
+struct BoxRay {
+  float ix, iy, iz, ox, oy, oz, px, py, pz;
+};
+
+__device__ __forceinline__ float safe_inv(float d) {
+  float a = fabsf(d) < 1e-30f ? copysignf(1e-30f, d) : d;
+  return __frcp_rn(a);
+}
+
+__device__ __forceinline__ BoxRay make_boxray(V3 o, V3 d, float scene_mag) {
+  BoxRay b;
+  b.ix = safe_inv(d.x);
+  b.iy = safe_inv(d.y);
+  b.iz = safe_inv(d.z);
+  b.ox = o.x * b.ix;
+  b.oy = o.y * b.iy;
+  b.oz = o.z * b.iz;
+  float m = fmaxf(fmaxf(fabsf(o.x), fabsf(o.y)), fabsf(o.z));
+  float pad = 4e-6f * (m + scene_mag) + 1e-7f;
+  b.px = pad * fabsf(b.ix);
+  b.py = pad * fabsf(b.iy);
+  b.pz = pad * fabsf(b.iz);
+  return b;
+}
+
+// Slab test of the two children of a node against [tlo, thi].
+__device__ __forceinline__ void node_test(const float4& f0, const float4& f1, const float4& f2, const BoxRay& r,
+                                          float tlo, float thi, float& n0, float& n1, bool& h0, bool& h1) {
+  float ax = __fmaf_rn(f0.x, r.ix, -r.ox), bx = __fmaf_rn(f0.y, r.ix, -r.ox);
+  float ay = __fmaf_rn(f0.z, r.iy, -r.oy), by = __fmaf_rn(f0.w, r.iy, -r.oy);
+  float az = __fmaf_rn(f2.x, r.iz, -r.oz), bz = __fmaf_rn(f2.y, r.iz, -r.oz);
+  n0 = fmaxf(fmaxf(fminf(ax, bx) - r.px, fminf(ay, by) - r.py), fmaxf(fminf(az, bz) - r.pz, tlo));
+  float x0 = fminf(fminf(fmaxf(ax, bx) + r.px, fmaxf(ay, by) + r.py), fminf(fmaxf(az, bz) + r.pz, thi));
+  h0 = n0 <= x0;
+  float cx = __fmaf_rn(f1.x, r.ix, -r.ox), dx = __fmaf_rn(f1.y, r.ix, -r.ox);
+  float cy = __fmaf_rn(f1.z, r.iy, -r.oy), dy = __fmaf_rn(f1.w, r.iy, -r.oy);
+  float cz = __fmaf_rn(f2.z, r.iz, -r.oz), dz = __fmaf_rn(f2.w, r.iz, -r.oz);
+  n1 = fmaxf(fmaxf(fminf(cx, dx) - r.px, fminf(cy, dy) - r.py), fmaxf(fminf(cz, dz) - r.pz, tlo));
+  float x1 = fminf(fminf(fmaxf(cx, dx) + r.px, fmaxf(cy, dy) + r.py), fminf(fmaxf(cz, dz) + r.pz, thi));
+  h1 = n1 <= x1;
+}
+
+// Ray/proxy test.  Calls on_hit(t, face) for every face hit by the reference
+// triangle test with t in (tlo, thi) that is front-facing (CULL) or any
+// (!CULL).  Three exact filters run before that test; each skips only work
+// whose outcome is already known:
+//   * bounding sphere: every triangle lies inside the circumsphere, and the
+//     triangle test cannot report a point farther than its rounding error
+//     (covered by the 1e-3 + 1e-5 |o_obj| margin) from its triangle;
+//   * facing: dot(n, d_obj) and the reference's world-space facing product
+//     both approximate n^T W2O d within tau = 1e-5 * nmax * sum(|W2O||d|), so
+//     a face whose dot(n, d_obj) exceeds tau is back-facing.  Faces come in
+//     antipodal pairs with n_b == -n_a bit for bit, so dot(n_b, d) ==
+//     -dot(n_a, d) exactly and one dot product serves both;
+//   * t range: the triangle test's t times dn lies within
+//     E = 10 u nmax (|p0|_1 + |o|_1) of num = n.p0 - n.o (u = 2^-24), so a
+//     face with num >= tlo*dn + M or num <= thi*dn - M (dn < 0) has its t
+//     outside (tlo, thi); M = 3e-5 nmax (|o|_1 + 2) + 1e-6 (|tlo|+|thi|)|dn|
+//     is ~50x that error.
+template <bool CULL, class OnHit>
+__device__ __forceinline__ void proxy_test(const FaceTable& F, const float4* w2o, uint32_t j, V3 o, V3 d, float tlo,
+                                           float thi, OnHit&& on_hit) {
+  Affine W = load_affine(w2o + 3 * (size_t)j);
+  V3 oo = xpoint(W, o), od = xdir(W, d);
+  float l1o = fabsf(oo.x) + fabsf(oo.y) + fabsf(oo.z);
+  {
+    float dd = __fmaf_rn(od.x, od.x, __fmaf_rn(od.y, od.y, od.z * od.z));
+    float ox = __fmaf_rn(oo.x, od.x, __fmaf_rn(oo.y, od.y, oo.z * od.z));
+    float tc = -__fdividef(ox, dd);
+    float cx = __fmaf_rn(tc, od.x, oo.x), cy = __fmaf_rn(tc, od.y, oo.y), cz = __fmaf_rn(tc, od.z, oo.z);
+    float r2 = __fmaf_rn(cx, cx, __fmaf_rn(cy, cy, cz * cz));
+    float rp = __fmaf_rn(1e-5f, l1o, F.r_circ + 1e-3f);
+    if (!(r2 <= rp * rp)) {
+      if (dd == dd && r2 == r2) return;  // NaN falls through to the exact test
+    }
+  }
+  if (!CULL) {
+#pragma unroll 1
+    for (int f = 0; f < 20; ++f) {
+      float dn = vdot(mk(F.n[f][0], F.n[f][1], F.n[f][2]), od);
+      float t;
+      if (tri_test(F, f, oo, tlo, od, thi, dn, t)) on_hit(t, f);
+    }
+    return;
+  }
+  const float* m = W.m;
+  float s = fabsf(d.x) * (fabsf(m[0]) + fabsf(m[1]) + fabsf(m[2])) +
+            fabsf(d.y) * (fabsf(m[3]) + fabsf(m[4]) + fabsf(m[5])) +
+            fabsf(d.z) * (fabsf(m[6]) + fabsf(m[7]) + fabsf(m[8]));
+  const float tau = 1e-5f * F.nmax * s;
+  const float mbase = 3e-5f * F.nmax * (l1o + 2.0f);
+  const float trange = 1e-6f * (fabsf(tlo) + fminf(fabsf(thi), 1e30f));
+  // rolled on purpose: one copy of the triangle test and of the caller's
+  // k-buffer insertion keeps the kernel small enough for the instruction cache
+#pragma unroll 1
+  for (int pair = 0; pair < 10; ++pair) {
+    const int fa = F.pa[pair];
+    const V3 na = mk(F.n[fa][0], F.n[fa][1], F.n[fa][2]);
+    const float dna = vdot(na, od);
+    if (fabsf(dna) > tau) {
+      // exactly one face of the pair can face the ray
+      const int f = dna < 0.0f ? fa : F.pb[pair];
+      const float dn = dna < 0.0f ? dna : -dna;
+      const float no = __fmaf_rn(na.x, oo.x, __fmaf_rn(na.y, oo.y, na.z * oo.z));
+      const float num = F.c[f] - (dna < 0.0f ? no : -no);
+      const float mg = __fmaf_rn(trange, fabsf(dn), mbase);
+      if (num >= __fmaf_rn(tlo, dn, mg) || num <= __fmaf_rn(thi, dn, -mg)) continue;
+      float t;
+      if (tri_test(F, f, oo, tlo, od, thi, dn, t) && front_facing(F, f, W, d)) on_hit(t, f);
+    } else {
+      // grazing pair: both faces go to the exact test
+#pragma unroll 1
+      for (int c = 0; c < 2; ++c) {
+        const int f = c ? F.pb[pair] : fa;
+        const float dn = c ? -dna : dna;
+        float t;
+        if (tri_test(F, f, oo, tlo, od, thi, dn, t) && front_facing(F, f, W, d)) on_hit(t, f);
+      }
+    }
+  }
+}
+
+// next float above x: the far bound of the triangle test that still admits
+// a tie with the k-th hit
+__device__ __forceinline__ float next_up(float x) { return nextafterf(x, CUDART_INF_F); }
+
+__device__ __forceinline__ void flush_stats(DevCounters* ctr, RayStats& st, uint32_t rays, uint32_t status) {
+  unsigned long long v[7] = {rays, st.rounds, st.entries, st.contributing, st.proxy_tests, st.node_visits, st.anyhits};
+#pragma unroll
+  for (int i = 0; i < 7; ++i) {
+    unsigned long long x = v[i];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xFFFFFFFFu, x, off);
+    v[i] = x;
+  }
+  uint32_t s = __reduce_or_sync(0xFFFFFFFFu, status);
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&ctr->rays, v[0]);
+    atomicAdd(&ctr->rounds, v[1]);
+    atomicAdd(&ctr->entries, v[2]);
+    atomicAdd(&ctr->contributing, v[3]);
+    atomicAdd(&ctr->proxy_tests, v[4]);
+    atomicAdd(&ctr->node_visits, v[5]);
+    atomicAdd(&ctr->anyhits, v[6]);
+    if (s) atomicOr(&ctr->status, s);
+  }
+}
+
+__device__ __forceinline__ uint32_t find_view(const ViewDev* views, uint32_t n_views, uint32_t tile) {
+  uint32_t lo = 0, hi = n_views - 1;
+  while (lo < hi) {
+    uint32_t mid = (lo + hi + 1) >> 1;
+    if (views[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+}  // namespace gt
