@@ -73,6 +73,28 @@ __device__ __forceinline__ void warp_sort(float& key, uint32_t& val, uint32_t la
   }
 }
 
+// Sorts lanes [0, w) ascending by key, w = the power of two >= m (m <= 32);
+// keys of lanes >= m are +inf.
+__device__ __forceinline__ void warp_sort_prefix(float& key, uint32_t& val, uint32_t lane, int m) {
+  const int w = m <= 2 ? 2 : m <= 4 ? 4 : m <= 8 ? 8 : m <= 16 ? 16 : 32;
+#pragma unroll
+  for (int k = 2; k <= 32; k <<= 1) {
+    if (k > w) break;
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      float ok = __shfl_xor_sync(kFull, key, j);
+      uint32_t ov = __shfl_xor_sync(kFull, val, j);
+      bool up = (lane & k) == 0;
+      bool lower = (lane & j) == 0;
+      bool take = (lower == up) ? (ok < key) : (ok > key);
+      if (take) {
+        key = ok;
+        val = ov;
+      }
+    }
+  }
+}
+
 // Inserts (t, p) into the warp k-buffer (lane i = i-th closest, ascending in
 // (t, particle index)).  Entries greater than the hit form a suffix.
 __device__ __forceinline__ void warp_insert(float& bt, uint32_t& bp, float t, uint32_t p, uint32_t lane) {
@@ -124,20 +146,26 @@ __device__ __forceinline__ void traverse8(const SceneDev& S, const FaceTable& F,
       status |= kStatusVisitCap;
       return;
     }
-    // pop up to 4 nodes still in range
-    uint32_t pn[4] = {0, 0, 0, 0};
+    // pop up to 4 nodes still in range (kept in registers: no indexed array)
+    uint32_t pn0 = 0, pn1 = 0, pn2 = 0, pn3 = 0;
     int np = 0;
     while (np < 4 && sp > 0) {
       --sp;
       float t = W.st[sp];
       uint32_t n = W.snode[sp];
-      if (t <= thi) pn[np++] = n;
+      if (t <= thi) {
+        pn3 = pn2;
+        pn2 = pn1;
+        pn1 = pn0;
+        pn0 = n;
+        ++np;
+      }
     }
     __syncwarp();
     if (np > 0) {
       const int slot = (int)(lane >> 3);
       const bool valid = slot < np;
-      uint32_t node = slot == 0 ? pn[0] : slot == 1 ? pn[1] : slot == 2 ? pn[2] : pn[3];
+      uint32_t node = slot == 0 ? pn0 : slot == 1 ? pn1 : slot == 2 ? pn2 : pn3;
       float tnear = CUDART_INF_F;
       uint32_t ref = kInvalid;
       bool hit = false;
@@ -171,14 +199,12 @@ __device__ __forceinline__ void traverse8(const SceneDev& S, const FaceTable& F,
           status |= kStatusStackOverflow;
           return;
         }
-        float key = (hit && !leaf) ? tnear : CUDART_INF_F;
-        uint32_t val = ref;
-        if (m > 1) warp_sort(key, val, lane);
-        else if (imask) {
-          int src = __ffs(imask) - 1;
-          key = __shfl_sync(kFull, key, src);
-          val = __shfl_sync(kFull, val, src);
-        }
+        // gather the m hit children into lanes 0..m-1, then sort that segment
+        const uint32_t src = (int)lane < m ? __fns(imask, 0, (int)lane + 1) : lane;
+        float key = __shfl_sync(kFull, tnear, src);
+        uint32_t val = __shfl_sync(kFull, ref, src);
+        if ((int)lane >= m) key = CUDART_INF_F;
+        if (m > 1) warp_sort_prefix(key, val, lane, m);
         if ((int)lane < m) {
           W.snode[sp + m - 1 - (int)lane] = val;
           W.st[sp + m - 1 - (int)lane] = key;
@@ -213,14 +239,19 @@ __device__ __forceinline__ void traverse8(const SceneDev& S, const FaceTable& F,
         __syncwarp();
       }
       nq -= nb;
-      // one proxy per lane
-      float ht[kMaxHitsPerProxy];
+      // one proxy per lane; its hits are kept in a register queue h0..h5
+      float h0 = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, h4 = 0.f, h5 = 0.f;
       int nh = 0;
       if (have) {
         ++st.proxy_tests;
         const float tb = MODE == kCountFront ? t_max : fminf(next_up(thi), t_max);
         proxy_test<MODE != kClosestAny>(F, S.w2o, j, o, d, tlo, tb, [&](float t, int) {
-          if (nh < kMaxHitsPerProxy) ht[nh] = t;
+          h5 = h4;
+          h4 = h3;
+          h3 = h2;
+          h2 = h1;
+          h1 = h0;
+          h0 = t;
           ++nh;
         });
         if (nh > kMaxHitsPerProxy) {
@@ -233,18 +264,20 @@ __device__ __forceinline__ void traverse8(const SceneDev& S, const FaceTable& F,
       } else {
         uint32_t p = nh ? __ldg(S.leaf_pidx + j) : 0u;
         st.anyhits += nh;
-        int hi = 0;
         while (true) {
-          uint32_t pend = __ballot_sync(kFull, hi < nh);
+          uint32_t pend = __ballot_sync(kFull, nh > 0);
           if (!pend) break;
           int src = __ffs(pend) - 1;
-          float myt = 0.f;
-#pragma unroll
-          for (int q = 0; q < kMaxHitsPerProxy; ++q)
-            if (q == hi) myt = ht[q];
-          float t = __shfl_sync(kFull, myt, src);
+          float t = __shfl_sync(kFull, h0, src);
           uint32_t pp = __shfl_sync(kFull, p, src);
-          if ((int)lane == src) ++hi;
+          if ((int)lane == src) {
+            h0 = h1;
+            h1 = h2;
+            h2 = h3;
+            h3 = h4;
+            h4 = h5;
+            --nh;
+          }
           warp_insert(bt, bp, t, pp, lane);
         }
         thi = __shfl_sync(kFull, bt, cull_lane);
@@ -403,7 +436,7 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
 // counter (slot = 32 * tile + position in the 8x4 tile, views back to back),
 // so neighbouring pixels run on neighbouring warps at the same time.
 template <bool RECORD>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_trace8(const ViewDev* __restrict__ views, uint32_t n_views,
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_trace8(const ViewDev* __restrict__ views, uint32_t n_views,
                                                                   uint32_t total_tiles, DevCounters* ctr,
                                                                   const __grid_constant__ FaceTable F,
                                                                   const uint32_t* pixels, uint32_t n_pix,
