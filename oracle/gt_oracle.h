@@ -93,6 +93,15 @@ int or_backward_f64(const or_scene_f64* s, const void* uniforms, uint32_t w, uin
                     const uint32_t* pixels, uint32_t n_pix, const double* dL_drgba,
                     int threads, double* dL_dparams);
 
+/* FP64 adjoint on given entry lists: for each listed pixel, the composited
+ * hit sequence of a render (particle indices, `counts` entries, rows of
+ * `max_e`) and optionally which entries passed alpha_min (NULL: decided in
+ * double).  Rounds are implicit in the lists. */
+int or_backward_lists_f64(const or_scene_f64* s, const void* uniforms, uint32_t w, uint32_t h,
+                          const uint32_t* pixels, uint32_t n_pix, const uint32_t* lists,
+                          const uint8_t* contrib, const uint32_t* counts, uint32_t max_e,
+                          const double* dL_drgba, int threads, double* dL_dparams);
+
 #ifdef __cplusplus
 }
 #endif

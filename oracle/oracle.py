@@ -58,6 +58,8 @@ def lib():
             r.argtypes = [vp, vp, u32, u32, vp, u32, i32, i32, vp, C.POINTER(OrHits)]
         L.or_backward_f64.restype = i32
         L.or_backward_f64.argtypes = [vp, vp, u32, u32, vp, u32, vp, i32, vp]
+        L.or_backward_lists_f64.restype = i32
+        L.or_backward_lists_f64.argtypes = [vp, vp, u32, u32, vp, u32, vp, vp, vp, u32, vp, i32, vp]
         _lib = L
     return _lib
 
@@ -137,6 +139,33 @@ class Scene:
         if rc != 0:
             raise RuntimeError(f"oracle backward failed ({rc})")
         return out[:, :self.n]
+
+
+def backward_lists(scene: "Scene", uniforms, w: int, h: int, hits: dict, dL_drgba, pixels=None,
+                   alpha_min: float | None = None, threads: int = 0) -> np.ndarray:
+    """FP64 adjoint on the entry lists of a (float) render: `hits` holds
+    pidx (n_pix x max_e), count and alpha; entries with alpha > alpha_min
+    (the float decision) are the composited ones."""
+    if scene.precision != "f64":
+        raise ValueError("the oracle adjoint is FP64")
+    u = np.frombuffer(bytes(uniforms), dtype=np.uint8).copy()
+    pix = None if pixels is None else np.ascontiguousarray(pixels, dtype=np.uint32)
+    npix = w * h if pix is None else pix.shape[0]
+    lists = np.ascontiguousarray(hits["pidx"], dtype=np.uint32)
+    max_e = lists.shape[1]
+    if (np.asarray(hits["count"]) > max_e).any():
+        raise ValueError("entry lists are truncated")
+    contrib = None
+    if alpha_min is not None:
+        contrib = np.ascontiguousarray(np.asarray(hits["alpha"]) > np.float32(alpha_min), dtype=np.uint8)
+    counts = np.ascontiguousarray(hits["count"], dtype=np.uint32)
+    g = np.ascontiguousarray(dL_drgba, dtype=np.float64).reshape(npix, 4)
+    out = np.zeros((59, max(scene.n, 1)), dtype=np.float64)
+    rc = lib().or_backward_lists_f64(scene._h, _ptr(u), w, h, _ptr(pix), npix, _ptr(lists), _ptr(contrib),
+                                     _ptr(counts), max_e, _ptr(g), threads, _ptr(out))
+    if rc != 0:
+        raise RuntimeError(f"oracle backward failed ({rc})")
+    return out[:, :scene.n]
 
 
 def ply_to_aos(data: bytes) -> np.ndarray:

@@ -1,0 +1,101 @@
+"""GPU adjoint: gt_backward against the oracle's FP64 adjoint (itself checked
+against central finite differences in test_backward_cpu.py), both
+checkpoint and replay modes, batches and accumulation.  The FP64 reference
+runs on the composited entry lists of the float render (which the CUDA
+forward reproduces bit for bit), so both sides differentiate the same
+piecewise-smooth function.
+
+Tolerance: relative error <= 1e-3 per parameter row in the 2-norm, and per
+element |cuda - fp64| <= 1e-3 |fp64| + 1e-4 max|row| (float arithmetic and
+atomic summation order against double)."""
+import numpy as np
+import pytest
+
+from conftest import small_scene, view
+from oracle import oracle
+from gtrace.tracer import Scene
+
+pytestmark = pytest.mark.gpu
+
+
+def _ref_grad(rec, amin, uniforms, w, h, g):
+    from gtrace.uniforms import unpack_uniforms
+    _, hits = oracle.Scene(rec, amin, "f32").render(uniforms, w, h, max_entries=1024)
+    s64 = oracle.Scene(rec, amin, "f64")
+    return oracle.backward_lists(s64, uniforms, w, h, hits, np.asarray(g, np.float64).reshape(-1, 4),
+                                 alpha_min=unpack_uniforms(uniforms)["alpha_min"])
+
+
+def _check(got, ref, rel=1e-3):
+    for i in range(59):
+        r = ref[i]
+        scale = np.abs(r).max()
+        if scale == 0:
+            assert np.abs(got[i]).max() <= 1e-6
+            continue
+        assert np.linalg.norm(got[i] - r) <= rel * np.linalg.norm(r) + 1e-6 * scale, i
+        assert (np.abs(got[i] - r) <= rel * np.abs(r) + 1e-4 * scale).mean() >= 0.999, i
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("k", [4, 16])
+def test_gradient_matches_fp64_oracle(ctx, mode, k):
+    pg = small_scene(n=1500, seed=41)
+    rec = pg.gaussiansBuffer
+    w, h = 48, 40
+    v = view(w, h, k=k)
+    rng = np.random.default_rng(k)
+    g = rng.normal(size=(h, w, 4)).astype(np.float32)
+    s = Scene(ctx, rec, 0.01)
+    got, info = ctx.backward(s, v.uniforms, w, h, g, mode=mode)
+    assert info["used_mode"] == mode
+    ref = _ref_grad(rec, 0.01, v.uniforms, w, h, g)
+    _check(got, ref)
+    assert np.abs(got).sum() > 0
+
+
+def test_checkpoint_and_replay_agree_and_grow(ctx):
+    pg = small_scene(n=2000, seed=42)
+    s = Scene(ctx, pg.gaussiansBuffer, 0.01)
+    w, h = 40, 30
+    v = view(w, h, k=2)  # many rounds per ray: forces the checkpoint to grow past 2 rounds
+    g = np.random.default_rng(3).normal(size=(h, w, 4)).astype(np.float32)
+    a, ia = ctx.backward(s, v.uniforms, w, h, g, mode=1, max_rounds=2)
+    b, ib = ctx.backward(s, v.uniforms, w, h, g, mode=2, max_rounds=2)
+    assert ia["max_rounds"] > 2 and ib["max_rounds"] > 2
+    np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-6 * np.abs(a).max())
+
+
+def test_l2_loss_against_perturbed_target(ctx):
+    """The differentiable configuration in miniature: L = sum (rgb - target)^2."""
+    from gtrace import synth
+    raw = synth.raw_clusters(3000, seed=77)
+    target_raw = synth.perturb(raw, seed=78)
+    pg, tg = synth.pack(raw), synth.pack(target_raw)
+    w, h = 56, 56
+    v = view(w, h, pos=(0.0, 0.0, 12.0), k=8)
+    s, st = Scene(ctx, pg.gaussiansBuffer, 0.01), Scene(ctx, tg.gaussiansBuffer, 0.01)
+    img = ctx.render(s, v.uniforms, w, h)
+    tgt = ctx.render(st, v.uniforms, w, h)
+    g = np.zeros_like(img)
+    g[..., :3] = 2.0 * (img[..., :3] - tgt[..., :3])
+    got, _ = ctx.backward(s, v.uniforms, w, h, g)
+    ref = _ref_grad(pg.gaussiansBuffer, 0.01, v.uniforms, w, h, g)
+    _check(got, ref)
+
+
+def test_batch_sums_views_and_accumulate_flag(ctx):
+    pg = small_scene(n=1200, seed=43)
+    s = Scene(ctx, pg.gaussiansBuffer, 0.01)
+    v1 = view(32, 24, k=6)
+    v2 = view(20, 36, pos=(1.5, 0.5, 3.5), k=6)
+    rng = np.random.default_rng(5)
+    g1 = rng.normal(size=(24, 32, 4)).astype(np.float32)
+    g2 = rng.normal(size=(36, 20, 4)).astype(np.float32)
+    a, _ = ctx.backward(s, v1.uniforms, 32, 24, g1)
+    b, _ = ctx.backward(s, v2.uniforms, 20, 36, g2)
+    res, info = ctx.backward_batch([(s, v1.uniforms, 32, 24, g1), (s, v2.uniforms, 20, 36, g2)])
+    np.testing.assert_allclose(res[s], a + b, rtol=1e-5, atol=1e-6 * np.abs(a + b).max())
+    acc = a.copy()
+    acc2, _ = ctx.backward(s, v2.uniforms, 20, 36, g2, out=acc, accumulate=True)
+    np.testing.assert_allclose(acc2, a + b, rtol=1e-5, atol=1e-6 * np.abs(a + b).max())

@@ -106,6 +106,7 @@ static SceneDev scene_dev(const gt_scene* s) {
   d.leaf_pidx = s->b.leaf_pidx;
   d.shade = s->b.shade;
   d.sh = s->b.sh;
+  d.params = s->b.params;
   d.root = s->b.root;
   d.n_kept = (uint32_t)s->b.n_kept;
   d.n_sh = s->b.n_sh;
@@ -168,6 +169,7 @@ LaunchShape api_shape_for(gt_context* ctx, const gt_scene* s, uint32_t w, uint32
   return shape_for(ctx, s, w, h, k);
 }
 void api_fill_stats(const DevCounters& c, gt_render_stats* st) { fill_stats(c, st); }
+gt_status api_ensure_views(gt_context* ctx, uint32_t n) { return ensure_views(ctx, n); }
 }  // namespace gt
 
 // ============================================================== context
@@ -196,6 +198,14 @@ extern "C" gt_status gt_context_create(int device, gt_context** out) {
   CTX_TRY(cudaSetDevice(device));
   CTX_TRY(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
   CTX_TRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  {
+    // keep stream-ordered temporaries (scene builds, adjoint checkpoints) cached
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = ~0ull;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  }
   CTX_TRY(cudaMalloc(&ctx->d_ctr, sizeof(DevCounters)));
   CTX_TRY(cudaHostAlloc((void**)&ctx->h_ctr, sizeof(DevCounters), cudaHostAllocDefault));
   CTX_TRY(cudaEventCreate(&ctx->call0));

@@ -1,11 +1,532 @@
-// gt_backward.cu — adjoint of the tracer (placeholder until the adjoint kernel lands).
-#include "gt_internal.cuh"
+// gt_backward.cu — adjoint of the tracer: dLoss/d(particle parameters) from
+// dLoss/d(pixel).  No counterpart in the reference (it has no training path,
+// README.md:69); the forward it differentiates is tracePath
+// (src/GS_shader.ts:192-273) as implemented in gt_trace.cu.
+//
+// Scheme.  A forward pass writes, per ray and round, t_curr and the
+// transmittance T at the round's start (and, in checkpoint mode, the round's
+// particle indices).  The adjoint then walks each ray's rounds from the last
+// to the first, one warp per ray:
+//   * the round's entries come from the checkpoint, or are found again by a
+//     traversal from the stored t_curr (replay mode; the set is the same: it is
+//     the k closest front-face hits beyond t_curr);
+//   * lanes recompute alpha_i and the SH colour c_i of one entry each, and the
+//     transmittance before each entry, T_i, in entry order from the stored T
+//     (bit-identical to the forward's);
+//   * back to front, with R the radiance behind the current entry divided by
+//     its transmittance (R <- a c + (1 - a) R, carried across rounds),
+//     dL/dalpha_i = T_i (g.c_i - g.R) and dL/dc_i = T_i alpha_i g; no division
+//     by (1 - alpha), so alpha close to 1 is harmless;
+//   * alpha = opacity * exp(E), E = -(p - mu)^T A (p - mu) at the point of
+//     maximum density p, where dE/dtau = 0: mu and A act only directly,
+//     dE/dmu = 2 A (p - mu), dE/dA = -(p - mu)(p - mu)^T, A = R S^-2 R^T with
+//     R the rotation of the stored quaternion (as computeResponse builds it,
+//     src/GS_shader.ts:115-130) and S the scales;
+//   * the SH direction normalize(mu - origin) (src/GS_shader.ts:264) adds its
+//     own position gradient.
+// Hit sets are held fixed: the proxy geometry is piecewise constant.
+// Per-particle gradients accumulate with 16-byte vector atomics into a
+// particle-major buffer (60 floats per particle) that a final kernel writes
+// out parameter-major.
+#include <cuda_runtime.h>
+#include <string.h>
 
-extern "C" gt_status gt_backward(gt_context*, const gt_scene*, const gt_uniforms*, uint32_t, uint32_t, const float*,
-                                 float*, uint32_t, gt_bwd_opts*, gt_render_stats*) {
-  return GT_ERR_UNSUPPORTED;
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "gt_device.cuh"
+#include "gt_handles.h"
+#include "gt_internal.cuh"
+#include "gt_trace_common.cuh"
+#include "gt_warp.cuh"
+
+namespace gt {
+
+constexpr int kGradStride = 60;  // floats per particle in the accumulation buffer
+
+// Real SH basis of degree <= deg at direction d and its gradient
+// (the polynomials of shToRadiance, src/GS_shader.ts:138-177).
+__device__ __forceinline__ void sh_basis(V3 d, uint32_t deg, float B[16], float dB[16][3]) {
+  const float x = d.x, y = d.y, z = d.z, xx = x * x, yy = y * y, zz = z * z;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    B[k] = 0.f;
+    dB[k][0] = dB[k][1] = dB[k][2] = 0.f;
+  }
+  B[0] = GT_SH_C0;
+  if (deg >= 1) {
+    B[1] = -GT_SH_C1 * y; dB[1][1] = -GT_SH_C1;
+    B[2] = GT_SH_C1 * z;  dB[2][2] = GT_SH_C1;
+    B[3] = -GT_SH_C1 * x; dB[3][0] = -GT_SH_C1;
+  }
+  if (deg >= 2) {
+    B[4] = GT_SH_C2_0 * x * y; dB[4][0] = GT_SH_C2_0 * y; dB[4][1] = GT_SH_C2_0 * x;
+    B[5] = GT_SH_C2_1 * y * z; dB[5][1] = GT_SH_C2_1 * z; dB[5][2] = GT_SH_C2_1 * y;
+    B[6] = GT_SH_C2_2 * (2.f * zz - xx - yy);
+    dB[6][0] = -2.f * GT_SH_C2_2 * x; dB[6][1] = -2.f * GT_SH_C2_2 * y; dB[6][2] = 4.f * GT_SH_C2_2 * z;
+    B[7] = GT_SH_C2_3 * x * z; dB[7][0] = GT_SH_C2_3 * z; dB[7][2] = GT_SH_C2_3 * x;
+    B[8] = GT_SH_C2_4 * (xx - yy); dB[8][0] = 2.f * GT_SH_C2_4 * x; dB[8][1] = -2.f * GT_SH_C2_4 * y;
+  }
+  if (deg >= 3) {
+    B[9] = GT_SH_C3_0 * y * (3.f * xx - yy);
+    dB[9][0] = GT_SH_C3_0 * 6.f * x * y; dB[9][1] = GT_SH_C3_0 * (3.f * xx - 3.f * yy);
+    B[10] = GT_SH_C3_1 * x * y * z;
+    dB[10][0] = GT_SH_C3_1 * y * z; dB[10][1] = GT_SH_C3_1 * x * z; dB[10][2] = GT_SH_C3_1 * x * y;
+    B[11] = GT_SH_C3_2 * y * (4.f * zz - xx - yy);
+    dB[11][0] = -2.f * GT_SH_C3_2 * x * y; dB[11][1] = GT_SH_C3_2 * (4.f * zz - xx - 3.f * yy);
+    dB[11][2] = 8.f * GT_SH_C3_2 * y * z;
+    B[12] = GT_SH_C3_3 * z * (2.f * zz - 3.f * xx - 3.f * yy);
+    dB[12][0] = -6.f * GT_SH_C3_3 * x * z; dB[12][1] = -6.f * GT_SH_C3_3 * y * z;
+    dB[12][2] = GT_SH_C3_3 * (6.f * zz - 3.f * xx - 3.f * yy);
+    B[13] = GT_SH_C3_4 * x * (4.f * zz - xx - yy);
+    dB[13][0] = GT_SH_C3_4 * (4.f * zz - 3.f * xx - yy); dB[13][1] = -2.f * GT_SH_C3_4 * x * y;
+    dB[13][2] = 8.f * GT_SH_C3_4 * x * z;
+    B[14] = GT_SH_C3_5 * z * (xx - yy);
+    dB[14][0] = 2.f * GT_SH_C3_5 * x * z; dB[14][1] = -2.f * GT_SH_C3_5 * y * z; dB[14][2] = GT_SH_C3_5 * (xx - yy);
+    B[15] = GT_SH_C3_6 * x * (xx - 3.f * yy);
+    dB[15][0] = GT_SH_C3_6 * (3.f * xx - 3.f * yy); dB[15][1] = -6.f * GT_SH_C3_6 * x * y;
+  }
 }
-extern "C" gt_status gt_backward_batch(gt_context*, const gt_batch_item*, uint32_t, const gt_scene* const*,
-                                       float* const*, uint32_t, uint32_t, gt_bwd_opts*, gt_render_stats*) {
-  return GT_ERR_UNSUPPORTED;
+
+// Gradient contribution of one composited entry (alpha > alpha_min).
+//   T: transmittance before the entry; a: its alpha; resp: exp(E);
+//   q: p - mu at the point of maximum density; craw: SH colour before the
+//   clamp; ga: dL/dalpha; g: dL/dpixel (rgb).
+__device__ __forceinline__ void entry_gradient(const SceneDev& S, uint32_t p, const Shade& sd, V3 o, V3 dr, float T,
+                                               float a, float resp, V3 q, const float craw[3], float ga,
+                                               const float g[3], uint32_t deg, float* G) {
+  double aqd[3];
+  float out[kGradStride];
+#pragma unroll
+  for (int i = 0; i < kGradStride; ++i) out[i] = 0.f;
+  // colour: SH coefficients and the direction normalize(mu - o)
+  float gc[3];
+#pragma unroll
+  for (int ch = 0; ch < 3; ++ch) gc[ch] = craw[ch] > 0.f ? T * a * g[ch] : 0.f;
+  V3 v = vsub(sd.mu, o);
+  float len = sqrtf(vdot(v, v));
+  V3 dir = mk(v.x / len, v.y / len, v.z / len);
+  float B[16], dB[16][3];
+  sh_basis(dir, deg, B, dB);
+  const float4* shp = S.sh + 12 * (size_t)p;
+  float shv[48];
+#pragma unroll
+  for (int i = 0; i < 12; ++i) {
+    float4 c = __ldg(shp + i);
+    shv[4 * i] = c.x;
+    shv[4 * i + 1] = c.y;
+    shv[4 * i + 2] = c.z;
+    shv[4 * i + 3] = c.w;
+  }
+  float dd0 = 0.f, dd1 = 0.f, dd2 = 0.f;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    float sg = shv[3 * k] * gc[0] + shv[3 * k + 1] * gc[1] + shv[3 * k + 2] * gc[2];
+    dd0 += dB[k][0] * sg;
+    dd1 += dB[k][1] * sg;
+    dd2 += dB[k][2] * sg;
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) out[11 + 3 * k + ch] = B[k] * gc[ch];
+  }
+  float dd = dd0 * dir.x + dd1 * dir.y + dd2 * dir.z;
+  float dmu0 = (dd0 - dir.x * dd) / len, dmu1 = (dd1 - dir.y * dd) / len, dmu2 = (dd2 - dir.z * dd) / len;
+  // alpha = opacity * exp(E).  q = p - mu is the small difference of two
+  // points about |origin - mu| away, so it is formed in double here; A q is
+  // nearly orthogonal to the ray and keeps its small components only so.
+  out[10] = ga * resp;
+  const float gE = ga * sd.opacity * resp;
+  {
+    const double a00 = sd.a00, a01 = sd.a01, a02 = sd.a02, a11 = sd.a11, a12 = sd.a12, a22 = sd.a22;
+    const double dx = dr.x, dy = dr.y, dz = dr.z;
+    const double mx = (double)sd.mu.x - (double)o.x, my = (double)sd.mu.y - (double)o.y,
+                 mz = (double)sd.mu.z - (double)o.z;
+    const double t0 = a00 * dx + a01 * dy + a02 * dz, t1 = a01 * dx + a11 * dy + a12 * dz,
+                 t2 = a02 * dx + a12 * dy + a22 * dz;
+    const double tau = (mx * t0 + my * t1 + mz * t2) / (dx * t0 + dy * t1 + dz * t2);
+    const double qx = tau * dx - mx, qy = tau * dy - my, qz = tau * dz - mz;
+    q = mk((float)qx, (float)qy, (float)qz);
+    aqd[0] = a00 * qx + a01 * qy + a02 * qz;
+    aqd[1] = a01 * qx + a11 * qy + a12 * qz;
+    aqd[2] = a02 * qx + a12 * qy + a22 * qz;
+  }
+  const float aq0 = (float)aqd[0], aq1 = (float)aqd[1], aq2 = (float)aqd[2];
+  out[0] = dmu0 + 2.f * gE * aq0;
+  out[1] = dmu1 + 2.f * gE * aq1;
+  out[2] = dmu2 + 2.f * gE * aq2;
+  const float4 sa = __ldg(S.params + 2 * (size_t)p), qa = __ldg(S.params + 2 * (size_t)p + 1);
+  const float s[3] = {sa.x, sa.y, sa.z};
+  const float qw = qa.x, qx = qa.y, qy = qa.z, qz = qa.w;
+  // rotation of the quaternion (rows); computeResponse's matrix is its transpose
+  const float R[3][3] = {{1.f - 2.f * (qy * qy + qz * qz), 2.f * (qx * qy - qw * qz), 2.f * (qx * qz + qw * qy)},
+                         {2.f * (qx * qy + qw * qz), 1.f - 2.f * (qx * qx + qz * qz), 2.f * (qy * qz - qw * qx)},
+                         {2.f * (qx * qz - qw * qy), 2.f * (qy * qz + qw * qx), 1.f - 2.f * (qx * qx + qy * qy)}};
+  const float qv[3] = {q.x, q.y, q.z};
+  float u[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) u[k] = R[0][k] * qv[0] + R[1][k] * qv[1] + R[2][k] * qv[2];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) out[3 + k] = gE * 2.f * u[k] * u[k] / (s[k] * s[k] * s[k]);
+  float GR[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) GR[r][c] = -2.f * gE * qv[r] * u[c] / (s[c] * s[c]);
+  out[6] = 2.f * (-qz * GR[0][1] + qy * GR[0][2] + qz * GR[1][0] - qx * GR[1][2] - qy * GR[2][0] + qx * GR[2][1]);
+  out[7] = 2.f * (qy * GR[0][1] + qz * GR[0][2] + qy * GR[1][0] - 2.f * qx * GR[1][1] - qw * GR[1][2] +
+                  qz * GR[2][0] + qw * GR[2][1] - 2.f * qx * GR[2][2]);
+  out[8] = 2.f * (-2.f * qy * GR[0][0] + qx * GR[0][1] + qw * GR[0][2] + qx * GR[1][0] + qz * GR[1][2] -
+                  qw * GR[2][0] + qz * GR[2][1] - 2.f * qy * GR[2][2]);
+  out[9] = 2.f * (-2.f * qz * GR[0][0] - qw * GR[0][1] + qx * GR[0][2] + qw * GR[1][0] - 2.f * qz * GR[1][1] +
+                  qy * GR[1][2] + qx * GR[2][0] + qy * GR[2][1]);
+  float4* dst = reinterpret_cast<float4*>(G + (size_t)p * kGradStride);
+#pragma unroll
+  for (int c = 0; c < kGradStride / 4; ++c) {
+    float4 v4 = make_float4(out[4 * c], out[4 * c + 1], out[4 * c + 2], out[4 * c + 3]);
+    if (v4.x != 0.f || v4.y != 0.f || v4.z != 0.f || v4.w != 0.f) atomicAdd(dst + c, v4);
+  }
+}
+
+// The adjoint, one warp per ray slot (same slot numbering as the forward).
+template <bool CKPT_PIDX>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewDev* __restrict__ views,
+                                                                    uint32_t n_views, uint32_t total_tiles,
+                                                                    DevCounters* ctr, const __grid_constant__ FaceTable F,
+                                                                    const Ckpt ck) {
+  __shared__ WarpScratch scratch[kWarpsPerBlock];
+  const uint32_t lane = threadIdx.x & 31;
+  WarpScratch& W = scratch[threadIdx.x >> 5];
+  RayStats st = {0, 0, 0, 0, 0, 0};
+  uint32_t status = 0, rays = 0;
+  const uint32_t total = total_tiles * 32u;
+  while (true) {
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(&ctr->work, 1u);
+    item = __shfl_sync(kFull, item, 0);
+    if (item >= total) break;
+    uint32_t tile = item >> 5, sl = item & 31u;
+    const uint32_t vi = n_views == 1 ? 0u : find_view(views, n_views, tile);
+    const ViewDev& V = views[vi];
+    uint32_t lt = tile - V.tile_begin;
+    uint32_t px = (lt % V.tiles_x) * kTileW + (sl % kTileW);
+    uint32_t py = (lt / V.tiles_x) * kTileH + (sl / kTileW);
+    if (px >= V.w || py >= V.h) continue;
+    const uint32_t nr = min(ck.nrounds[item], ck.cap);
+    if (nr == 0) continue;
+    const float4 g4 = V.dL[(size_t)py * V.w + px];
+    if (g4.x == 0.f && g4.y == 0.f && g4.z == 0.f) continue;
+    const float g[3] = {g4.x, g4.y, g4.z};
+    V3 o, d;
+    ray_gen(V.u, V.w, V.h, px, py, o, d);
+    const BoxRay br = make_boxray(o, d, V.s.scene_mag);
+    const uint32_t k = V.u.k;
+    float R0 = 0.f, R1 = 0.f, R2 = 0.f;
+    ++rays;
+    for (int r = (int)nr - 1; r >= 0; --r) {
+      const size_t at = (size_t)item * ck.cap + r;
+      const float2 ri = ck.rinfo[at];
+      uint32_t p = kInvalid;
+      bool valid;
+      if (CKPT_PIDX) {
+        p = lane < ck.kc ? ck.pidx[at * ck.kc + lane] : kInvalid;
+        valid = lane < k && p != kInvalid;
+      } else {
+        float bt = V.u.t_max;
+        uint32_t bp = kInvalid;
+        traverse8<kCollect>(V.s, F, W, o, d, br, ri.x, V.u.t_max, bt, bp, nullptr, st, status, lane);
+        if (__reduce_or_sync(kFull, status) & (kStatusStackOverflow | kStatusVisitCap | kStatusHitOverflow)) break;
+        valid = lane < k && bp != kInvalid;
+        p = bp;
+      }
+      const uint32_t vmask = __ballot_sync(kFull, valid);
+      const int n = __popc(vmask);
+      float alpha = 0.f, resp = 0.f;
+      float craw[3] = {0.f, 0.f, 0.f};
+      V3 q = mk(0.f, 0.f, 0.f);
+      Shade sd;
+      bool contrib = false;
+      if (valid) {
+        sd = load_shade(V.s.shade, p);
+        resp = response(sd, o, d, &q);
+        alpha = resp * sd.opacity;
+        contrib = V.u.alpha_min < alpha;
+        if (contrib) sh_radiance(V.s.sh, p, vnorm(vsub(sd.mu, o)), V.u.deg, craw);
+      }
+      const uint32_t cmask = __ballot_sync(kFull, contrib);
+      // transmittance before each entry, in entry order from the round's start
+      float T = ri.y, Tme = 0.f;
+      for (int e = 0; e < n; ++e) {
+        if ((int)lane == e) Tme = T;
+        float a = __shfl_sync(kFull, alpha, e);
+        if ((cmask >> e) & 1u) T = T * (1.0f - a);
+      }
+      // back to front
+      float ga = 0.f;
+      for (int e = n - 1; e >= 0; --e) {
+        float a = __shfl_sync(kFull, alpha, e);
+        float c0 = __shfl_sync(kFull, craw[0], e), c1 = __shfl_sync(kFull, craw[1], e),
+              c2 = __shfl_sync(kFull, craw[2], e);
+        float te = __shfl_sync(kFull, Tme, e);
+        if ((cmask >> e) & 1u) {
+          c0 = c0 > 0.f ? c0 : 0.f;
+          c1 = c1 > 0.f ? c1 : 0.f;
+          c2 = c2 > 0.f ? c2 : 0.f;
+          float gae = te * ((g[0] * c0 + g[1] * c1 + g[2] * c2) - (g[0] * R0 + g[1] * R1 + g[2] * R2));
+          if ((int)lane == e) ga = gae;
+          R0 = a * c0 + (1.f - a) * R0;
+          R1 = a * c1 + (1.f - a) * R1;
+          R2 = a * c2 + (1.f - a) * R2;
+        }
+      }
+      if (contrib) entry_gradient(V.s, p, sd, o, d, Tme, alpha, resp, q, craw, ga, g, V.u.deg, V.grad);
+      st.rounds += lane == 0 ? 1u : 0u;
+      st.entries += lane == 0 ? (uint32_t)n : 0u;
+      st.contributing += lane == 0 ? (uint32_t)__popc(cmask) : 0u;
+    }
+  }
+  flush_stats(ctr, st, rays, status);
+}
+
+// Parameter-major output: out[i * n + p] (+)= G[p * 60 + i], i < 59.
+__global__ void k_grad_out(const float* G, uint64_t n, float* out, bool accumulate) {
+  uint64_t idx = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (idx >= n * GT_PARAMS_PER_PARTICLE) return;
+  uint64_t i = idx / n, p = idx % n;
+  float v = G[p * kGradStride + i];
+  out[idx] = accumulate ? out[idx] + v : v;
+}
+
+}  // namespace gt
+
+using namespace gt;
+
+namespace {
+
+struct BwdView {
+  const gt_scene* scene;
+  gt_uniforms u;
+  uint32_t w, h;
+  const float* dL;
+};
+
+gt_status backward_impl(gt_context* ctx, const BwdView* views, uint32_t count, const gt_scene* const* scenes,
+                        float* const* outs, uint32_t n_scenes, uint32_t flags, gt_bwd_opts* opts,
+                        gt_render_stats* stats) {
+  if (count == 0) return GT_OK;
+  cudaError_t ce = cudaSetDevice(ctx->device);
+  if (ce != cudaSuccess) return api_fail(ctx, GT_ERR_CUDA, cudaGetErrorString(ce));
+  cudaStream_t st = ctx->stream;
+  std::vector<void*> temps;
+  auto cleanup = [&]() {
+    for (void* p : temps) cudaFreeAsync(p, st);
+    cudaStreamSynchronize(st);
+  };
+  auto talloc = [&](void** p, size_t bytes) -> cudaError_t {
+    cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 16, st);
+    if (e == cudaSuccess) temps.push_back(*p);
+    return e;
+  };
+#define BWD_TRY(expr)                                                                                     \
+  do {                                                                                                    \
+    cudaError_t e_ = (expr);                                                                              \
+    if (e_ != cudaSuccess) {                                                                              \
+      cleanup();                                                                                          \
+      return api_fail(ctx, e_ == cudaErrorMemoryAllocation ? GT_ERR_OOM : GT_ERR_CUDA,                      \
+                      std::string(#expr) + ": " + cudaGetErrorString(e_));                                \
+    }                                                                                                     \
+  } while (0)
+  // per-scene accumulation buffers
+  std::vector<float*> G(n_scenes, nullptr);
+  for (uint32_t s = 0; s < n_scenes; ++s) {
+    uint64_t n = scenes[s]->n;
+    BWD_TRY(talloc((void**)&G[s], (size_t)std::max<uint64_t>(n, 1) * kGradStride * 4));
+    BWD_TRY(cudaMemsetAsync(G[s], 0, (size_t)std::max<uint64_t>(n, 1) * kGradStride * 4, st));
+  }
+  // view table: outputs go to scratch images; dL on the device
+  uint32_t total_tiles = 0, kc = 1;
+  size_t pixels = 0;
+  for (uint32_t i = 0; i < count; ++i) pixels += (size_t)views[i].w * views[i].h;
+  float4* img = nullptr;
+  float4* dl_dev = nullptr;
+  BWD_TRY(talloc((void**)&img, pixels * sizeof(float4)));
+  if (!(flags & GT_FLAG_INPUT_DEVICE)) BWD_TRY(talloc((void**)&dl_dev, pixels * sizeof(float4)));
+  gt_status sst = GT_OK;
+  std::vector<ViewDev> vd(count);
+  size_t off = 0;
+  for (uint32_t i = 0; i < count; ++i) {
+    const BwdView& bv = views[i];
+    vd[i] = api_make_view(bv.scene, bv.u, bv.w, bv.h, img + off, total_tiles);
+    total_tiles += vd[i].n_tiles;
+    kc = std::max(kc, bv.u.k);
+    size_t px = (size_t)bv.w * bv.h;
+    if (flags & GT_FLAG_INPUT_DEVICE) {
+      vd[i].dL = reinterpret_cast<const float4*>(bv.dL);
+    } else {
+      BWD_TRY(cudaMemcpyAsync(dl_dev + off, bv.dL, px * sizeof(float4), cudaMemcpyHostToDevice, st));
+      vd[i].dL = dl_dev + off;
+    }
+    uint32_t s = 0;
+    while (s < n_scenes && scenes[s] != bv.scene) ++s;
+    vd[i].grad = G[s];
+    off += px;
+  }
+  sst = api_ensure_views(ctx, count);
+  if (sst != GT_OK) {
+    cleanup();
+    return sst;
+  }
+  const uint64_t slots = (uint64_t)total_tiles * 32u;
+  // checkpoint capacity and mode
+  uint32_t cap = opts && opts->max_rounds ? opts->max_rounds : 16u;
+  uint32_t mode = opts ? opts->mode : 0u;
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  uint64_t budget = opts && opts->mem_budget ? opts->mem_budget : free_b / 2;
+  uint32_t* ck_misc = nullptr;  // [0] max rounds, [1] overflow
+  BWD_TRY(talloc((void**)&ck_misc, 8));
+  Ckpt ck;
+  ck.kc = kc;
+  ck.max_rounds = ck_misc;
+  ck.overflow = ck_misc + 1;
+  LaunchShape shape = api_shape_for(ctx, views[0].scene, views[0].w, views[0].h, views[0].u.k);
+  float fwd_ms = 0.f, bwd_ms = 0.f;
+  uint32_t used_mode = 0;
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    uint64_t need_replay = slots * (4 + (uint64_t)cap * 8);
+    uint64_t need_ckpt = need_replay + slots * (uint64_t)cap * kc * 4;
+    used_mode = mode == 1 ? 1u : (mode == 2 ? 2u : (need_ckpt <= budget ? 1u : 2u));
+    BWD_TRY(talloc((void**)&ck.nrounds, slots * 4));
+    BWD_TRY(talloc((void**)&ck.rinfo, slots * (size_t)cap * sizeof(float2)));
+    ck.pidx = nullptr;
+    if (used_mode == 1) BWD_TRY(talloc((void**)&ck.pidx, slots * (size_t)cap * kc * 4));
+    ck.cap = cap;
+    BWD_TRY(cudaMemsetAsync(ck.nrounds, 0, slots * 4, st));
+    BWD_TRY(cudaMemsetAsync(ck_misc, 0, 8, st));
+    BWD_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), st));
+    BWD_TRY(cudaEventRecord(ctx->timer0, st));
+    Err e = launch_trace(vd.data(), count, total_tiles, ctx->d_ctr, ctx->faces, shape, ctx->num_sms, st,
+                         &ctx->launches, ctx->d_views, &ck);
+    if (e.code != GT_OK) {
+      cleanup();
+      return api_fail(ctx, e.code, e.msg);
+    }
+    BWD_TRY(cudaEventRecord(ctx->timer1, st));
+    uint32_t misc[2];
+    BWD_TRY(cudaMemcpyAsync(misc, ck_misc, 8, cudaMemcpyDeviceToHost, st));
+    BWD_TRY(cudaMemcpyAsync(ctx->h_ctr, ctx->d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
+    BWD_TRY(cudaStreamSynchronize(st));
+    cudaEventElapsedTime(&fwd_ms, ctx->timer0, ctx->timer1);
+    sst = api_status_to_error(ctx, ctx->h_ctr->status);
+    if (sst != GT_OK) {
+      cleanup();
+      return sst;
+    }
+    if (!misc[1]) break;
+    if (attempt == 3) {
+      cleanup();
+      return api_fail(ctx, GT_ERR_DEVICE_TIMEOUT, "checkpoint capacity exceeded");
+    }
+    // grow to the deepest ray and run the checkpointing forward again
+    cap = std::max(misc[0], 2 * cap);
+  }
+  // adjoint
+  BWD_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), st));
+  BWD_TRY(cudaEventRecord(ctx->timer0, st));
+  {
+    uint32_t block = kWarpsPerBlock * 32;
+    uint32_t grid = (uint32_t)ctx->num_sms * std::max(1u, shape.blocks_per_sm);
+    uint64_t max_grid = (slots + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    if (grid > max_grid) grid = (uint32_t)std::max<uint64_t>(1, max_grid);
+    if (used_mode == 1)
+      k_backward<true><<<grid, block, 0, st>>>(ctx->d_views, count, total_tiles, ctx->d_ctr, ctx->faces, ck);
+    else
+      k_backward<false><<<grid, block, 0, st>>>(ctx->d_views, count, total_tiles, ctx->d_ctr, ctx->faces, ck);
+    ++ctx->launches;
+    BWD_TRY(cudaGetLastError());
+  }
+  // parameter-major outputs
+  for (uint32_t s = 0; s < n_scenes; ++s) {
+    uint64_t n = scenes[s]->n;
+    if (n == 0) continue;
+    float* dst = outs[s];
+    float* dev_out = dst;
+    if (!(flags & GT_FLAG_OUTPUT_DEVICE)) {
+      BWD_TRY(talloc((void**)&dev_out, n * GT_PARAMS_PER_PARTICLE * 4));
+      if (flags & GT_FLAG_ACCUMULATE)
+        BWD_TRY(cudaMemcpyAsync(dev_out, dst, n * GT_PARAMS_PER_PARTICLE * 4, cudaMemcpyHostToDevice, st));
+    }
+    uint64_t total = n * GT_PARAMS_PER_PARTICLE;
+    k_grad_out<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(G[s], n, dev_out, (flags & GT_FLAG_ACCUMULATE) != 0);
+    ++ctx->launches;
+    BWD_TRY(cudaGetLastError());
+    if (!(flags & GT_FLAG_OUTPUT_DEVICE))
+      BWD_TRY(cudaMemcpyAsync(dst, dev_out, n * GT_PARAMS_PER_PARTICLE * 4, cudaMemcpyDeviceToHost, st));
+  }
+  BWD_TRY(cudaEventRecord(ctx->timer1, st));
+  BWD_TRY(cudaMemcpyAsync(ctx->h_ctr, ctx->d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
+  BWD_TRY(cudaStreamSynchronize(st));
+  cudaEventElapsedTime(&bwd_ms, ctx->timer0, ctx->timer1);
+  sst = api_status_to_error(ctx, ctx->h_ctr->status);
+  if (stats) {
+    memset(stats, 0, sizeof *stats);
+    api_fill_stats(*ctx->h_ctr, stats);
+    stats->kernel_ms = bwd_ms;
+    stats->total_ms = fwd_ms + bwd_ms;
+  }
+  if (opts) {
+    opts->used_mode = used_mode;
+    opts->fwd_ms = fwd_ms;
+    opts->bwd_ms = bwd_ms;
+    opts->max_rounds = cap;
+  }
+  cleanup();
+  return sst;
+#undef BWD_TRY
+}
+
+gt_status check_bwd_view(gt_context* ctx, const gt_scene* s, const gt_uniforms* u, uint32_t w, uint32_t h,
+                         const float* dL) {
+  if (!s || s->ctx != ctx) return api_fail(ctx, GT_ERR_INVALID_ARG, "scene is NULL or from another context");
+  gt_status st = api_check_uniforms(ctx, u);
+  if (st != GT_OK) return st;
+  if (u->debug_mode != 0) return api_fail(ctx, GT_ERR_INVALID_ARG, "backward needs debug_mode 0");
+  if (!dL) return api_fail(ctx, GT_ERR_INVALID_ARG, "dL_drgba is NULL");
+  if (w == 0 || h == 0 || (uint64_t)w * h > (1ull << 31)) return api_fail(ctx, GT_ERR_INVALID_ARG, "bad image size");
+  return GT_OK;
+}
+
+}  // namespace
+
+extern "C" gt_status gt_backward(gt_context* ctx, const gt_scene* scene, const gt_uniforms* u, uint32_t w, uint32_t h,
+                                 const float* dL_drgba, float* dL_dparams, uint32_t flags, gt_bwd_opts* opts,
+                                 gt_render_stats* stats) {
+  if (!ctx) return api_fail(nullptr, GT_ERR_INVALID_ARG, "context is NULL");
+  gt_status st = check_bwd_view(ctx, scene, u, w, h, dL_drgba);
+  if (st != GT_OK) return st;
+  if (!dL_dparams && scene->n > 0) return api_fail(ctx, GT_ERR_INVALID_ARG, "dL_dparams is NULL");
+  if (flags & GT_FLAG_ASYNC) return api_fail(ctx, GT_ERR_INVALID_ARG, "gt_backward is synchronous");
+  BwdView v{scene, *u, w, h, dL_drgba};
+  return backward_impl(ctx, &v, 1, &scene, &dL_dparams, 1, flags, opts, stats);
+}
+
+extern "C" gt_status gt_backward_batch(gt_context* ctx, const gt_batch_item* items, uint32_t count,
+                                       const gt_scene* const* scenes, float* const* dL_dparams, uint32_t n_scenes,
+                                       uint32_t flags, gt_bwd_opts* opts, gt_render_stats* stats) {
+  if (!ctx) return api_fail(nullptr, GT_ERR_INVALID_ARG, "context is NULL");
+  if (count == 0) return GT_OK;
+  if (!items || !scenes || !dL_dparams || n_scenes == 0) return api_fail(ctx, GT_ERR_INVALID_ARG, "NULL argument");
+  if (flags & GT_FLAG_ASYNC) return api_fail(ctx, GT_ERR_INVALID_ARG, "gt_backward_batch is synchronous");
+  std::vector<BwdView> v(count);
+  for (uint32_t i = 0; i < count; ++i) {
+    gt_status st = check_bwd_view(ctx, items[i].scene, &items[i].u, items[i].w, items[i].h, items[i].dL_drgba);
+    if (st != GT_OK) return st;
+    uint32_t s = 0;
+    while (s < n_scenes && scenes[s] != items[i].scene) ++s;
+    if (s == n_scenes) return api_fail(ctx, GT_ERR_INVALID_ARG, "a batch item's scene is not in `scenes`");
+    v[i] = BwdView{items[i].scene, items[i].u, items[i].w, items[i].h, items[i].dL_drgba};
+  }
+  for (uint32_t s = 0; s < n_scenes; ++s)
+    if (!scenes[s] || scenes[s]->ctx != ctx || (!dL_dparams[s] && scenes[s]->n > 0))
+      return api_fail(ctx, GT_ERR_INVALID_ARG, "bad scene or gradient output");
+  return backward_impl(ctx, v.data(), count, scenes, dL_dparams, n_scenes, flags, opts, stats);
 }

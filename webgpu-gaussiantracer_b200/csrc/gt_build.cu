@@ -572,7 +572,7 @@ __global__ void k_depth(uint32_t m, const uint32_t* parent_int, const uint32_t* 
 // Shading records in particle order: (mu, opacity), precision matrix A of
 // computeResponse (6 unique entries), and the 48 SH floats made tight.
 __global__ void k_shade(const uint8_t* packed, uint64_t n, uint32_t stride, uint32_t n_sh, const uint32_t* flags,
-                        float4* shade, float4* sh) {
+                        float4* shade, float4* sh, float4* params) {
   uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (p >= n || !flags[p]) return;
   const float* rec = record(packed, p, stride);
@@ -581,6 +581,8 @@ __global__ void k_shade(const uint8_t* packed, uint64_t n, uint32_t stride, uint
   float A[3][3];
   precision_matrix(q, sc, A);
   shade[3 * p] = make_float4(rec[0], rec[1], rec[2], rec[12]);
+  params[2 * p] = make_float4(sc[0], sc[1], sc[2], 0.f);
+  params[2 * p + 1] = make_float4(q[0], q[1], q[2], q[3]);
   shade[3 * p + 1] = make_float4(A[0][0], A[1][0], A[2][0], A[1][1]);
   shade[3 * p + 2] = make_float4(A[2][1], A[2][2], 0.f, 0.f);
   float v[48];
@@ -745,6 +747,7 @@ void free_scene(SceneBuffers* b) {
   cudaFree(b->leaf_pidx);
   cudaFree(b->shade);
   cudaFree(b->sh);
+  cudaFree(b->params);
   *b = SceneBuffers{};
 }
 
@@ -763,7 +766,8 @@ Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride, double alph
   // shading records (every particle slot; only kept ones are written/read)
   GT_CUDA_TRY(cudaMalloc(&b.shade, n * 3 * sizeof(float4)));
   GT_CUDA_TRY(cudaMalloc(&b.sh, n * 12 * sizeof(float4)));
-  b.bytes += n * 15 * sizeof(float4);
+  GT_CUDA_TRY(cudaMalloc(&b.params, n * 2 * sizeof(float4)));
+  b.bytes += n * 17 * sizeof(float4);
   uint32_t *flags = nullptr, *slots = nullptr, *bounds = nullptr;
   GT_CUDA_TRY(cudaMallocAsync(&flags, n * 4, st));
   GT_CUDA_TRY(cudaMallocAsync(&slots, n * 4, st));
@@ -780,7 +784,7 @@ Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride, double alph
   GT_CUDA_TRY(cudaStreamSynchronize(st));
   uint32_t m = last_slot + last_flag;
   b.n_kept = m;
-  k_shade<<<grid_for(n, 128), 128, 0, st>>>(packed, n, stride, b.n_sh, flags, b.shade, b.sh);
+  k_shade<<<grid_for(n, 128), 128, 0, st>>>(packed, n, stride, b.n_sh, flags, b.shade, b.sh, b.params);
   ++*launches;
   if (m == 0) {
     cudaFreeAsync(flags, st);

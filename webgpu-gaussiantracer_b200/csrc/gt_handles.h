@@ -60,4 +60,5 @@ ViewDev api_make_view(const gt_scene* s, const gt_uniforms& u, uint32_t w, uint3
                       uint32_t tile_begin);
 LaunchShape api_shape_for(gt_context* ctx, const gt_scene* s, uint32_t w, uint32_t h, uint32_t k);
 void api_fill_stats(const DevCounters& c, gt_render_stats* st);
+gt_status api_ensure_views(gt_context* ctx, uint32_t n);
 }  // namespace gt

@@ -68,6 +68,7 @@ struct SceneDev {
   const uint32_t* leaf_pidx;// particle index of leaf j
   const float4* shade;      // 3 float4 per particle: (mu, opacity), (a00,a01,a02,a11), (a12,a22,-,-)
   const float4* sh;         // 12 float4 per particle: 16 RGB coefficients, tight
+  const float4* params;     // 2 float4 per particle: (scale, 0), rotation (w, x, y, z)
   uint32_t root;            // root reference (kLeafBit | j for a one-proxy scene)
   uint32_t n_kept;
   uint32_t n_sh;            // coefficients present (16 for degree-3 data)
@@ -143,6 +144,7 @@ struct SceneBuffers {
   uint32_t* leaf_pidx = nullptr;
   float4* shade = nullptr;
   float4* sh = nullptr;
+  float4* params = nullptr;  // per particle: (scale, 0), (w, x, y, z)
   uint32_t root = 0;
   uint64_t n_kept = 0;
   uint32_t depth = 0;
@@ -155,26 +157,27 @@ Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride_bytes, doubl
                 cudaStream_t stream, SceneBuffers* out, uint64_t* launches);
 void free_scene(SceneBuffers* b);
 
+// Round checkpoint written by the forward pass of gt_backward: per ray slot,
+// the number of rounds, and per round (t_curr, T) at its start and, when
+// `pidx` is set, the particle indices of its entries (kInvalid past the end).
+struct Ckpt {
+  uint32_t* nrounds = nullptr;  // [slots]
+  float2* rinfo = nullptr;      // [slots][cap]
+  uint32_t* pidx = nullptr;     // [slots][cap][kc] or null (replay mode)
+  uint32_t cap = 0;             // rounds stored per ray
+  uint32_t kc = 0;              // entries stored per round
+  uint32_t* max_rounds = nullptr;
+  uint32_t* overflow = nullptr;
+};
+
 // Trace launches (gt_trace.cu).
 Err launch_trace(const ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
                  const FaceTable& faces, const LaunchShape& shape, int num_sms, cudaStream_t stream,
-                 uint64_t* launches, ViewDev* d_views_scratch);
+                 uint64_t* launches, ViewDev* d_views_scratch, const Ckpt* ckpt = nullptr);
 Err launch_trace_hits(const ViewDev& view, ViewDev* d_views, const uint32_t* pixels, uint32_t n_pix,
                       uint32_t max_entries, uint32_t* out_pidx, float* out_t, float* out_alpha, uint32_t* out_count,
                       uint32_t* out_rounds, float4* out_rgba, DevCounters* counters, const FaceTable& faces,
                       cudaStream_t stream, uint64_t* launches);
 uint32_t kmax_for(uint32_t k);
-
-// Backward (gt_backward.cu).
-struct BwdConfig {
-  uint32_t mode;         // 1 checkpoint, 2 replay
-  uint32_t max_rounds;
-  uint32_t* ckpt_pidx;   // [rays][max_rounds][k] (checkpoint mode)
-  float* ckpt_round;     // [rays][max_rounds][2]: t_curr at round start, T at round start
-  uint32_t* ckpt_nrounds;// [rays]
-};
-Err launch_backward(const ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
-                    const FaceTable& faces, const BwdConfig& cfg, int num_sms, cudaStream_t stream,
-                    uint64_t* launches, ViewDev* d_views_scratch, cudaEvent_t mid_event);
 
 }  // namespace gt

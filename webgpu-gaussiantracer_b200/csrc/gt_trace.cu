@@ -28,264 +28,9 @@
 #include "gt_device.cuh"
 #include "gt_internal.cuh"
 #include "gt_trace_common.cuh"
+#include "gt_warp.cuh"
 
 namespace gt {
-
-constexpr int kWarpsPerBlock = 4;
-constexpr int kWarpStack = 256;  // stack entries per warp
-constexpr int kLeafQueue = 96;   // leaf queue entries per warp (<= 63 in use)
-constexpr int kMaxHitsPerProxy = 6;
-constexpr uint32_t kFull = 0xFFFFFFFFu;
-
-struct WarpScratch {
-  uint32_t snode[kWarpStack];
-  float st[kWarpStack];
-  uint32_t leafq[kLeafQueue];
-  float leaft[kLeafQueue];
-};
-
-struct HitOut {
-  uint32_t* pidx;   // [slot][max_entries]
-  float* t;
-  float* alpha;
-  uint32_t* count;  // [slot]
-  uint32_t* rounds; // [slot]
-  float4* rgba;     // [slot] or null
-  uint32_t max_entries;
-};
-
-// Warp bitonic sort of (key, val), ascending by key over the 32 lanes.
-__device__ __forceinline__ void warp_sort(float& key, uint32_t& val, uint32_t lane) {
-#pragma unroll
-  for (int k = 2; k <= 32; k <<= 1) {
-#pragma unroll
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      float ok = __shfl_xor_sync(kFull, key, j);
-      uint32_t ov = __shfl_xor_sync(kFull, val, j);
-      bool up = (lane & k) == 0;
-      bool lower = (lane & j) == 0;
-      bool take = (lower == up) ? (ok < key) : (ok > key);
-      if (take) {
-        key = ok;
-        val = ov;
-      }
-    }
-  }
-}
-
-// Sorts lanes [0, w) ascending by key, w = the power of two >= m (m <= 32);
-// keys of lanes >= m are +inf.
-__device__ __forceinline__ void warp_sort_prefix(float& key, uint32_t& val, uint32_t lane, int m) {
-  const int w = m <= 2 ? 2 : m <= 4 ? 4 : m <= 8 ? 8 : m <= 16 ? 16 : 32;
-#pragma unroll
-  for (int k = 2; k <= 32; k <<= 1) {
-    if (k > w) break;
-#pragma unroll
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      float ok = __shfl_xor_sync(kFull, key, j);
-      uint32_t ov = __shfl_xor_sync(kFull, val, j);
-      bool up = (lane & k) == 0;
-      bool lower = (lane & j) == 0;
-      bool take = (lower == up) ? (ok < key) : (ok > key);
-      if (take) {
-        key = ok;
-        val = ov;
-      }
-    }
-  }
-}
-
-// Inserts (t, p) into the warp k-buffer (lane i = i-th closest, ascending in
-// (t, particle index)).  Entries greater than the hit form a suffix.
-__device__ __forceinline__ void warp_insert(float& bt, uint32_t& bp, float t, uint32_t p, uint32_t lane) {
-  bool after = t < bt || (t == bt && p < bp);
-  uint32_t m = __ballot_sync(kFull, after);
-  if (m) {
-    int pos = __ffs(m) - 1;
-    float ut = __shfl_up_sync(kFull, bt, 1);
-    uint32_t up = __shfl_up_sync(kFull, bp, 1);
-    if ((int)lane > pos) {
-      bt = ut;
-      bp = up;
-    }
-    if ((int)lane == pos) {
-      bt = t;
-      bp = p;
-    }
-  }
-}
-
-// Modes of one traversal.
-enum TraverseMode { kCollect = 0, kClosestAny = 1, kCountFront = 2 };
-
-// Warp-cooperative traversal from the root with interval (tlo, t_max).
-//   kCollect:    the 32 closest front-face hits go into (bt, bp)
-//   kClosestAny: the closest hit of any facing goes into lane 0 of (bt, bp)
-//   kCountFront: every front-face hit is counted into *count
-// Far bound of the box tests: the buffer's last entry (kCollect), its first
-// entry (kClosestAny) or t_max (kCountFront).
-template <int MODE>
-__device__ __forceinline__ void traverse8(const SceneDev& S, const FaceTable& F, WarpScratch& W, V3 o, V3 d,
-                                          const BoxRay& br, float tlo, float t_max, float& bt, uint32_t& bp,
-                                          uint32_t* count, RayStats& st, uint32_t& status, uint32_t lane) {
-  if (S.n_kept == 0) return;
-  const uint32_t lt_mask = (1u << lane) - 1u;
-  const int cull_lane = MODE == kClosestAny ? 0 : 31;
-  int sp = 0, nq = 0;
-  if (lane == 0) {
-    W.snode[0] = 0;
-    W.st[0] = -CUDART_INF_F;
-  }
-  sp = 1;
-  __syncwarp();
-  float thi = MODE == kCountFront ? t_max : __shfl_sync(kFull, bt, cull_lane);
-  uint32_t iters = 0;
-  const uint32_t max_iters = 4u * S.n_kept + 64u;
-  while (true) {
-    if (++iters > max_iters) {
-      status |= kStatusVisitCap;
-      return;
-    }
-    // pop up to 4 nodes still in range (kept in registers: no indexed array)
-    uint32_t pn0 = 0, pn1 = 0, pn2 = 0, pn3 = 0;
-    int np = 0;
-    while (np < 4 && sp > 0) {
-      --sp;
-      float t = W.st[sp];
-      uint32_t n = W.snode[sp];
-      if (t <= thi) {
-        pn3 = pn2;
-        pn2 = pn1;
-        pn1 = pn0;
-        pn0 = n;
-        ++np;
-      }
-    }
-    __syncwarp();
-    if (np > 0) {
-      const int slot = (int)(lane >> 3);
-      const bool valid = slot < np;
-      uint32_t node = slot == 0 ? pn0 : slot == 1 ? pn1 : slot == 2 ? pn2 : pn3;
-      float tnear = CUDART_INF_F;
-      uint32_t ref = kInvalid;
-      bool hit = false;
-      if (valid) {
-        const float4* rec = S.nodes8 + 16 * (size_t)node + 2 * (lane & 7);
-        float4 a = __ldg(rec), b = __ldg(rec + 1);
-        ref = __float_as_uint(b.z);
-        float x0 = __fmaf_rn(a.x, br.ix, -br.ox), x1 = __fmaf_rn(a.w, br.ix, -br.ox);
-        float y0 = __fmaf_rn(a.y, br.iy, -br.oy), y1 = __fmaf_rn(b.x, br.iy, -br.oy);
-        float z0 = __fmaf_rn(a.z, br.iz, -br.oz), z1 = __fmaf_rn(b.y, br.iz, -br.oz);
-        float tn = fmaxf(fmaxf(fminf(x0, x1) - br.px, fminf(y0, y1) - br.py), fmaxf(fminf(z0, z1) - br.pz, tlo));
-        float tf = fminf(fminf(fmaxf(x0, x1) + br.px, fmaxf(y0, y1) + br.py), fminf(fmaxf(z0, z1) + br.pz, thi));
-        hit = ref != kInvalid && tn <= tf;
-        tnear = tn;
-      }
-      st.node_visits += (lane & 7) == 0 && valid ? 1u : 0u;
-      const bool leaf = (ref & kLeafBit) != 0;
-      const uint32_t lmask = __ballot_sync(kFull, hit && leaf);
-      const uint32_t imask = __ballot_sync(kFull, hit && !leaf);
-      if (lmask) {
-        if (hit && leaf) {
-          int q = nq + __popc(lmask & lt_mask);
-          W.leafq[q] = ref & ~kLeafBit;
-          W.leaft[q] = tnear;
-        }
-        nq += __popc(lmask);
-      }
-      if (imask) {
-        const int m = __popc(imask);
-        if (sp + m > kWarpStack) {
-          status |= kStatusStackOverflow;
-          return;
-        }
-        // gather the m hit children into lanes 0..m-1, then sort that segment
-        const uint32_t src = (int)lane < m ? __fns(imask, 0, (int)lane + 1) : lane;
-        float key = __shfl_sync(kFull, tnear, src);
-        uint32_t val = __shfl_sync(kFull, ref, src);
-        if ((int)lane >= m) key = CUDART_INF_F;
-        if (m > 1) warp_sort_prefix(key, val, lane, m);
-        if ((int)lane < m) {
-          W.snode[sp + m - 1 - (int)lane] = val;
-          W.st[sp + m - 1 - (int)lane] = key;
-        }
-        sp += m;
-      }
-      __syncwarp();
-    }
-    const bool drain = sp == 0;
-    if (nq >= 32 || (drain && nq > 0)) {
-      const int nb = nq < 32 ? nq : 32;
-      uint32_t j = 0;
-      bool have = (int)lane < nb;
-      if (have) {
-        j = W.leafq[lane];
-        have = W.leaft[lane] <= thi;
-      }
-      __syncwarp();
-      if (nq > nb) {  // keep the rest (at most 31 entries) at the front of the queue
-        uint32_t qj = 0;
-        float qt = 0.f;
-        bool mv = (int)lane < nq - nb;
-        if (mv) {
-          qj = W.leafq[nb + lane];
-          qt = W.leaft[nb + lane];
-        }
-        __syncwarp();
-        if (mv) {
-          W.leafq[lane] = qj;
-          W.leaft[lane] = qt;
-        }
-        __syncwarp();
-      }
-      nq -= nb;
-      // one proxy per lane; its hits are kept in a register queue h0..h5
-      float h0 = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, h4 = 0.f, h5 = 0.f;
-      int nh = 0;
-      if (have) {
-        ++st.proxy_tests;
-        const float tb = MODE == kCountFront ? t_max : fminf(next_up(thi), t_max);
-        proxy_test<MODE != kClosestAny>(F, S.w2o, j, o, d, tlo, tb, [&](float t, int) {
-          h5 = h4;
-          h4 = h3;
-          h3 = h2;
-          h2 = h1;
-          h1 = h0;
-          h0 = t;
-          ++nh;
-        });
-        if (nh > kMaxHitsPerProxy) {
-          status |= kStatusHitOverflow;
-          nh = kMaxHitsPerProxy;
-        }
-      }
-      if (MODE == kCountFront) {
-        st.anyhits += nh;
-      } else {
-        uint32_t p = nh ? __ldg(S.leaf_pidx + j) : 0u;
-        st.anyhits += nh;
-        while (true) {
-          uint32_t pend = __ballot_sync(kFull, nh > 0);
-          if (!pend) break;
-          int src = __ffs(pend) - 1;
-          float t = __shfl_sync(kFull, h0, src);
-          uint32_t pp = __shfl_sync(kFull, p, src);
-          if ((int)lane == src) {
-            h0 = h1;
-            h1 = h2;
-            h2 = h3;
-            h3 = h4;
-            h4 = h5;
-            --nh;
-          }
-          warp_insert(bt, bp, t, pp, lane);
-        }
-        thi = __shfl_sync(kFull, bt, cull_lane);
-      }
-    }
-    if (sp == 0 && nq == 0) break;
-  }
-}
 
 // Per-ray state (identical in all lanes).
 struct WRay {
@@ -300,10 +45,12 @@ __device__ __forceinline__ bool wray_more(const ViewDev& V, const WRay& R) {
 }
 
 // tracePath (src/GS_shader.ts:192-273) for one pixel, by one warp.
-template <bool RECORD>
+// RECORD: write the composited hit sequence (gt_render_hits).
+// CKPT: write the round checkpoint the adjoint replays (gt_backward).
+template <bool RECORD, bool CKPT>
 __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTable& F, WarpScratch& W, uint32_t px,
                                                  uint32_t py, RayStats& st, uint32_t& status, uint32_t lane,
-                                                 const HitOut& ho, uint32_t slot) {
+                                                 const HitOut& ho, uint32_t slot, const Ckpt& ck) {
   WRay R;
   ray_gen(V.u, V.w, V.h, px, py, R.o, R.d);
   R.br = make_boxray(R.o, R.d, V.s.scene_mag);
@@ -358,10 +105,8 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
     float bt = t_max;
     uint32_t bp = kInvalid;
     traverse8<kCollect>(V.s, F, W, R.o, R.d, R.br, R.t_curr, t_max, bt, bp, nullptr, st, status, lane);
-    if (status & (kStatusStackOverflow | kStatusVisitCap | kStatusHitOverflow)) {
-      status = __reduce_or_sync(kFull, status);
-      break;
-    }
+    // status bits may be set in single lanes: reduce before branching on them
+    if (__reduce_or_sync(kFull, status) & (kStatusStackOverflow | kStatusVisitCap | kStatusHitOverflow)) break;
     const uint32_t cnt = __popc(__ballot_sync(kFull, bp != kInvalid));
     const bool complete = cnt < 32u;
     // rounds served from this buffer
@@ -369,9 +114,17 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
       const uint32_t skip = __popc(__ballot_sync(kFull, bp != kInvalid && !(bt > R.t_curr)));
       const uint32_t avail = cnt - skip;
       if (!complete && avail < k) break;  // the next round reaches past the buffer
+      const uint32_t n = avail < k ? avail : k;
+      if (CKPT && R.step < ck.cap) {
+        const size_t at = (size_t)slot * ck.cap + R.step;
+        if (lane == 0) ck.rinfo[at] = make_float2(R.t_curr, R.T);
+        if (ck.pidx) {
+          uint32_t v = __shfl_sync(kFull, bp, (int)((skip + lane) & 31u));
+          if (lane < ck.kc) ck.pidx[at * ck.kc + lane] = lane < n ? v : kInvalid;
+        }
+      }
       ++R.step;
       st.rounds += lane == 0 ? 1u : 0u;
-      const uint32_t n = avail < k ? avail : k;
       float new_t = n == k ? __shfl_sync(kFull, bt, (int)(skip + k - 1)) + 1e-4f : t_max;
       // lanes skip..skip+n-1 hold this round's entries
       const bool mine = lane >= skip && lane < skip + n;
@@ -429,18 +182,25 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
     ho.count[slot] = R.n_entries;
     ho.rounds[slot] = R.step;
   }
+  if (CKPT && lane == 0) {
+    ck.nrounds[slot] = R.step;
+    if (R.step > ck.cap) {
+      atomicOr(ck.overflow, 1u);
+      atomicMax(ck.max_rounds, R.step);
+    }
+  }
   return make_float4(R.L0, R.L1, R.L2, 1.0f);
 }
 
 // Persistent kernel: each warp takes one pixel slot at a time from a global
 // counter (slot = 32 * tile + position in the 8x4 tile, views back to back),
 // so neighbouring pixels run on neighbouring warps at the same time.
-template <bool RECORD>
+template <bool RECORD, bool CKPT>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_trace8(const ViewDev* __restrict__ views, uint32_t n_views,
                                                                   uint32_t total_tiles, DevCounters* ctr,
                                                                   const __grid_constant__ FaceTable F,
                                                                   const uint32_t* pixels, uint32_t n_pix,
-                                                                  const HitOut ho) {
+                                                                  const HitOut ho, const Ckpt ck) {
   __shared__ WarpScratch scratch[kWarpsPerBlock];
   const uint32_t lane = threadIdx.x & 31;
   WarpScratch& W = scratch[threadIdx.x >> 5];
@@ -469,7 +229,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_trace8(const ViewDev
       if (px >= V.w || py >= V.h) continue;
     }
     const ViewDev& V = views[vi];
-    float4 r = trace_ray_warp<RECORD>(V, F, W, px, py, st, status, lane, ho, item);
+    float4 r = trace_ray_warp<RECORD, CKPT>(V, F, W, px, py, st, status, lane, ho, item, ck);
     if (lane == 0) {
       if (RECORD) {
         if (ho.rgba) ho.rgba[item] = r;
@@ -486,7 +246,7 @@ uint32_t kmax_for(uint32_t k) { return k <= 8 ? 8u : (k <= 16 ? 16u : 32u); }
 
 Err launch_trace(const ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
                   const FaceTable& faces, const LaunchShape& shape, int num_sms, cudaStream_t stream,
-                  uint64_t* launches, ViewDev* d_views) {
+                  uint64_t* launches, ViewDev* d_views, const Ckpt* ckpt) {
   GT_CUDA_TRY(cudaMemcpyAsync(d_views, views, sizeof(ViewDev) * n_views, cudaMemcpyHostToDevice, stream));
   uint32_t block = kWarpsPerBlock * 32;
   uint32_t grid = (uint32_t)num_sms * std::max(1u, shape.blocks_per_sm);
@@ -494,7 +254,12 @@ Err launch_trace(const ViewDev* views, uint32_t n_views, uint32_t total_tiles, D
   uint64_t max_grid = (warps_needed + kWarpsPerBlock - 1) / kWarpsPerBlock;
   if (grid > max_grid) grid = (uint32_t)std::max<uint64_t>(1, max_grid);
   HitOut ho{};
-  k_trace8<false><<<grid, block, 0, stream>>>(d_views, n_views, total_tiles, counters, faces, nullptr, 0u, ho);
+  if (ckpt)
+    k_trace8<false, true><<<grid, block, 0, stream>>>(d_views, n_views, total_tiles, counters, faces, nullptr, 0u, ho,
+                                                      *ckpt);
+  else
+    k_trace8<false, false><<<grid, block, 0, stream>>>(d_views, n_views, total_tiles, counters, faces, nullptr, 0u, ho,
+                                                       Ckpt{});
   ++*launches;
   GT_CUDA_TRY(cudaGetLastError());
   return Err{};
@@ -508,7 +273,8 @@ Err launch_trace_hits(const ViewDev& view, ViewDev* d_views, const uint32_t* pix
   GT_CUDA_TRY(cudaMemcpyAsync(d_views, &view, sizeof(ViewDev), cudaMemcpyHostToDevice, stream));
   HitOut ho{out_pidx, out_t, out_alpha, out_count, out_rounds, out_rgba, max_entries};
   uint32_t grid = std::min<uint32_t>((n_pix + kWarpsPerBlock - 1) / kWarpsPerBlock, 148u * 8u);
-  k_trace8<true><<<grid, kWarpsPerBlock * 32, 0, stream>>>(d_views, 1, 0, counters, faces, pixels, n_pix, ho);
+  k_trace8<true, false><<<grid, kWarpsPerBlock * 32, 0, stream>>>(d_views, 1, 0, counters, faces, pixels, n_pix, ho,
+                                                                  Ckpt{});
   ++*launches;
   GT_CUDA_TRY(cudaGetLastError());
   return Err{};

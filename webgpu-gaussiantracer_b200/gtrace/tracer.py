@@ -133,8 +133,37 @@ class Context:
                                          g.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p), flags,
                                          C.byref(opts), C.byref(st)))
         info = st.as_dict()
-        info.update(used_mode=opts.used_mode, fwd_ms=opts.fwd_ms, bwd_ms=opts.bwd_ms)
+        info.update(used_mode=opts.used_mode, fwd_ms=opts.fwd_ms, bwd_ms=opts.bwd_ms, max_rounds=opts.max_rounds)
         return out, info
+
+    def backward_batch(self, views, mode: int = 0, max_rounds: int = 0, mem_budget: int = 0):
+        """views: list of (scene, uniforms, width, height, dL_drgba) -> {scene: (59 x n) gradient}, info.
+        Gradients of all views of a scene are summed in one adjoint launch."""
+        items = (L.BatchItem * len(views))()
+        keep = []
+        scenes = []
+        for i, (scene, uniforms, w, h, g) in enumerate(views):
+            ga = np.ascontiguousarray(g, dtype=np.float32)
+            if ga.size != w * h * 4:
+                raise ValueError("dL_drgba must hold width*height*4 values")
+            keep.append(ga)
+            items[i].scene = scene.handle
+            items[i].u = _uniforms(uniforms)
+            items[i].w, items[i].h = w, h
+            items[i].out_rgba = None
+            items[i].dL_drgba = ga.ctypes.data
+            if scene not in scenes:
+                scenes.append(scene)
+        outs = [np.zeros((59, s.n), dtype=np.float32) for s in scenes]
+        sc = (C.c_void_p * len(scenes))(*[s.handle.value for s in scenes])
+        op = (C.c_void_p * len(scenes))(*[o.ctypes.data for o in outs])
+        opts = L.BwdOpts(mode, max_rounds, mem_budget, 0, 0, 0.0, 0.0)
+        st = L.RenderStats()
+        self.check(self._lib.gt_backward_batch(self._h, items, len(views), sc, op, len(scenes), 0, C.byref(opts),
+                                               C.byref(st)))
+        info = st.as_dict()
+        info.update(used_mode=opts.used_mode, fwd_ms=opts.fwd_ms, bwd_ms=opts.bwd_ms, max_rounds=opts.max_rounds)
+        return dict(zip(scenes, outs)), info
 
     def render_batch(self, views, outs=None, device_outputs=False, asynchronous=False):
         """views: list of (scene, uniforms, width, height[, out]) -> list of outputs, stats."""
