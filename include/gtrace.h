@@ -58,6 +58,8 @@ enum {
 #define GT_FLAG_OUTPUT_DEVICE  0x2u  /* output buffers are device pointers    */
 #define GT_FLAG_ASYNC          0x4u  /* do not wait (device buffers only)     */
 #define GT_FLAG_ACCUMULATE     0x8u  /* backward: add into dL_dparams         */
+#define GT_FLAG_CHECKPOINT     0x10u /* render: keep the round checkpoint in the context;
+                                        backward: reuse it when the views match  */
 
 /* -------------------------------------------------------- opaque handles */
 typedef struct gt_context gt_context;
@@ -205,7 +207,9 @@ typedef struct gt_bwd_opts {
  *                (coefficient c, channel ch at row 11 + 3*c + ch).  Particles
  *                without a proxy get 0.  Overwritten unless GT_FLAG_ACCUMULATE.
  *   flags        GT_FLAG_INPUT_DEVICE (dL_drgba), GT_FLAG_OUTPUT_DEVICE
- *                (dL_dparams), GT_FLAG_ACCUMULATE
+ *                (dL_dparams), GT_FLAG_ACCUMULATE, GT_FLAG_CHECKPOINT (skip the
+ *                checkpointing forward when the last gt_render/gt_render_batch
+ *                call with GT_FLAG_CHECKPOINT rendered exactly these views)
  * Hit sets are held fixed (the proxy geometry is piecewise constant); the
  * response, opacity, SH colour and compositing are differentiated exactly. */
 gt_status gt_backward(gt_context* ctx, const gt_scene* scene, const gt_uniforms* u,
@@ -254,6 +258,14 @@ gt_status gt_backward_batch(gt_context* ctx, const gt_batch_item* items, uint32_
                             const gt_scene* const* scenes, float* const* dL_dparams,
                             uint32_t n_scenes, uint32_t flags, gt_bwd_opts* opts,
                             gt_render_stats* stats);
+
+/* L2 image loss for the differentiable path: loss = sum over pixels of
+ * |rgb - target_rgb|^2 (A ignored), dL_drgba = 2 (rgb - target), A = 0.
+ * All three image buffers are device buffers of n_pixels * 4 floats; `loss`
+ * (host, optional) receives the sum in double.  No counterpart in the
+ * reference. */
+gt_status gt_l2_loss(gt_context* ctx, const float* rgba, const float* target, uint64_t n_pixels,
+                     float* dL_drgba, double* loss);
 
 /* ============================================================ tuning
  * No counterpart in the reference.  Times the tracer's launch shapes on the

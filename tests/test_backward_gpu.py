@@ -99,3 +99,46 @@ def test_batch_sums_views_and_accumulate_flag(ctx):
     acc = a.copy()
     acc2, _ = ctx.backward(s, v2.uniforms, 20, 36, g2, out=acc, accumulate=True)
     np.testing.assert_allclose(acc2, a + b, rtol=1e-5, atol=1e-6 * np.abs(a + b).max())
+
+
+def test_render_checkpoint_reused_by_backward(ctx):
+    """A render with GT_FLAG_CHECKPOINT leaves the round checkpoint in the
+    context; the following backward of the same view skips its own forward."""
+    pg = small_scene(n=1500, seed=44)
+    s = Scene(ctx, pg.gaussiansBuffer, 0.01)
+    w, h = 36, 28
+    v = view(w, h, k=8)
+    g = np.random.default_rng(9).normal(size=(h, w, 4)).astype(np.float32)
+    plain = ctx.render(s, v.uniforms, w, h)
+    img = ctx.render(s, v.uniforms, w, h, checkpoint=True)
+    np.testing.assert_array_equal(img, plain)
+    a, ia = ctx.backward(s, v.uniforms, w, h, g, reuse_checkpoint=True)
+    assert ia["fwd_ms"] == 0.0
+    b, ib = ctx.backward(s, v.uniforms, w, h, g)
+    assert ib["fwd_ms"] > 0.0
+    np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-6 * np.abs(b).max())
+    # a different view does not reuse the stored checkpoint
+    v2 = view(w, h, pos=(0.3, 0.2, 4.0), k=8)
+    c, ic = ctx.backward(s, v2.uniforms, w, h, g, reuse_checkpoint=True)
+    assert ic["fwd_ms"] > 0.0
+
+
+def test_l2_loss_helper(ctx):
+    n = 1000
+    rng = np.random.default_rng(1)
+    a = rng.normal(size=(n, 4)).astype(np.float32)
+    b = rng.normal(size=(n, 4)).astype(np.float32)
+    da, db, dg = (ctx.device_alloc(n * 16) for _ in range(3))
+    try:
+        ctx.memcpy(da, a.ctypes.data, n * 16, 0)
+        ctx.memcpy(db, b.ctypes.data, n * 16, 0)
+        loss = ctx.l2_loss(da, db, n, dg)
+        g = np.zeros((n, 4), np.float32)
+        ctx.memcpy(g.ctypes.data, dg, n * 16, 1)
+    finally:
+        for p in (da, db, dg):
+            ctx.device_free(p)
+    d = a[:, :3].astype(np.float64) - b[:, :3]
+    assert abs(loss - (d ** 2).sum()) <= 1e-6 * (d ** 2).sum()
+    np.testing.assert_allclose(g[:, :3], 2 * (a[:, :3] - b[:, :3]), rtol=1e-6)
+    assert (g[:, 3] == 0).all()

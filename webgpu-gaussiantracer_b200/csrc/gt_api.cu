@@ -228,6 +228,7 @@ extern "C" gt_status gt_context_destroy(gt_context* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   drop_graphs(ctx);
+  api_free_ckpt(ctx);
   for (gt_scene* s : ctx->scenes) {
     free_scene(&s->b);
     delete s;
@@ -359,6 +360,19 @@ extern "C" gt_status gt_render(gt_context* ctx, const gt_scene* scene, const gt_
     if (st != GT_OK) return st;
     out = ctx->staging;
   }
+  if (flags & GT_FLAG_CHECKPOINT) {
+    if (flags & GT_FLAG_ASYNC) return fail(ctx, GT_ERR_INVALID_ARG, "a checkpointing render is synchronous");
+    if (u->debug_mode != 0) return fail(ctx, GT_ERR_INVALID_ARG, "checkpointing needs debug_mode 0");
+    API_CUDA(ctx, cudaEventRecord(ctx->call0, ctx->stream));
+    st = api_forward_ckpt(ctx, &scene, u, &w, &h, &out, 1, 0, 0, 0, stats);
+    if (st != GT_OK) return st;
+    if (!(flags & GT_FLAG_OUTPUT_DEVICE))
+      API_CUDA(ctx, cudaMemcpyAsync(out_rgba, out, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    API_CUDA(ctx, cudaEventRecord(ctx->call1, ctx->stream));
+    API_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (stats) cudaEventElapsedTime(&stats->total_ms, ctx->call0, ctx->call1);
+    return GT_OK;
+  }
   st = ensure_views(ctx, 1);
   if (st != GT_OK) return st;
   ViewDev v = make_view(scene, *u, w, h, out, 0);
@@ -471,6 +485,31 @@ extern "C" gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items
   if (!(flags & GT_FLAG_OUTPUT_DEVICE)) {
     st = ensure_staging(ctx, staging * sizeof(float4));
     if (st != GT_OK) return st;
+  }
+  if (flags & GT_FLAG_CHECKPOINT) {
+    if (flags & GT_FLAG_ASYNC) return fail(ctx, GT_ERR_INVALID_ARG, "a checkpointing render is synchronous");
+    std::vector<const gt_scene*> sc(count);
+    std::vector<gt_uniforms> us(count);
+    std::vector<uint32_t> ws(count), hs(count);
+    std::vector<float4*> os(count);
+    size_t o = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+      if (items[i].u.debug_mode != 0) return fail(ctx, GT_ERR_INVALID_ARG, "checkpointing needs debug_mode 0");
+      sc[i] = items[i].scene;
+      us[i] = items[i].u;
+      ws[i] = items[i].w;
+      hs[i] = items[i].h;
+      os[i] = (flags & GT_FLAG_OUTPUT_DEVICE) ? reinterpret_cast<float4*>(items[i].out_rgba) : ctx->staging + o;
+      o += (size_t)items[i].w * items[i].h;
+    }
+    st = api_forward_ckpt(ctx, sc.data(), us.data(), ws.data(), hs.data(), os.data(), count, 0, 0, 0, stats);
+    if (st != GT_OK) return st;
+    if (!(flags & GT_FLAG_OUTPUT_DEVICE))
+      for (uint32_t i = 0; i < count; ++i)
+        API_CUDA(ctx, cudaMemcpyAsync(items[i].out_rgba, os[i], (size_t)ws[i] * hs[i] * sizeof(float4),
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    API_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return GT_OK;
   }
   size_t off = 0;
   for (uint32_t i = 0; i < count; ++i) {

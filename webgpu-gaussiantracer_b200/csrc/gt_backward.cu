@@ -296,6 +296,26 @@ __global__ void k_grad_out(const float* G, uint64_t n, float* out, bool accumula
   out[idx] = accumulate ? out[idx] + v : v;
 }
 
+// Writes the L2 loss gradient and per-block partial sums of the loss.
+__global__ void k_l2_loss(const float4* rgba, const float4* target, uint64_t n, float4* dL, double* partial) {
+  __shared__ double red[256];
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (i < n) {
+    float4 a = rgba[i], b = target[i];
+    float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
+    dL[i] = make_float4(2.f * dx, 2.f * dy, 2.f * dz, 0.f);
+    v = (double)dx * dx + (double)dy * dy + (double)dz * dz;
+  }
+  red[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+}
+
 }  // namespace gt
 
 using namespace gt;
@@ -309,12 +329,140 @@ struct BwdView {
   const float* dL;
 };
 
+#define CK_TRY(expr)                                                                                     \
+  do {                                                                                                   \
+    cudaError_t e_ = (expr);                                                                             \
+    if (e_ != cudaSuccess)                                                                               \
+      return api_fail(ctx, e_ == cudaErrorMemoryAllocation ? GT_ERR_OOM : GT_ERR_CUDA,                     \
+                      std::string(#expr) + ": " + cudaGetErrorString(e_));                               \
+  } while (0)
+
+// Grows a context-owned device buffer to at least `bytes`.
+gt_status grow(gt_context* ctx, void** p, size_t* have, size_t bytes) {
+  if (*have >= bytes) return GT_OK;
+  cudaFree(*p);
+  *p = nullptr;
+  *have = 0;
+  CK_TRY(cudaMalloc(p, bytes ? bytes : 16));
+  *have = bytes;
+  return GT_OK;
+}
+
+bool key_matches(const CkptStore& ck, const BwdView* v, uint32_t count) {
+  if (!ck.valid || ck.key.size() != count) return false;
+  for (uint32_t i = 0; i < count; ++i) {
+    const CkptKey& k = ck.key[i];
+    if (k.scene != v[i].scene || k.w != v[i].w || k.h != v[i].h || memcmp(&k.u, &v[i].u, sizeof(gt_uniforms)) != 0)
+      return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+namespace gt {
+
+void api_free_ckpt(gt_context* ctx) {
+  CkptStore& c = ctx->ckpt;
+  cudaFree(c.nrounds);
+  cudaFree(c.rinfo);
+  cudaFree(c.pidx);
+  cudaFree(c.misc);
+  c = CkptStore{};
+}
+
+// Checkpointing forward: renders the views into `outs` and keeps, per ray
+// slot, the round count and per round (t_curr, T) at its start, plus the
+// round's particle indices in checkpoint mode (mode 1) — chosen when they
+// fit in `budget` bytes, or forced by `mode`.  A ray with more rounds than
+// the capacity sets an overflow flag; the capacity then grows to the
+// deepest ray and the forward runs again.
+gt_status api_forward_ckpt(gt_context* ctx, const gt_scene* const* scenes, const gt_uniforms* us, const uint32_t* ws,
+                           const uint32_t* hs, float4* const* outs, uint32_t count, uint32_t mode, uint32_t cap,
+                           uint64_t budget, gt_render_stats* stats) {
+  CkptStore& ck = ctx->ckpt;
+  ck.valid = false;
+  cudaStream_t st = ctx->stream;
+  gt_status sst = api_ensure_views(ctx, count);
+  if (sst != GT_OK) return sst;
+  std::vector<ViewDev> vd(count);
+  uint32_t total_tiles = 0, kc = 1;
+  for (uint32_t i = 0; i < count; ++i) {
+    vd[i] = api_make_view(scenes[i], us[i], ws[i], hs[i], outs[i], total_tiles);
+    total_tiles += vd[i].n_tiles;
+    kc = std::max(kc, us[i].k);
+  }
+  const uint64_t slots = (uint64_t)total_tiles * 32u;
+  if (cap == 0) cap = ck.cap ? ck.cap : 16u;
+  if (budget == 0) {
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    budget = free_b / 2;
+  }
+  if (!ck.misc) CK_TRY(cudaMalloc(&ck.misc, 8));
+  LaunchShape shape = api_shape_for(ctx, scenes[0], ws[0], hs[0], us[0].k);
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    uint64_t need_replay = slots * (4 + (uint64_t)cap * 8);
+    uint64_t need_pidx = slots * (uint64_t)cap * kc * 4;
+    uint32_t m = mode == 1 ? 1u : (mode == 2 ? 2u : (need_replay + need_pidx <= budget ? 1u : 2u));
+    sst = grow(ctx, (void**)&ck.nrounds, &ck.nrounds_bytes, slots * 4);
+    if (sst == GT_OK) sst = grow(ctx, (void**)&ck.rinfo, &ck.rinfo_bytes, slots * (size_t)cap * sizeof(float2));
+    if (sst == GT_OK && m == 1) sst = grow(ctx, (void**)&ck.pidx, &ck.pidx_bytes, slots * (size_t)cap * kc * 4);
+    if (sst != GT_OK) return sst;
+    Ckpt c;
+    c.nrounds = ck.nrounds;
+    c.rinfo = ck.rinfo;
+    c.pidx = m == 1 ? ck.pidx : nullptr;
+    c.cap = cap;
+    c.kc = kc;
+    c.max_rounds = ck.misc;
+    c.overflow = ck.misc + 1;
+    CK_TRY(cudaMemsetAsync(ck.nrounds, 0, slots * 4, st));
+    CK_TRY(cudaMemsetAsync(ck.misc, 0, 8, st));
+    CK_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), st));
+    CK_TRY(cudaEventRecord(ctx->timer0, st));
+    Err e = launch_trace(vd.data(), count, total_tiles, ctx->d_ctr, ctx->faces, shape, ctx->num_sms, st,
+                         &ctx->launches, ctx->d_views, &c);
+    if (e.code != GT_OK) return api_fail(ctx, e.code, e.msg);
+    CK_TRY(cudaEventRecord(ctx->timer1, st));
+    uint32_t misc[2];
+    CK_TRY(cudaMemcpyAsync(misc, ck.misc, 8, cudaMemcpyDeviceToHost, st));
+    CK_TRY(cudaMemcpyAsync(ctx->h_ctr, ctx->d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
+    CK_TRY(cudaStreamSynchronize(st));
+    cudaEventElapsedTime(&ck.fwd_ms, ctx->timer0, ctx->timer1);
+    sst = api_status_to_error(ctx, ctx->h_ctr->status);
+    if (sst != GT_OK) return sst;
+    if (stats) {
+      memset(stats, 0, sizeof *stats);
+      api_fill_stats(*ctx->h_ctr, stats);
+      stats->kernel_ms = ck.fwd_ms;
+      stats->total_ms = ck.fwd_ms;
+    }
+    if (!misc[1]) {
+      ck.slots = slots;
+      ck.cap = cap;
+      ck.kc = kc;
+      ck.mode = m;
+      ck.total_tiles = total_tiles;
+      ck.key.resize(count);
+      for (uint32_t i = 0; i < count; ++i) ck.key[i] = CkptKey{scenes[i], us[i], ws[i], hs[i]};
+      ck.valid = true;
+      return GT_OK;
+    }
+    cap = std::max(misc[0], 2 * cap);
+  }
+  return api_fail(ctx, GT_ERR_DEVICE_TIMEOUT, "checkpoint capacity exceeded");
+}
+
+}  // namespace gt
+
+namespace {
+
 gt_status backward_impl(gt_context* ctx, const BwdView* views, uint32_t count, const gt_scene* const* scenes,
                         float* const* outs, uint32_t n_scenes, uint32_t flags, gt_bwd_opts* opts,
                         gt_render_stats* stats) {
   if (count == 0) return GT_OK;
-  cudaError_t ce = cudaSetDevice(ctx->device);
-  if (ce != cudaSuccess) return api_fail(ctx, GT_ERR_CUDA, cudaGetErrorString(ce));
+  CK_TRY(cudaSetDevice(ctx->device));
   cudaStream_t st = ctx->stream;
   std::vector<void*> temps;
   auto cleanup = [&]() {
@@ -335,29 +483,58 @@ gt_status backward_impl(gt_context* ctx, const BwdView* views, uint32_t count, c
                       std::string(#expr) + ": " + cudaGetErrorString(e_));                                \
     }                                                                                                     \
   } while (0)
-  // per-scene accumulation buffers
-  std::vector<float*> G(n_scenes, nullptr);
-  for (uint32_t s = 0; s < n_scenes; ++s) {
-    uint64_t n = scenes[s]->n;
-    BWD_TRY(talloc((void**)&G[s], (size_t)std::max<uint64_t>(n, 1) * kGradStride * 4));
-    BWD_TRY(cudaMemsetAsync(G[s], 0, (size_t)std::max<uint64_t>(n, 1) * kGradStride * 4, st));
-  }
-  // view table: outputs go to scratch images; dL on the device
-  uint32_t total_tiles = 0, kc = 1;
   size_t pixels = 0;
   for (uint32_t i = 0; i < count; ++i) pixels += (size_t)views[i].w * views[i].h;
-  float4* img = nullptr;
+  // 1. the checkpointing forward, unless the context holds it for these views
+  float fwd_ms = 0.f;
+  const bool reuse = (flags & GT_FLAG_CHECKPOINT) && key_matches(ctx->ckpt, views, count);
+  if (!reuse) {
+    float4* img = nullptr;
+    BWD_TRY(talloc((void**)&img, pixels * sizeof(float4)));
+    std::vector<const gt_scene*> sc(count);
+    std::vector<gt_uniforms> us(count);
+    std::vector<uint32_t> ws(count), hs(count);
+    std::vector<float4*> os(count);
+    size_t off = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+      sc[i] = views[i].scene;
+      us[i] = views[i].u;
+      ws[i] = views[i].w;
+      hs[i] = views[i].h;
+      os[i] = img + off;
+      off += (size_t)views[i].w * views[i].h;
+    }
+    gt_status sst = api_forward_ckpt(ctx, sc.data(), us.data(), ws.data(), hs.data(), os.data(), count,
+                                     opts ? opts->mode : 0u, opts ? opts->max_rounds : 0u,
+                                     opts ? opts->mem_budget : 0ull, nullptr);
+    if (sst != GT_OK) {
+      cleanup();
+      return sst;
+    }
+    fwd_ms = ctx->ckpt.fwd_ms;
+  }
+  const CkptStore& cs = ctx->ckpt;
+  // 2. per-scene accumulation buffers, dL on the device, the adjoint's view table
+  std::vector<float*> G(n_scenes, nullptr);
+  for (uint32_t s = 0; s < n_scenes; ++s) {
+    uint64_t n = std::max<uint64_t>(scenes[s]->n, 1);
+    BWD_TRY(talloc((void**)&G[s], (size_t)n * kGradStride * 4));
+    BWD_TRY(cudaMemsetAsync(G[s], 0, (size_t)n * kGradStride * 4, st));
+  }
   float4* dl_dev = nullptr;
-  BWD_TRY(talloc((void**)&img, pixels * sizeof(float4)));
   if (!(flags & GT_FLAG_INPUT_DEVICE)) BWD_TRY(talloc((void**)&dl_dev, pixels * sizeof(float4)));
-  gt_status sst = GT_OK;
+  gt_status sst = api_ensure_views(ctx, count);
+  if (sst != GT_OK) {
+    cleanup();
+    return sst;
+  }
   std::vector<ViewDev> vd(count);
+  uint32_t total_tiles = 0;
   size_t off = 0;
   for (uint32_t i = 0; i < count; ++i) {
     const BwdView& bv = views[i];
-    vd[i] = api_make_view(bv.scene, bv.u, bv.w, bv.h, img + off, total_tiles);
+    vd[i] = api_make_view(bv.scene, bv.u, bv.w, bv.h, nullptr, total_tiles);
     total_tiles += vd[i].n_tiles;
-    kc = std::max(kc, bv.u.k);
     size_t px = (size_t)bv.w * bv.h;
     if (flags & GT_FLAG_INPUT_DEVICE) {
       vd[i].dL = reinterpret_cast<const float4*>(bv.dL);
@@ -370,81 +547,31 @@ gt_status backward_impl(gt_context* ctx, const BwdView* views, uint32_t count, c
     vd[i].grad = G[s];
     off += px;
   }
-  sst = api_ensure_views(ctx, count);
-  if (sst != GT_OK) {
-    cleanup();
-    return sst;
-  }
-  const uint64_t slots = (uint64_t)total_tiles * 32u;
-  // checkpoint capacity and mode
-  uint32_t cap = opts && opts->max_rounds ? opts->max_rounds : 16u;
-  uint32_t mode = opts ? opts->mode : 0u;
-  size_t free_b = 0, total_b = 0;
-  cudaMemGetInfo(&free_b, &total_b);
-  uint64_t budget = opts && opts->mem_budget ? opts->mem_budget : free_b / 2;
-  uint32_t* ck_misc = nullptr;  // [0] max rounds, [1] overflow
-  BWD_TRY(talloc((void**)&ck_misc, 8));
+  BWD_TRY(cudaMemcpyAsync(ctx->d_views, vd.data(), sizeof(ViewDev) * count, cudaMemcpyHostToDevice, st));
   Ckpt ck;
-  ck.kc = kc;
-  ck.max_rounds = ck_misc;
-  ck.overflow = ck_misc + 1;
-  LaunchShape shape = api_shape_for(ctx, views[0].scene, views[0].w, views[0].h, views[0].u.k);
-  float fwd_ms = 0.f, bwd_ms = 0.f;
-  uint32_t used_mode = 0;
-  for (int attempt = 0; attempt < 4; ++attempt) {
-    uint64_t need_replay = slots * (4 + (uint64_t)cap * 8);
-    uint64_t need_ckpt = need_replay + slots * (uint64_t)cap * kc * 4;
-    used_mode = mode == 1 ? 1u : (mode == 2 ? 2u : (need_ckpt <= budget ? 1u : 2u));
-    BWD_TRY(talloc((void**)&ck.nrounds, slots * 4));
-    BWD_TRY(talloc((void**)&ck.rinfo, slots * (size_t)cap * sizeof(float2)));
-    ck.pidx = nullptr;
-    if (used_mode == 1) BWD_TRY(talloc((void**)&ck.pidx, slots * (size_t)cap * kc * 4));
-    ck.cap = cap;
-    BWD_TRY(cudaMemsetAsync(ck.nrounds, 0, slots * 4, st));
-    BWD_TRY(cudaMemsetAsync(ck_misc, 0, 8, st));
-    BWD_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), st));
-    BWD_TRY(cudaEventRecord(ctx->timer0, st));
-    Err e = launch_trace(vd.data(), count, total_tiles, ctx->d_ctr, ctx->faces, shape, ctx->num_sms, st,
-                         &ctx->launches, ctx->d_views, &ck);
-    if (e.code != GT_OK) {
-      cleanup();
-      return api_fail(ctx, e.code, e.msg);
-    }
-    BWD_TRY(cudaEventRecord(ctx->timer1, st));
-    uint32_t misc[2];
-    BWD_TRY(cudaMemcpyAsync(misc, ck_misc, 8, cudaMemcpyDeviceToHost, st));
-    BWD_TRY(cudaMemcpyAsync(ctx->h_ctr, ctx->d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
-    BWD_TRY(cudaStreamSynchronize(st));
-    cudaEventElapsedTime(&fwd_ms, ctx->timer0, ctx->timer1);
-    sst = api_status_to_error(ctx, ctx->h_ctr->status);
-    if (sst != GT_OK) {
-      cleanup();
-      return sst;
-    }
-    if (!misc[1]) break;
-    if (attempt == 3) {
-      cleanup();
-      return api_fail(ctx, GT_ERR_DEVICE_TIMEOUT, "checkpoint capacity exceeded");
-    }
-    // grow to the deepest ray and run the checkpointing forward again
-    cap = std::max(misc[0], 2 * cap);
-  }
-  // adjoint
+  ck.nrounds = cs.nrounds;
+  ck.rinfo = cs.rinfo;
+  ck.pidx = cs.mode == 1 ? cs.pidx : nullptr;
+  ck.cap = cs.cap;
+  ck.kc = cs.kc;
+  // 3. the adjoint
+  float bwd_ms = 0.f;
   BWD_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), st));
   BWD_TRY(cudaEventRecord(ctx->timer0, st));
   {
+    LaunchShape shape = api_shape_for(ctx, views[0].scene, views[0].w, views[0].h, views[0].u.k);
     uint32_t block = kWarpsPerBlock * 32;
     uint32_t grid = (uint32_t)ctx->num_sms * std::max(1u, shape.blocks_per_sm);
-    uint64_t max_grid = (slots + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    uint64_t max_grid = ((uint64_t)total_tiles * 32u + kWarpsPerBlock - 1) / kWarpsPerBlock;
     if (grid > max_grid) grid = (uint32_t)std::max<uint64_t>(1, max_grid);
-    if (used_mode == 1)
+    if (cs.mode == 1)
       k_backward<true><<<grid, block, 0, st>>>(ctx->d_views, count, total_tiles, ctx->d_ctr, ctx->faces, ck);
     else
       k_backward<false><<<grid, block, 0, st>>>(ctx->d_views, count, total_tiles, ctx->d_ctr, ctx->faces, ck);
     ++ctx->launches;
     BWD_TRY(cudaGetLastError());
   }
-  // parameter-major outputs
+  // 4. parameter-major outputs
   for (uint32_t s = 0; s < n_scenes; ++s) {
     uint64_t n = scenes[s]->n;
     if (n == 0) continue;
@@ -474,10 +601,10 @@ gt_status backward_impl(gt_context* ctx, const BwdView* views, uint32_t count, c
     stats->total_ms = fwd_ms + bwd_ms;
   }
   if (opts) {
-    opts->used_mode = used_mode;
+    opts->used_mode = cs.mode;
     opts->fwd_ms = fwd_ms;
     opts->bwd_ms = bwd_ms;
-    opts->max_rounds = cap;
+    opts->max_rounds = cs.cap;
   }
   cleanup();
   return sst;
@@ -529,4 +656,36 @@ extern "C" gt_status gt_backward_batch(gt_context* ctx, const gt_batch_item* ite
     if (!scenes[s] || scenes[s]->ctx != ctx || (!dL_dparams[s] && scenes[s]->n > 0))
       return api_fail(ctx, GT_ERR_INVALID_ARG, "bad scene or gradient output");
   return backward_impl(ctx, v.data(), count, scenes, dL_dparams, n_scenes, flags, opts, stats);
+}
+
+extern "C" gt_status gt_l2_loss(gt_context* ctx, const float* rgba, const float* target, uint64_t n_pixels,
+                                float* dL_drgba, double* loss) {
+  if (!ctx) return api_fail(nullptr, GT_ERR_INVALID_ARG, "context is NULL");
+  if (n_pixels == 0) {
+    if (loss) *loss = 0.0;
+    return GT_OK;
+  }
+  if (!rgba || !target || !dL_drgba) return api_fail(ctx, GT_ERR_INVALID_ARG, "NULL buffer");
+  if (((uintptr_t)rgba | (uintptr_t)target | (uintptr_t)dL_drgba) % 16)
+    return api_fail(ctx, GT_ERR_INVALID_ARG, "buffers must be 16-byte aligned");
+  CK_TRY(cudaSetDevice(ctx->device));
+  const unsigned blocks = (unsigned)((n_pixels + 255) / 256);
+  double* partial = nullptr;
+  CK_TRY(cudaMallocAsync((void**)&partial, blocks * sizeof(double), ctx->stream));
+  k_l2_loss<<<blocks, 256, 0, ctx->stream>>>(reinterpret_cast<const float4*>(rgba),
+                                             reinterpret_cast<const float4*>(target), n_pixels,
+                                             reinterpret_cast<float4*>(dL_drgba), partial);
+  ++ctx->launches;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && loss) {
+    std::vector<double> h(blocks);
+    e = cudaMemcpyAsync(h.data(), partial, blocks * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    double sum = 0.0;
+    for (double v : h) sum += v;
+    *loss = sum;
+  }
+  cudaFreeAsync(partial, ctx->stream);
+  if (e != cudaSuccess) return api_fail(ctx, GT_ERR_CUDA, cudaGetErrorString(e));
+  return GT_OK;
 }

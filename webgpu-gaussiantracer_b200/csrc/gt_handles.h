@@ -7,6 +7,7 @@
 #include <set>
 #include <string>
 #include <tuple>
+#include <vector>
 
 #include "gt_internal.cuh"
 
@@ -16,6 +17,28 @@ constexpr int kEventRing = 256;
 struct GraphEntry {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+};
+}  // namespace gt
+
+namespace gt {
+// Checkpoint of the last checkpointing forward of a context (see gt_backward.cu).
+struct CkptKey {
+  const gt_scene* scene;
+  gt_uniforms u;
+  uint32_t w, h;
+};
+struct CkptStore {
+  uint32_t* nrounds = nullptr;
+  float2* rinfo = nullptr;
+  uint32_t* pidx = nullptr;
+  uint32_t* misc = nullptr;      // device: [0] max rounds, [1] overflow
+  size_t nrounds_bytes = 0, rinfo_bytes = 0, pidx_bytes = 0;
+  uint64_t slots = 0;
+  uint32_t cap = 0, kc = 0, mode = 0;
+  uint32_t total_tiles = 0;
+  bool valid = false;
+  std::vector<CkptKey> key;
+  float fwd_ms = 0.f;
 };
 }  // namespace gt
 
@@ -40,6 +63,7 @@ struct gt_context {
   std::map<std::tuple<uint64_t, uint32_t, uint32_t, uint32_t>, gt_tune_result> tune;
   std::map<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t>, gt::GraphEntry> graphs;
   std::set<gt_scene*> scenes;  // live scenes; destroyed with the context
+  gt::CkptStore ckpt;
 };
 
 struct gt_scene {
@@ -61,4 +85,10 @@ ViewDev api_make_view(const gt_scene* s, const gt_uniforms& u, uint32_t w, uint3
 LaunchShape api_shape_for(gt_context* ctx, const gt_scene* s, uint32_t w, uint32_t h, uint32_t k);
 void api_fill_stats(const DevCounters& c, gt_render_stats* st);
 gt_status api_ensure_views(gt_context* ctx, uint32_t n);
+// Checkpointing forward (gt_backward.cu): renders the views into `outs`
+// (device, one per view) and keeps the round checkpoint in ctx->ckpt.
+gt_status api_forward_ckpt(gt_context* ctx, const gt_scene* const* scenes, const gt_uniforms* us, const uint32_t* ws,
+                           const uint32_t* hs, float4* const* outs, uint32_t count, uint32_t mode, uint32_t cap,
+                           uint64_t budget, gt_render_stats* stats);
+void api_free_ckpt(gt_context* ctx);
 }  // namespace gt

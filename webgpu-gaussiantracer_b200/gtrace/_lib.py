@@ -25,6 +25,7 @@ GT_FLAG_INPUT_DEVICE = 0x1
 GT_FLAG_OUTPUT_DEVICE = 0x2
 GT_FLAG_ASYNC = 0x4
 GT_FLAG_ACCUMULATE = 0x8
+GT_FLAG_CHECKPOINT = 0x10
 
 STATUS_NAMES = {GT_OK: "GT_OK", GT_ERR_INVALID_ARG: "GT_ERR_INVALID_ARG", GT_ERR_OOM: "GT_ERR_OOM",
                 GT_ERR_CUDA: "GT_ERR_CUDA", GT_ERR_DEVICE_TIMEOUT: "GT_ERR_DEVICE_TIMEOUT",
@@ -91,6 +92,7 @@ SIGNATURES = [
     ("gt_render_batch_noalloc", _i32, [_vp, C.POINTER(BatchItem), _u32, _u32, C.POINTER(RenderStats)]),
     ("gt_backward_batch", _i32, [_vp, C.POINTER(BatchItem), _u32, C.POINTER(_vp), C.POINTER(_vp), _u32, _u32,
                                  C.POINTER(BwdOpts), C.POINTER(RenderStats)]),
+    ("gt_l2_loss", _i32, [_vp, _vp, _vp, _u64, _vp, C.POINTER(C.c_double)]),
     ("gt_autotune", _i32, [_vp, _vp, C.POINTER(Uniforms), _u32, _u32, C.POINTER(TuneResult)]),
     ("gt_autotune_reset", _i32, [_vp]),
     ("gt_device_alloc", _i32, [_vp, _u64, C.POINTER(_vp)]),

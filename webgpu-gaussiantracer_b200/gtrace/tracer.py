@@ -79,24 +79,28 @@ class Context:
 
     # ------------------------------------------------------------- render
     def render(self, scene: "Scene", uniforms, width: int, height: int, out: np.ndarray | None = None,
-               stats: bool = False):
-        """Renders one view to a host array of shape (height, width, 4)."""
+               stats: bool = False, checkpoint: bool = False):
+        """Renders one view to a host array of shape (height, width, 4).
+        checkpoint=True keeps the round checkpoint for a following backward."""
         u = _uniforms(uniforms)
         if out is None:
             out = np.empty((height, width, 4), dtype=np.float32)
         if out.dtype != np.float32 or not out.flags.c_contiguous or out.size != width * height * 4:
             raise ValueError("out must be a C-contiguous float32 array of width*height*4 values")
         st = L.RenderStats()
+        flags = L.GT_FLAG_CHECKPOINT if checkpoint else 0
         self.check(self._lib.gt_render(self._h, scene.handle, C.byref(u), width, height,
-                                       out.ctypes.data_as(C.c_void_p), 0, C.byref(st)))
+                                       out.ctypes.data_as(C.c_void_p), flags, C.byref(st)))
         return (out, st.as_dict()) if stats else out
 
     trace_rays = render
 
-    def render_device(self, scene: "Scene", uniforms, width: int, height: int, out_dev: int, asynchronous=False):
+    def render_device(self, scene: "Scene", uniforms, width: int, height: int, out_dev: int, asynchronous=False,
+                      checkpoint: bool = False):
         """Renders into a device buffer (pointer from ``device_alloc``)."""
         u = _uniforms(uniforms)
-        flags = L.GT_FLAG_OUTPUT_DEVICE | (L.GT_FLAG_ASYNC if asynchronous else 0)
+        flags = L.GT_FLAG_OUTPUT_DEVICE | (L.GT_FLAG_ASYNC if asynchronous else 0) | \
+            (L.GT_FLAG_CHECKPOINT if checkpoint else 0)
         st = L.RenderStats()
         self.check(self._lib.gt_render(self._h, scene.handle, C.byref(u), width, height, C.c_void_p(out_dev), flags,
                                        None if asynchronous else C.byref(st)))
@@ -118,7 +122,8 @@ class Context:
         return rec
 
     def backward(self, scene: "Scene", uniforms, width: int, height: int, dL_drgba: np.ndarray, mode: int = 0,
-                 max_rounds: int = 0, mem_budget: int = 0, out: np.ndarray | None = None, accumulate=False):
+                 max_rounds: int = 0, mem_budget: int = 0, out: np.ndarray | None = None, accumulate=False,
+                 reuse_checkpoint: bool = False):
         """dLoss/dparams (59 x n, parameter-major) from dLoss/drgba (h, w, 4)."""
         u = _uniforms(uniforms)
         g = np.ascontiguousarray(dL_drgba, dtype=np.float32)
@@ -128,7 +133,7 @@ class Context:
             out = np.zeros((59, scene.n), dtype=np.float32)
         opts = L.BwdOpts(mode, max_rounds, mem_budget, 0, 0, 0.0, 0.0)
         st = L.RenderStats()
-        flags = L.GT_FLAG_ACCUMULATE if accumulate else 0
+        flags = (L.GT_FLAG_ACCUMULATE if accumulate else 0) | (L.GT_FLAG_CHECKPOINT if reuse_checkpoint else 0)
         self.check(self._lib.gt_backward(self._h, scene.handle, C.byref(u), width, height,
                                          g.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p), flags,
                                          C.byref(opts), C.byref(st)))
@@ -188,6 +193,25 @@ class Context:
         st = L.RenderStats()
         self.check(self._lib.gt_render_batch(self._h, items, len(views), flags, None if asynchronous else C.byref(st)))
         return results, st.as_dict()
+
+    def backward_device(self, scene: "Scene", uniforms, width: int, height: int, dL_dev: int, out_dev: int,
+                        reuse_checkpoint: bool = True, mode: int = 0):
+        """Device-buffer backward (gradient 59 x n at out_dev); returns the info dict."""
+        u = _uniforms(uniforms)
+        opts = L.BwdOpts(mode, 0, 0, 0, 0, 0.0, 0.0)
+        st = L.RenderStats()
+        flags = L.GT_FLAG_INPUT_DEVICE | L.GT_FLAG_OUTPUT_DEVICE | (L.GT_FLAG_CHECKPOINT if reuse_checkpoint else 0)
+        self.check(self._lib.gt_backward(self._h, scene.handle, C.byref(u), width, height, C.c_void_p(dL_dev),
+                                         C.c_void_p(out_dev), flags, C.byref(opts), C.byref(st)))
+        info = st.as_dict()
+        info.update(used_mode=opts.used_mode, fwd_ms=opts.fwd_ms, bwd_ms=opts.bwd_ms, max_rounds=opts.max_rounds)
+        return info
+
+    def l2_loss(self, rgba_dev: int, target_dev: int, n_pixels: int, dL_dev: int) -> float:
+        loss = C.c_double()
+        self.check(self._lib.gt_l2_loss(self._h, C.c_void_p(rgba_dev), C.c_void_p(target_dev), n_pixels,
+                                        C.c_void_p(dL_dev), C.byref(loss)))
+        return loss.value
 
     def autotune(self, scene: "Scene", uniforms, width: int, height: int):
         r = L.TuneResult()
