@@ -150,6 +150,152 @@ def cpu_port_throughput(pg, amin, v, budget_s: float, threads: int = 0):
     return len(pix) / dt / 1e6, len(pix), stride, dt, prep
 
 
+def _time_device(ctx, fn, reps: int):
+    """Device time (CUDA events on the library stream) of reps calls of fn."""
+    ctx.synchronize()
+    ctx.timer_start()
+    for _ in range(reps):
+        fn()
+    return ctx.timer_stop() / reps
+
+
+def extra_batched(ctx, reps: int = 2):
+    """8 scenes (100k-1M Gaussians, log-uniform), 64 views of uneven size: one
+    batched launch against the 64 views rendered one by one."""
+    from gtrace import synth
+    from gtrace.tracer import Scene
+    raw_scenes, views = synth.batched_scenes_config()
+    scenes = [Scene(ctx, synth.pack(raw).gaussiansBuffer, amin) for raw, amin in raw_scenes]
+    amins = [amin for _, amin in raw_scenes]
+    items, bufs = [], []
+    rays = 0
+    for s, w, h, pos in views:
+        v = synth.view(w, h, pos, k=16, alpha_min=amins[s])
+        ptr = ctx.device_alloc(w * h * 16)
+        bufs.append(ptr)
+        items.append((scenes[s], v.uniforms, w, h, ptr))
+        rays += w * h
+    batched = lambda: ctx.render_batch(items, device_outputs=True, asynchronous=True)  # noqa: E731
+    def plain():
+        for sc, u, w, h, ptr in items:
+            ctx.render_device(sc, u, w, h, ptr, asynchronous=True)
+    batched()
+    plain()
+    tb = _time_device(ctx, batched, reps)
+    tp = _time_device(ctx, plain, reps)
+    for ptr in bufs:
+        ctx.device_free(ptr)
+    n_total = sum(s.n for s in scenes)
+    for s in scenes:
+        s.close()
+    return {"workload": f"8 scenes ({n_total} Gaussians in all, 100k-1M each, 64 clusters), 64 views 320-1920 x "
+                        "240-1080, k=16, alpha_min per scene in {0.01, 0.05, 0.1}, camera radius 8-14",
+            "rays": rays, "batched_ms": tb, "plain_ms": tp, "batched_mrays": rays / tb / 1e3,
+            "plain_mrays": rays / tp / 1e3}
+
+
+def _train_step_single(ctx, scene, v, img, tgt, dl, gout):
+    ctx.render_device(scene, v.uniforms, v.width, v.height, img, checkpoint=True)
+    ctx.l2_loss(img, tgt, v.width * v.height, dl)
+    return ctx.backward_device(scene, v.uniforms, v.width, v.height, dl, gout, reuse_checkpoint=True)
+
+
+def extra_fwd_bwd(ctx, reps: int = 3):
+    """200k Gaussians, 800x800, k=8, L2 loss against a render of the perturbed
+    scene: plain forward vs forward + loss + backward."""
+    from gtrace import synth
+    from gtrace.tracer import Scene
+    raw, amin, v = synth.clusters_200k_config()
+    scene = Scene(ctx, synth.pack(raw).gaussiansBuffer, amin)
+    target = Scene(ctx, synth.pack(synth.perturb(raw, synth.SEED_BASE + 33)).gaussiansBuffer, amin)
+    px = v.width * v.height
+    img, tgt, dl = ctx.device_alloc(px * 16), ctx.device_alloc(px * 16), ctx.device_alloc(px * 16)
+    gout = ctx.device_alloc(59 * scene.n * 4)
+    ctx.render_device(target, v.uniforms, v.width, v.height, tgt)
+    fwd = lambda: ctx.render_device(scene, v.uniforms, v.width, v.height, img, asynchronous=True)  # noqa: E731
+    info = {}
+    def step():
+        info.update(_train_step_single(ctx, scene, v, img, tgt, dl, gout))
+    fwd()
+    step()
+    tf = _time_device(ctx, fwd, reps)
+    tfb = _time_device(ctx, step, reps)
+    for p in (img, tgt, dl, gout):
+        ctx.device_free(p)
+    scene.close()
+    target.close()
+    return {"workload": "200k Gaussians (64 clusters), 800x800, k=8, alpha_min=0.01, L2 loss vs perturbed scene",
+            "fwd_ms": tf, "fwd_bwd_ms": tfb, "ratio": tfb / tf, "adjoint_ms": info.get("bwd_ms"),
+            "checkpoint_fwd_ms": None, "mode": "checkpoint" if info.get("used_mode") == 1 else "replay"}
+
+
+def extra_batched_fwd_bwd(ctx, pg, amin, reps: int = 1):
+    """32 views (640x480 - 1920x1080) of the 1M scene: batched forward with
+    checkpoint + per-view L2 loss + one batched adjoint accumulating all views,
+    against 32 plain forwards one by one."""
+    import ctypes as C
+    from gtrace import _lib as L
+    from gtrace import synth
+    from gtrace.tracer import Scene, _uniforms
+    rng = np.random.Generator(np.random.PCG64(synth.SEED_BASE + 4))
+    scene = Scene(ctx, pg.gaussiansBuffer, amin)
+    target_raw = synth.perturb(synth.raw_clusters(1_000_000, synth.SEED_BASE + 1), synth.SEED_BASE + 44)
+    target = Scene(ctx, synth.pack(target_raw).gaussiansBuffer, amin)
+    views = []
+    for i in range(32):
+        w = int(rng.integers(640, 1921))
+        h = int(rng.integers(480, 1081))
+        pos = synth.random_sphere_camera(rng, 10.0, 14.0)
+        views.append(synth.view(w, h, pos, k=16))
+    imgs = [ctx.device_alloc(v.width * v.height * 16) for v in views]
+    tgts = [ctx.device_alloc(v.width * v.height * 16) for v in views]
+    dls = [ctx.device_alloc(v.width * v.height * 16) for v in views]
+    gout = ctx.device_alloc(59 * scene.n * 4)
+    for v, t in zip(views, tgts):
+        ctx.render_device(target, v.uniforms, v.width, v.height, t)
+    items = [(scene, v.uniforms, v.width, v.height, p) for v, p in zip(views, imgs)]
+    lib = ctx._lib
+    bitems = (L.BatchItem * len(views))()
+    for i, v in enumerate(views):
+        bitems[i].scene = scene.handle
+        bitems[i].u = _uniforms(v.uniforms)
+        bitems[i].w, bitems[i].h = v.width, v.height
+        bitems[i].out_rgba = None
+        bitems[i].dL_drgba = dls[i]
+    sc = (C.c_void_p * 1)(scene.handle.value)
+    op = (C.c_void_p * 1)(gout)
+    rays = sum(v.width * v.height for v in views)
+    its = (L.BatchItem * len(views))()
+    for i, (s_, u_, w_, h_, p_) in enumerate(items):
+        its[i].scene = s_.handle
+        its[i].u = _uniforms(u_)
+        its[i].w, its[i].h = w_, h_
+        its[i].out_rgba = p_
+
+    def step():
+        flags = L.GT_FLAG_OUTPUT_DEVICE | L.GT_FLAG_CHECKPOINT
+        ctx.check(lib.gt_render_batch(ctx.handle, its, len(views), flags, None))
+        for v, i_, t_, d_ in zip(views, imgs, tgts, dls):
+            ctx.l2_loss(i_, t_, v.width * v.height, d_)
+        opts = L.BwdOpts(0, 0, 0, 0, 0, 0.0, 0.0)
+        ctx.check(lib.gt_backward_batch(ctx.handle, bitems, len(views), sc, op, 1,
+                                        L.GT_FLAG_INPUT_DEVICE | L.GT_FLAG_OUTPUT_DEVICE | L.GT_FLAG_CHECKPOINT,
+                                        C.byref(opts), None))
+    def plain():
+        for s_, u_, w_, h_, p_ in items:
+            ctx.render_device(s_, u_, w_, h_, p_, asynchronous=True)
+    step()
+    plain()
+    tfb = _time_device(ctx, step, reps)
+    tp = _time_device(ctx, plain, reps)
+    for p in imgs + tgts + dls + [gout]:
+        ctx.device_free(p)
+    scene.close()
+    target.close()
+    return {"workload": "1M Gaussians (64 clusters), 32 views 640x480-1920x1080, k=16, L2 loss vs perturbed scene",
+            "rays": rays, "batched_fwd_bwd_ms": tfb, "plain_fwd_ms": tp, "ratio": tfb / tp}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -159,6 +305,8 @@ def main():
     ap.add_argument("--workload", default="clusters-1m-1080p")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU baseline work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched and forward+backward measurements")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -270,6 +418,10 @@ def main():
                "sample": f"{n} pixels (every {stride}th pixel in x and y) of the {w}x{h} view, {dt:.1f} s; "
                          f"CPU restatement of the reference traversal"}
     clocks = clk.summary()
+    extras = None
+    if rank == 0 and world == 1 and not args.no_extras and args.workload == "clusters-1m-1080p":
+        extras = {"batched": extra_batched(ctx), "fwd_bwd": extra_fwd_bwd(ctx),
+                  "batched_fwd_bwd": extra_batched_fwd_bwd(ctx, pg, amin)}
     line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, no dataset)",
@@ -287,7 +439,7 @@ def main():
             "gpu_launches": n_launch, "clocks": clocks,
             "counters": {k2: st0[k2] for k2 in ("rounds", "entries", "contributing", "proxy_tests", "node_visits",
                                                  "anyhits")},
-            "image_checksum": checksum}
+            "image_checksum": checksum, "extras": extras}
     if rank == 0:
         print(json.dumps(line), flush=True)
     scene.close()
