@@ -190,7 +190,9 @@ gt_status gt_render_hits(gt_context* ctx, const gt_scene* scene, const gt_unifor
  * No counterpart in the reference (it has no training path, README.md:69). */
 typedef struct gt_bwd_opts {
   uint32_t mode;          /* 0 = auto (checkpoint if it fits), 1 = checkpoint, 2 = replay */
-  uint32_t max_rounds;    /* per-ray round capacity of the checkpoint; 0 = 64            */
+  uint32_t max_rounds;    /* in: expected rounds per ray, sizes the first checkpoint pool
+                             (0 = the previous call's count, else 4); the pool grows to
+                             the rounds actually traced.  out: round records used     */
   uint64_t mem_budget;    /* bytes the checkpoint may use; 0 = 1/2 of free device memory */
   uint32_t used_mode;     /* out: 1 = checkpoint, 2 = replay                              */
   uint32_t _pad;

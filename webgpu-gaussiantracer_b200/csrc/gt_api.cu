@@ -212,6 +212,8 @@ extern "C" gt_status gt_context_create(int device, gt_context** out) {
   CTX_TRY(cudaEventCreate(&ctx->call1));
   CTX_TRY(cudaEventCreate(&ctx->timer0));
   CTX_TRY(cudaEventCreate(&ctx->timer1));
+  CTX_TRY(cudaEventCreate(&ctx->int0));
+  CTX_TRY(cudaEventCreate(&ctx->int1));
   for (int i = 0; i < 2 * kEventRing; ++i) CTX_TRY(cudaEventCreate(&ctx->ring[i]));
 #undef CTX_TRY
   make_face_table(&ctx->faces);
@@ -239,7 +241,7 @@ extern "C" gt_status gt_context_destroy(gt_context* ctx) {
   cudaFree(ctx->d_views);
   cudaFreeHost(ctx->h_views);
   cudaFree(ctx->staging);
-  for (cudaEvent_t ev : {ctx->call0, ctx->call1, ctx->timer0, ctx->timer1})
+  for (cudaEvent_t ev : {ctx->call0, ctx->call1, ctx->timer0, ctx->timer1, ctx->int0, ctx->int1})
     if (ev) cudaEventDestroy(ev);
   for (int i = 0; i < 2 * kEventRing; ++i)
     if (ctx->ring[i]) cudaEventDestroy(ctx->ring[i]);
@@ -581,14 +583,14 @@ extern "C" gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const g
     float ms_min = 1e30f;
     for (int rep = 0; rep < 3; ++rep) {
       API_CUDA(ctx, cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), ctx->stream));
-      API_CUDA(ctx, cudaEventRecord(ctx->timer0, ctx->stream));
+      API_CUDA(ctx, cudaEventRecord(ctx->int0, ctx->stream));
       Err e = launch_trace(&v, 1, v.n_tiles, ctx->d_ctr, ctx->faces, sh, ctx->num_sms, ctx->stream, &ctx->launches,
                            ctx->d_views);
       if (e.code != GT_OK) return fail(ctx, e);
-      API_CUDA(ctx, cudaEventRecord(ctx->timer1, ctx->stream));
-      API_CUDA(ctx, cudaEventSynchronize(ctx->timer1));
+      API_CUDA(ctx, cudaEventRecord(ctx->int1, ctx->stream));
+      API_CUDA(ctx, cudaEventSynchronize(ctx->int1));
       float ms = 0.0f;
-      cudaEventElapsedTime(&ms, ctx->timer0, ctx->timer1);
+      cudaEventElapsedTime(&ms, ctx->int0, ctx->int1);
       ms_min = std::min(ms_min, ms);
     }
     if (b == LaunchShape().blocks_per_sm) def = ms_min;

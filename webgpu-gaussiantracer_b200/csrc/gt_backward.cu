@@ -211,8 +211,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewD
     uint32_t px = (lt % V.tiles_x) * kTileW + (sl % kTileW);
     uint32_t py = (lt / V.tiles_x) * kTileH + (sl / kTileW);
     if (px >= V.w || py >= V.h) continue;
-    const uint32_t nr = min(ck.nrounds[item], ck.cap);
-    if (nr == 0) continue;
+    uint32_t rec = ck.head[item];
+    if (rec == kInvalid) continue;
     const float4 g4 = V.dL[(size_t)py * V.w + px];
     if (g4.x == 0.f && g4.y == 0.f && g4.z == 0.f) continue;
     const float g[3] = {g4.x, g4.y, g4.z};
@@ -222,22 +222,25 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewD
     const uint32_t k = V.u.k;
     float R0 = 0.f, R1 = 0.f, R2 = 0.f;
     ++rays;
-    for (int r = (int)nr - 1; r >= 0; --r) {
-      const size_t at = (size_t)item * ck.cap + r;
-      const float2 ri = ck.rinfo[at];
+    // rounds from the last to the first along the record links
+    for (uint32_t guard = 0; rec != kInvalid && guard < ck.pool_cap; ++guard) {
+      const uint32_t* rr = ck.pool + (size_t)rec * (kCkptHeader + ck.kc);
+      const float2 ri = make_float2(__uint_as_float(rr[0]), __uint_as_float(rr[1]));
+      const uint32_t prev = rr[2], nrec = rr[3];
       uint32_t p = kInvalid;
       bool valid;
       if (CKPT_PIDX) {
-        p = lane < ck.kc ? ck.pidx[at * ck.kc + lane] : kInvalid;
-        valid = lane < k && p != kInvalid;
+        p = lane < ck.kc ? rr[kCkptHeader + lane] : kInvalid;
+        valid = lane < nrec && p != kInvalid;
       } else {
         float bt = V.u.t_max;
         uint32_t bp = kInvalid;
         traverse8<kCollect>(V.s, F, W, o, d, br, ri.x, V.u.t_max, bt, bp, nullptr, st, status, lane);
         if (__reduce_or_sync(kFull, status) & (kStatusStackOverflow | kStatusVisitCap | kStatusHitOverflow)) break;
-        valid = lane < k && bp != kInvalid;
+        valid = lane < k && lane < nrec && bp != kInvalid;
         p = bp;
       }
+      rec = prev;
       const uint32_t vmask = __ballot_sync(kFull, valid);
       const int n = __popc(vmask);
       float alpha = 0.f, resp = 0.f;
@@ -364,19 +367,18 @@ namespace gt {
 
 void api_free_ckpt(gt_context* ctx) {
   CkptStore& c = ctx->ckpt;
-  cudaFree(c.nrounds);
-  cudaFree(c.rinfo);
-  cudaFree(c.pidx);
-  cudaFree(c.misc);
+  cudaFree(c.head);
+  cudaFree(c.pool);
+  cudaFree(c.pool_next);
   c = CkptStore{};
 }
 
-// Checkpointing forward: renders the views into `outs` and keeps, per ray
-// slot, the round count and per round (t_curr, T) at its start, plus the
-// round's particle indices in checkpoint mode (mode 1) — chosen when they
-// fit in `budget` bytes, or forced by `mode`.  A ray with more rounds than
-// the capacity sets an overflow flag; the capacity then grows to the
-// deepest ray and the forward runs again.
+// Checkpointing forward: renders the views into `outs` and keeps one record
+// per traced round (see Ckpt).  Mode 1 stores the rounds' particle indices
+// (no traversal in the adjoint) when the records fit in `budget` bytes;
+// mode 2 stores only (t_curr, T) and the adjoint finds each round's entries
+// again.  The pool is sized from the previous call; when the rounds outgrow
+// it, the forward runs again with the exact size.
 gt_status api_forward_ckpt(gt_context* ctx, const gt_scene* const* scenes, const gt_uniforms* us, const uint32_t* ws,
                            const uint32_t* hs, float4* const* outs, uint32_t count, uint32_t mode, uint32_t cap,
                            uint64_t budget, gt_render_stats* stats) {
@@ -386,50 +388,52 @@ gt_status api_forward_ckpt(gt_context* ctx, const gt_scene* const* scenes, const
   gt_status sst = api_ensure_views(ctx, count);
   if (sst != GT_OK) return sst;
   std::vector<ViewDev> vd(count);
-  uint32_t total_tiles = 0, kc = 1;
+  uint32_t total_tiles = 0, kmax = 1;
+  uint64_t rays = 0;
   for (uint32_t i = 0; i < count; ++i) {
     vd[i] = api_make_view(scenes[i], us[i], ws[i], hs[i], outs[i], total_tiles);
     total_tiles += vd[i].n_tiles;
-    kc = std::max(kc, us[i].k);
+    kmax = std::max(kmax, us[i].k);
+    rays += (uint64_t)ws[i] * hs[i];
   }
   const uint64_t slots = (uint64_t)total_tiles * 32u;
-  if (cap == 0) cap = ck.cap ? ck.cap : 16u;
   if (budget == 0) {
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
-    budget = free_b / 2;
+    budget = free_b / 2 + ck.pool_bytes;  // the pool we hold counts as available
   }
-  if (!ck.misc) CK_TRY(cudaMalloc(&ck.misc, 8));
+  // first guess of the records: the last call's count, else 4 rounds a ray
+  uint64_t want = ck.last_records ? ck.last_records + ck.last_records / 8 + 1024 : rays * 4 + 1024;
+  if (cap) want = std::max<uint64_t>(want, rays * (uint64_t)cap);
+  if (!ck.pool_next) CK_TRY(cudaMalloc(&ck.pool_next, 4));
+  sst = grow(ctx, (void**)&ck.head, &ck.head_bytes, slots * 4);
+  if (sst != GT_OK) return sst;
   LaunchShape shape = api_shape_for(ctx, scenes[0], ws[0], hs[0], us[0].k);
-  for (int attempt = 0; attempt < 4; ++attempt) {
-    uint64_t need_replay = slots * (4 + (uint64_t)cap * 8);
-    uint64_t need_pidx = slots * (uint64_t)cap * kc * 4;
-    uint32_t m = mode == 1 ? 1u : (mode == 2 ? 2u : (need_replay + need_pidx <= budget ? 1u : 2u));
-    sst = grow(ctx, (void**)&ck.nrounds, &ck.nrounds_bytes, slots * 4);
-    if (sst == GT_OK) sst = grow(ctx, (void**)&ck.rinfo, &ck.rinfo_bytes, slots * (size_t)cap * sizeof(float2));
-    if (sst == GT_OK && m == 1) sst = grow(ctx, (void**)&ck.pidx, &ck.pidx_bytes, slots * (size_t)cap * kc * 4);
+  for (int attempt = 0; attempt < 3; ++attempt) {
+    if (want > 0xFFFFFFF0ull) return api_fail(ctx, GT_ERR_OOM, "checkpoint needs more than 2^32 round records");
+    uint32_t m = mode == 1 ? 1u : (mode == 2 ? 2u : (want * (kCkptHeader + kmax) * 4 <= budget ? 1u : 2u));
+    const uint32_t kc = m == 1 ? kmax : 0u;
+    sst = grow(ctx, (void**)&ck.pool, &ck.pool_bytes, want * (kCkptHeader + kc) * 4);
     if (sst != GT_OK) return sst;
     Ckpt c;
-    c.nrounds = ck.nrounds;
-    c.rinfo = ck.rinfo;
-    c.pidx = m == 1 ? ck.pidx : nullptr;
-    c.cap = cap;
+    c.head = ck.head;
+    c.pool = ck.pool;
+    c.pool_next = ck.pool_next;
+    c.pool_cap = (uint32_t)std::min<uint64_t>(ck.pool_bytes / ((kCkptHeader + kc) * 4), 0xFFFFFFF0ull);
     c.kc = kc;
-    c.max_rounds = ck.misc;
-    c.overflow = ck.misc + 1;
-    CK_TRY(cudaMemsetAsync(ck.nrounds, 0, slots * 4, st));
-    CK_TRY(cudaMemsetAsync(ck.misc, 0, 8, st));
+    CK_TRY(cudaMemsetAsync(ck.head, 0xFF, slots * 4, st));
+    CK_TRY(cudaMemsetAsync(ck.pool_next, 0, 4, st));
     CK_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), st));
-    CK_TRY(cudaEventRecord(ctx->timer0, st));
+    CK_TRY(cudaEventRecord(ctx->int0, st));
     Err e = launch_trace(vd.data(), count, total_tiles, ctx->d_ctr, ctx->faces, shape, ctx->num_sms, st,
                          &ctx->launches, ctx->d_views, &c);
     if (e.code != GT_OK) return api_fail(ctx, e.code, e.msg);
-    CK_TRY(cudaEventRecord(ctx->timer1, st));
-    uint32_t misc[2];
-    CK_TRY(cudaMemcpyAsync(misc, ck.misc, 8, cudaMemcpyDeviceToHost, st));
+    CK_TRY(cudaEventRecord(ctx->int1, st));
+    uint32_t used = 0;
+    CK_TRY(cudaMemcpyAsync(&used, ck.pool_next, 4, cudaMemcpyDeviceToHost, st));
     CK_TRY(cudaMemcpyAsync(ctx->h_ctr, ctx->d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
     CK_TRY(cudaStreamSynchronize(st));
-    cudaEventElapsedTime(&ck.fwd_ms, ctx->timer0, ctx->timer1);
+    cudaEventElapsedTime(&ck.fwd_ms, ctx->int0, ctx->int1);
     sst = api_status_to_error(ctx, ctx->h_ctr->status);
     if (sst != GT_OK) return sst;
     if (stats) {
@@ -438,9 +442,10 @@ gt_status api_forward_ckpt(gt_context* ctx, const gt_scene* const* scenes, const
       stats->kernel_ms = ck.fwd_ms;
       stats->total_ms = ck.fwd_ms;
     }
-    if (!misc[1]) {
+    ck.last_records = used;
+    if (used <= c.pool_cap) {
       ck.slots = slots;
-      ck.cap = cap;
+      ck.pool_cap = c.pool_cap;
       ck.kc = kc;
       ck.mode = m;
       ck.total_tiles = total_tiles;
@@ -449,9 +454,9 @@ gt_status api_forward_ckpt(gt_context* ctx, const gt_scene* const* scenes, const
       ck.valid = true;
       return GT_OK;
     }
-    cap = std::max(misc[0], 2 * cap);
+    want = (uint64_t)used + 1024;  // exact size for the second run
   }
-  return api_fail(ctx, GT_ERR_DEVICE_TIMEOUT, "checkpoint capacity exceeded");
+  return api_fail(ctx, GT_ERR_DEVICE_TIMEOUT, "checkpoint pool kept overflowing");
 }
 
 }  // namespace gt
@@ -549,15 +554,15 @@ gt_status backward_impl(gt_context* ctx, const BwdView* views, uint32_t count, c
   }
   BWD_TRY(cudaMemcpyAsync(ctx->d_views, vd.data(), sizeof(ViewDev) * count, cudaMemcpyHostToDevice, st));
   Ckpt ck;
-  ck.nrounds = cs.nrounds;
-  ck.rinfo = cs.rinfo;
-  ck.pidx = cs.mode == 1 ? cs.pidx : nullptr;
-  ck.cap = cs.cap;
+  ck.head = cs.head;
+  ck.pool = cs.pool;
+  ck.pool_next = cs.pool_next;
+  ck.pool_cap = cs.pool_cap;
   ck.kc = cs.kc;
   // 3. the adjoint
   float bwd_ms = 0.f;
   BWD_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), st));
-  BWD_TRY(cudaEventRecord(ctx->timer0, st));
+  BWD_TRY(cudaEventRecord(ctx->int0, st));
   {
     LaunchShape shape = api_shape_for(ctx, views[0].scene, views[0].w, views[0].h, views[0].u.k);
     uint32_t block = kWarpsPerBlock * 32;
@@ -589,10 +594,10 @@ gt_status backward_impl(gt_context* ctx, const BwdView* views, uint32_t count, c
     if (!(flags & GT_FLAG_OUTPUT_DEVICE))
       BWD_TRY(cudaMemcpyAsync(dst, dev_out, n * GT_PARAMS_PER_PARTICLE * 4, cudaMemcpyDeviceToHost, st));
   }
-  BWD_TRY(cudaEventRecord(ctx->timer1, st));
+  BWD_TRY(cudaEventRecord(ctx->int1, st));
   BWD_TRY(cudaMemcpyAsync(ctx->h_ctr, ctx->d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
   BWD_TRY(cudaStreamSynchronize(st));
-  cudaEventElapsedTime(&bwd_ms, ctx->timer0, ctx->timer1);
+  cudaEventElapsedTime(&bwd_ms, ctx->int0, ctx->int1);
   sst = api_status_to_error(ctx, ctx->h_ctr->status);
   if (stats) {
     memset(stats, 0, sizeof *stats);
@@ -604,7 +609,7 @@ gt_status backward_impl(gt_context* ctx, const BwdView* views, uint32_t count, c
     opts->used_mode = cs.mode;
     opts->fwd_ms = fwd_ms;
     opts->bwd_ms = bwd_ms;
-    opts->max_rounds = cs.cap;
+    opts->max_rounds = (uint32_t)std::min<uint64_t>(cs.last_records, 0xFFFFFFFFull);
   }
   cleanup();
   return sst;

@@ -28,13 +28,15 @@ struct CkptKey {
   uint32_t w, h;
 };
 struct CkptStore {
-  uint32_t* nrounds = nullptr;
-  float2* rinfo = nullptr;
-  uint32_t* pidx = nullptr;
-  uint32_t* misc = nullptr;      // device: [0] max rounds, [1] overflow
-  size_t nrounds_bytes = 0, rinfo_bytes = 0, pidx_bytes = 0;
+  uint32_t* head = nullptr;       // [slots]
+  uint32_t* pool = nullptr;       // round records
+  uint32_t* pool_next = nullptr;  // device allocation counter
+  size_t head_bytes = 0, pool_bytes = 0;
   uint64_t slots = 0;
-  uint32_t cap = 0, kc = 0, mode = 0;
+  uint32_t pool_cap = 0;          // records that fit
+  uint32_t kc = 0;                // particle indices per record (0: replay mode)
+  uint32_t mode = 0;              // 1 checkpoint, 2 replay
+  uint64_t last_records = 0;      // records the last forward needed
   uint32_t total_tiles = 0;
   bool valid = false;
   std::vector<CkptKey> key;
@@ -57,6 +59,7 @@ struct gt_context {
   float4* staging = nullptr;
   size_t staging_bytes = 0;
   cudaEvent_t call0 = nullptr, call1 = nullptr, timer0 = nullptr, timer1 = nullptr;
+  cudaEvent_t int0 = nullptr, int1 = nullptr;  // library-internal timing (never the user's timer)
   cudaEvent_t ring[2 * gt::kEventRing];
   uint64_t ring_head = 0, ring_tail = 0;
   uint64_t launches = 0;

@@ -157,18 +157,22 @@ Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride_bytes, doubl
                 cudaStream_t stream, SceneBuffers* out, uint64_t* launches);
 void free_scene(SceneBuffers* b);
 
-// Round checkpoint written by the forward pass of gt_backward: per ray slot,
-// the number of rounds, and per round (t_curr, T) at its start and, when
-// `pidx` is set, the particle indices of its entries (kInvalid past the end).
+// Round checkpoint written by the forward pass of gt_backward.  Each traced
+// round gets one record from a shared pool (one atomic per round); records of
+// a ray are linked from its last round to its first, the order the adjoint
+// walks them, so memory follows the rounds actually traced.
+// Record layout (uint32 words): [0] t_curr at the round start (float bits),
+// [1] T at the round start (float bits), [2] previous record of the ray
+// (kInvalid for the first), [3] number of entries, [4, 4 + kc) particle
+// indices of the entries (checkpoint mode only; kc == 0 in replay mode).
 struct Ckpt {
-  uint32_t* nrounds = nullptr;  // [slots]
-  float2* rinfo = nullptr;      // [slots][cap]
-  uint32_t* pidx = nullptr;     // [slots][cap][kc] or null (replay mode)
-  uint32_t cap = 0;             // rounds stored per ray
-  uint32_t kc = 0;              // entries stored per round
-  uint32_t* max_rounds = nullptr;
-  uint32_t* overflow = nullptr;
+  uint32_t* head = nullptr;       // [slots] last record of the ray, kInvalid if none
+  uint32_t* pool = nullptr;       // [pool_cap][4 + kc]
+  uint32_t* pool_next = nullptr;  // allocation counter (counts past pool_cap on overflow)
+  uint32_t pool_cap = 0;          // records
+  uint32_t kc = 0;                // particle indices stored per record (0: replay mode)
 };
+constexpr uint32_t kCkptHeader = 4;
 
 // Trace launches (gt_trace.cu).
 Err launch_trace(const ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,

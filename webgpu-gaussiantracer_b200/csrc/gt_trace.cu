@@ -100,6 +100,7 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
   R.step = 0;
   R.n_entries = 0;
   const uint32_t k = V.u.k;
+  uint32_t ck_head = kInvalid;
   while (wray_more(V, R)) {
     // one traversal: the 32 closest front-face hits with t > t_curr
     float bt = t_max;
@@ -115,12 +116,21 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
       const uint32_t avail = cnt - skip;
       if (!complete && avail < k) break;  // the next round reaches past the buffer
       const uint32_t n = avail < k ? avail : k;
-      if (CKPT && R.step < ck.cap) {
-        const size_t at = (size_t)slot * ck.cap + R.step;
-        if (lane == 0) ck.rinfo[at] = make_float2(R.t_curr, R.T);
-        if (ck.pidx) {
+      if (CKPT) {
+        uint32_t rec = 0;
+        if (lane == 0) rec = atomicAdd(ck.pool_next, 1u);
+        rec = __shfl_sync(kFull, rec, 0);
+        if (rec < ck.pool_cap) {  // past the pool the host sizes it up and runs again
+          uint32_t* r = ck.pool + (size_t)rec * (kCkptHeader + ck.kc);
+          if (lane == 0) {
+            r[0] = __float_as_uint(R.t_curr);
+            r[1] = __float_as_uint(R.T);
+            r[2] = ck_head;
+            r[3] = n;
+          }
           uint32_t v = __shfl_sync(kFull, bp, (int)((skip + lane) & 31u));
-          if (lane < ck.kc) ck.pidx[at * ck.kc + lane] = lane < n ? v : kInvalid;
+          if (lane < ck.kc) r[kCkptHeader + lane] = lane < n ? v : kInvalid;
+          ck_head = rec;
         }
       }
       ++R.step;
@@ -182,13 +192,7 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
     ho.count[slot] = R.n_entries;
     ho.rounds[slot] = R.step;
   }
-  if (CKPT && lane == 0) {
-    ck.nrounds[slot] = R.step;
-    if (R.step > ck.cap) {
-      atomicOr(ck.overflow, 1u);
-      atomicMax(ck.max_rounds, R.step);
-    }
-  }
+  if (CKPT && lane == 0) ck.head[slot] = ck_head;
   return make_float4(R.L0, R.L1, R.L2, 1.0f);
 }
 
