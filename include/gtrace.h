@@ -279,10 +279,18 @@ typedef struct gt_tune_result {
   uint32_t tile_w, tile_h;/* pixel tile a warp takes per work-stealing step     */
   float best_ms;          /* fastest trace time measured                        */
   float default_ms;       /* trace time of the default launch shape             */
+  uint32_t kbuf;          /* k-buffer size of a traversal (k..128; raised to k) */
+  uint32_t leaf_batch;    /* queued leaves that start a batch of proxy tests    */
 } gt_tune_result;
 
 gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const gt_uniforms* u,
                       uint32_t w, uint32_t h, gt_tune_result* result);
+/* Installs a launch shape for the bucket of (scene, u->k, w x h) without
+ * timing anything (for example one found by gt_autotune in an earlier run).
+ * block_threads must be 128 and the tile 8 x 4; blocks_per_sm 1..32,
+ * kbuf 1..128 and leaf_batch 1..32.  best_ms/default_ms are ignored. */
+gt_status gt_set_tune(gt_context* ctx, const gt_scene* scene, const gt_uniforms* u, uint32_t w,
+                      uint32_t h, const gt_tune_result* shape);
 /* Drops every cached tuning result of the context. */
 gt_status gt_autotune_reset(gt_context* ctx);
 

@@ -143,3 +143,19 @@ def test_l2_loss_helper(ctx):
     assert abs(loss - (d ** 2).sum()) <= 1e-6 * (d ** 2).sum()
     np.testing.assert_allclose(g[:, :3], 2 * (a[:, :3] - b[:, :3]), rtol=1e-6)
     assert (g[:, 3] == 0).all()
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_gradient_with_wide_kbuffer(ctx, mode):
+    """A 64-entry k-buffer and a small leaf batch change nothing but speed."""
+    pg = small_scene(n=1500, seed=43)
+    rec = pg.gaussiansBuffer
+    w, h = 48, 40
+    v = view(w, h, k=12)
+    g = np.random.default_rng(5).normal(size=(h, w, 4)).astype(np.float32)
+    s = Scene(ctx, rec, 0.01)
+    ctx.set_tune(s, v.uniforms, w, h, kbuf=64, leaf_batch=8)
+    got, info = ctx.backward(s, v.uniforms, w, h, g, mode=mode)
+    ctx._lib.gt_autotune_reset(ctx._h)
+    assert info["used_mode"] == mode
+    _check(got, _ref_grad(rec, 0.01, v.uniforms, w, h, g))

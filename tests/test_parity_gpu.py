@@ -223,3 +223,21 @@ def test_autotune_keeps_results(ctx):
     assert r["blocks_per_sm"] >= 1 and r["best_ms"] > 0
     after = ctx.render(g, v.uniforms, 64, 64)
     np.testing.assert_array_equal(before, after)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k", [1, 5, 16])
+def test_tuned_shapes_are_bit_exact(ctx, k):
+    """Every k-buffer size and leaf batch gives the same image, bit for bit."""
+    pg = small_scene(n=3000, seed=31)
+    g = Scene(ctx, pg.gaussiansBuffer, 0.01)
+    w, h = 48, 40
+    v = view(w, h, k=k)
+    ref = ctx.render(g, v.uniforms, w, h)
+    for kbuf, lb, b in [(k, 8, 4), (min(32, k + 3), 16, 2), (32, 24, 8), (k, 32, 1), (32, 1, 4), (33, 32, 4),
+                         (48, 16, 4), (64, 32, 4), (64, 5, 2), (80, 32, 4), (128, 32, 4), (100, 12, 3)]:
+        ctx.set_tune(g, v.uniforms, w, h, blocks_per_sm=b, kbuf=kbuf, leaf_batch=lb)
+        np.testing.assert_array_equal(ctx.render(g, v.uniforms, w, h), ref, err_msg=f"kbuf={kbuf} lb={lb}")
+    with pytest.raises(RuntimeError):
+        ctx.set_tune(g, v.uniforms, w, h, kbuf=129)
+    ctx._lib.gt_autotune_reset(ctx._h)

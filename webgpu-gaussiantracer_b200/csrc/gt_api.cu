@@ -127,6 +127,8 @@ static ViewDev make_view(const gt_scene* s, const gt_uniforms& u, uint32_t w, ui
   v.n_tiles = v.tiles_x * ((h + 3) / 4);
   v.tile_begin = tile_begin;
   v.n_particles = s->n;
+  v.kbuf = 32;
+  v.leaf_batch = 32;
   return v;
 }
 
@@ -153,13 +155,19 @@ static void fill_stats(const DevCounters& c, gt_render_stats* st) {
   st->status_flags = c.status;
 }
 
+static std::tuple<uint64_t, uint32_t, uint32_t, uint32_t> tune_key(const gt_scene* s, uint32_t w, uint32_t h,
+                                                                   uint32_t k) {
+  return std::make_tuple((uint64_t)(s ? (uint64_t)log2((double)std::max<uint64_t>(s->b.n_kept, 1)) : 0),
+                         (uint32_t)log2((double)std::max<uint64_t>((uint64_t)w * h, 1)), kmax_for(k), 0u);
+}
+
 static LaunchShape shape_for(gt_context* ctx, const gt_scene* s, uint32_t w, uint32_t h, uint32_t k) {
   LaunchShape sh;
-  auto key = std::make_tuple((uint64_t)(s ? (uint64_t)log2((double)std::max<uint64_t>(s->b.n_kept, 1)) : 0),
-                             (uint32_t)log2((double)std::max<uint64_t>((uint64_t)w * h, 1)), kmax_for(k), 0u);
-  auto it = ctx->tune.find(key);
+  auto it = ctx->tune.find(tune_key(s, w, h, k));
   if (it != ctx->tune.end()) {
     sh.blocks_per_sm = it->second.blocks_per_sm;
+    sh.kbuf = it->second.kbuf;
+    sh.leaf_batch = it->second.leaf_batch;
   }
   return sh;
 }
@@ -513,13 +521,27 @@ extern "C" gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items
     API_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return GT_OK;
   }
-  size_t off = 0;
-  for (uint32_t i = 0; i < count; ++i) {
+  // Views of one scene run back to back (stable order by scene): its nodes
+  // and records then stay in L2 from one view to the next.  Each view keeps
+  // its own output, so the order does not show in the results.
+  std::vector<uint32_t> order(count);
+  for (uint32_t i = 0; i < count; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](uint32_t a, uint32_t b) { return items[a].scene < items[b].scene; });
+  std::vector<size_t> offs(count);
+  {
+    size_t o = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+      offs[i] = o;
+      o += (size_t)items[i].w * items[i].h;
+    }
+  }
+  for (uint32_t q = 0; q < count; ++q) {
+    const uint32_t i = order[q];
     const gt_batch_item& it = items[i];
-    float4* out = (flags & GT_FLAG_OUTPUT_DEVICE) ? reinterpret_cast<float4*>(it.out_rgba) : ctx->staging + off;
-    ctx->h_views[i] = make_view(it.scene, it.u, it.w, it.h, out, total_tiles);
-    total_tiles += ctx->h_views[i].n_tiles;
-    off += (size_t)it.w * it.h;
+    float4* out = (flags & GT_FLAG_OUTPUT_DEVICE) ? reinterpret_cast<float4*>(it.out_rgba) : ctx->staging + offs[i];
+    ctx->h_views[q] = make_view(it.scene, it.u, it.w, it.h, out, total_tiles);
+    total_tiles += ctx->h_views[q].n_tiles;
   }
   API_CUDA(ctx, cudaEventRecord(ctx->call0, ctx->stream));
   uint64_t slot = ring_slot(ctx);
@@ -574,14 +596,10 @@ extern "C" gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const g
   st = ensure_views(ctx, 1);
   if (st != GT_OK) return st;
   ViewDev v = make_view(scene, *u, w, h, ctx->staging, 0);
-  const uint32_t cands[] = {1, 2, 3, 4, 6, 8, 12, 16};
-  float best = 1e30f, def = 0.0f;
-  uint32_t best_b = 4;
-  for (uint32_t b : cands) {
-    LaunchShape sh;
-    sh.blocks_per_sm = b;
+  // fastest of `reps` launches of one shape
+  auto time_shape = [&](const LaunchShape& sh, int reps, float* out_ms) -> gt_status {
     float ms_min = 1e30f;
-    for (int rep = 0; rep < 3; ++rep) {
+    for (int rep = 0; rep < reps; ++rep) {
       API_CUDA(ctx, cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), ctx->stream));
       API_CUDA(ctx, cudaEventRecord(ctx->int0, ctx->stream));
       Err e = launch_trace(&v, 1, v.n_tiles, ctx->d_ctr, ctx->faces, sh, ctx->num_sms, ctx->stream, &ctx->launches,
@@ -593,24 +611,73 @@ extern "C" gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const g
       cudaEventElapsedTime(&ms, ctx->int0, ctx->int1);
       ms_min = std::min(ms_min, ms);
     }
-    if (b == LaunchShape().blocks_per_sm) def = ms_min;
-    if (ms_min < best) {
-      best = ms_min;
-      best_b = b;
+    *out_ms = ms_min;
+    return GT_OK;
+  };
+  // 1. resident blocks per SM at the default traversal settings
+  LaunchShape best_sh;
+  float best = 1e30f, def = 0.0f;
+  const uint32_t cands[] = {1, 2, 3, 4, 6, 8, 12, 16};
+  for (uint32_t b : cands) {
+    LaunchShape sh;
+    sh.blocks_per_sm = b;
+    float ms = 0.0f;
+    st = time_shape(sh, 3, &ms);
+    if (st != GT_OK) return st;
+    if (b == LaunchShape().blocks_per_sm) def = ms;
+    if (ms < best) {
+      best = ms;
+      best_sh = sh;
+    }
+  }
+  // 2. k-buffer size and leaf batch at that occupancy
+  const uint32_t k = u->k;
+  const uint32_t kbufs[] = {k, 32u, 64u, 96u, 128u};
+  const uint32_t batches[] = {8u, 16u, 24u, 32u};
+  for (uint32_t kb : kbufs) {
+    for (uint32_t lb : batches) {
+      LaunchShape sh = best_sh;
+      sh.kbuf = std::min(kMaxKbuf, kb);
+      sh.leaf_batch = lb;
+      if (sh.kbuf == best_sh.kbuf && sh.leaf_batch == best_sh.leaf_batch) continue;
+      float ms = 0.0f;
+      st = time_shape(sh, 2, &ms);
+      if (st != GT_OK) return st;
+      if (ms < best) {
+        best = ms;
+        best_sh = sh;
+      }
     }
   }
   gt_tune_result r;
   memset(&r, 0, sizeof r);
   r.block_threads = 128;
-  r.blocks_per_sm = best_b;
+  r.blocks_per_sm = best_sh.blocks_per_sm;
   r.tile_w = 8;
   r.tile_h = 4;
   r.best_ms = best;
   r.default_ms = def;
-  auto key = std::make_tuple((uint64_t)log2((double)std::max<uint64_t>(scene->b.n_kept, 1)),
-                             (uint32_t)log2((double)std::max<uint64_t>((uint64_t)w * h, 1)), kmax_for(u->k), 0u);
-  ctx->tune[key] = r;
+  r.kbuf = std::max(best_sh.kbuf, k);
+  r.leaf_batch = best_sh.leaf_batch;
+  ctx->tune[tune_key(scene, w, h, k)] = r;
   if (result) *result = r;
+  return GT_OK;
+}
+
+extern "C" gt_status gt_set_tune(gt_context* ctx, const gt_scene* scene, const gt_uniforms* u, uint32_t w,
+                                 uint32_t h, const gt_tune_result* shape) {
+  if (!ctx) return fail(nullptr, GT_ERR_INVALID_ARG, "context is NULL");
+  if (!scene || scene->ctx != ctx) return fail(ctx, GT_ERR_INVALID_ARG, "scene is NULL or from another context");
+  gt_status st = check_uniforms(ctx, u);
+  if (st != GT_OK) return st;
+  if (!shape) return fail(ctx, GT_ERR_INVALID_ARG, "shape is NULL");
+  if (shape->block_threads != 128 || shape->tile_w != 8 || shape->tile_h != 4)
+    return fail(ctx, GT_ERR_INVALID_ARG, "block_threads must be 128 and the tile 8 x 4");
+  if (shape->blocks_per_sm < 1 || shape->blocks_per_sm > 32 || shape->kbuf < 1 || shape->kbuf > kMaxKbuf ||
+      shape->leaf_batch < 1 || shape->leaf_batch > 32)
+    return fail(ctx, GT_ERR_INVALID_ARG, "blocks_per_sm and leaf_batch must lie in 1..32, kbuf in 1..128");
+  gt_tune_result r = *shape;
+  ctx->tune[tune_key(scene, w, h, u->k)] = r;
   return GT_OK;
 }
 

@@ -233,12 +233,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewD
         p = lane < ck.kc ? rr[kCkptHeader + lane] : kInvalid;
         valid = lane < nrec && p != kInvalid;
       } else {
-        float bt = V.u.t_max;
-        uint32_t bp = kInvalid;
-        traverse8<kCollect>(V.s, F, W, o, d, br, ri.x, V.u.t_max, bt, bp, nullptr, st, status, lane);
+        KBuf<1> kb;
+        kbuf_init(kb, V.u.t_max);
+        traverse8<kCollect>(V.s, F, W, o, d, br, ri.x, V.u.t_max, kb, st, status, lane, (int)k, V.leaf_batch);
         if (__reduce_or_sync(kFull, status) & (kStatusStackOverflow | kStatusVisitCap | kStatusHitOverflow)) break;
-        valid = lane < k && lane < nrec && bp != kInvalid;
-        p = bp;
+        valid = lane < k && lane < nrec && kb.p[0] != kInvalid;
+        p = kb.p[0];
       }
       rec = prev;
       const uint32_t vmask = __ballot_sync(kFull, valid);
@@ -552,6 +552,8 @@ gt_status backward_impl(gt_context* ctx, const BwdView* views, uint32_t count, c
     vd[i].grad = G[s];
     off += px;
   }
+  const LaunchShape shape = api_shape_for(ctx, views[0].scene, views[0].w, views[0].h, views[0].u.k);
+  apply_shape(vd.data(), count, shape);
   BWD_TRY(cudaMemcpyAsync(ctx->d_views, vd.data(), sizeof(ViewDev) * count, cudaMemcpyHostToDevice, st));
   Ckpt ck;
   ck.head = cs.head;
@@ -564,7 +566,6 @@ gt_status backward_impl(gt_context* ctx, const BwdView* views, uint32_t count, c
   BWD_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), st));
   BWD_TRY(cudaEventRecord(ctx->int0, st));
   {
-    LaunchShape shape = api_shape_for(ctx, views[0].scene, views[0].w, views[0].h, views[0].u.k);
     uint32_t block = kWarpsPerBlock * 32;
     uint32_t grid = (uint32_t)ctx->num_sms * std::max(1u, shape.blocks_per_sm);
     uint64_t max_grid = ((uint64_t)total_tiles * 32u + kWarpsPerBlock - 1) / kWarpsPerBlock;

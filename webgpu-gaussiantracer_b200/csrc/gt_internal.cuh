@@ -108,16 +108,22 @@ struct ViewDev {
   uint32_t tiles_x;     // tiles per row
   uint32_t tile_begin;  // first global tile index of this view
   uint32_t n_tiles;
+  uint32_t kbuf;        // k-buffer entries (k..128): a traversal keeps the kbuf closest hits
+  uint32_t leaf_batch;  // queued leaves that trigger a batch of proxy tests (8..32)
   const float4* dL;     // backward: dL/drgba (w*h)
   float* grad;          // backward: 59 x n parameter-major gradient
   uint64_t n_particles;
 };
 
 // Launch shape of the persistent trace kernel.
+constexpr uint32_t kMaxKbuf = 128;  // up to four buffer entries per lane
+
 struct LaunchShape {
   uint32_t block_threads = 128;
   uint32_t blocks_per_sm = 4;
-  uint32_t tile_w = 8, tile_h = 4;  // a warp's pixel tile (tile_w*tile_h == 32)
+  uint32_t tile_w = 8, tile_h = 4;  // pixel tile of the work order (tile_w*tile_h == 32)
+  uint32_t kbuf = 64;               // k-buffer entries (raised to k when k is larger; <= kMaxKbuf)
+  uint32_t leaf_batch = 32;         // leaf queue size that triggers proxy tests
 };
 
 // ----------------------------------------------------------- host helpers
@@ -174,8 +180,10 @@ struct Ckpt {
 };
 constexpr uint32_t kCkptHeader = 4;
 
-// Trace launches (gt_trace.cu).
-Err launch_trace(const ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
+// Trace launches (gt_trace.cu).  launch_trace writes the shape's k-buffer
+// size and leaf batch into the host view table before uploading it.
+void apply_shape(ViewDev* views, uint32_t n_views, const LaunchShape& shape);
+Err launch_trace(ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
                  const FaceTable& faces, const LaunchShape& shape, int num_sms, cudaStream_t stream,
                  uint64_t* launches, ViewDev* d_views_scratch, const Ckpt* ckpt = nullptr);
 Err launch_trace_hits(const ViewDev& view, ViewDev* d_views, const uint32_t* pixels, uint32_t n_pix,

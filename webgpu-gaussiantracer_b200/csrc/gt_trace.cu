@@ -47,7 +47,7 @@ __device__ __forceinline__ bool wray_more(const ViewDev& V, const WRay& R) {
 // tracePath (src/GS_shader.ts:192-273) for one pixel, by one warp.
 // RECORD: write the composited hit sequence (gt_render_hits).
 // CKPT: write the round checkpoint the adjoint replays (gt_backward).
-template <bool RECORD, bool CKPT>
+template <bool RECORD, bool CKPT, int NB>
 __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTable& F, WarpScratch& W, uint32_t px,
                                                  uint32_t py, RayStats& st, uint32_t& status, uint32_t lane,
                                                  const HitOut& ho, uint32_t slot, const Ckpt& ck) {
@@ -56,13 +56,13 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
   R.br = make_boxray(R.o, R.d, V.s.scene_mag);
   const float t_max = V.u.t_max;
   if (V.u.debug != 0) {
-    float bt = t_max;
-    uint32_t bp = kInvalid;
+    KBuf<1> kb;
+    kbuf_init(kb, t_max);
     uint32_t cnt = 0;
     if (V.u.debug == 1) {
-      traverse8<kClosestAny>(V.s, F, W, R.o, R.d, R.br, V.u.t_min, t_max, bt, bp, nullptr, st, status, lane);
+      traverse8<kClosestAny>(V.s, F, W, R.o, R.d, R.br, V.u.t_min, t_max, kb, st, status, lane);
       float4 out = make_float4(0.f, 0.f, 0.f, 1.f);
-      uint32_t p0 = __shfl_sync(kFull, bp, 0);
+      uint32_t p0 = __shfl_sync(kFull, kb.p[0], 0);
       if (p0 != kInvalid) {
         float c[3];
         sh_radiance(V.s.sh, p0, R.d, V.u.deg, c);
@@ -77,7 +77,7 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
     }
     // kCountFront: per-lane counts, reduced
     uint32_t before = st.anyhits;
-    traverse8<kCountFront>(V.s, F, W, R.o, R.d, R.br, V.u.t_min, t_max, bt, bp, nullptr, st, status, lane);
+    traverse8<kCountFront>(V.s, F, W, R.o, R.d, R.br, V.u.t_min, t_max, kb, st, status, lane);
     cnt = __reduce_add_sync(kFull, st.anyhits - before);
     float r = 0.f, g = 0.f, b = 0.f;
     if (cnt == 0) {
@@ -102,20 +102,44 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
   const uint32_t k = V.u.k;
   uint32_t ck_head = kInvalid;
   while (wray_more(V, R)) {
-    // one traversal: the 32 closest front-face hits with t > t_curr
-    float bt = t_max;
-    uint32_t bp = kInvalid;
-    traverse8<kCollect>(V.s, F, W, R.o, R.d, R.br, R.t_curr, t_max, bt, bp, nullptr, st, status, lane);
+    // one traversal: the kbuf closest front-face hits with t > t_curr
+    KBuf<NB> kb;
+    kbuf_init(kb, t_max);
+    const int kbuf = (int)V.kbuf;
+    traverse8<kCollect>(V.s, F, W, R.o, R.d, R.br, R.t_curr, t_max, kb, st, status, lane, kbuf, V.leaf_batch);
     // status bits may be set in single lanes: reduce before branching on them
     if (__reduce_or_sync(kFull, status) & (kStatusStackOverflow | kStatusVisitCap | kStatusHitOverflow)) break;
-    const uint32_t cnt = __popc(__ballot_sync(kFull, bp != kInvalid));
-    const bool complete = cnt < 32u;
+    // only entries below kbuf are certain: the far bound was entry kbuf-1
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int j = 0; j < NB; ++j) cnt += __popc(__ballot_sync(kFull, kb.p[j] != kInvalid && 32 * j + (int)lane < kbuf));
+    const bool complete = cnt < (uint32_t)kbuf;
     // rounds served from this buffer
     while (wray_more(V, R)) {
-      const uint32_t skip = __popc(__ballot_sync(kFull, bp != kInvalid && !(bt > R.t_curr)));
+      // entries past kbuf are not counted: hits just beyond entry kbuf-1 can
+      // lie below t_curr
+      uint32_t skip = 0;
+#pragma unroll
+      for (int j = 0; j < NB; ++j)
+        skip += __popc(
+            __ballot_sync(kFull, kb.p[j] != kInvalid && 32 * j + (int)lane < kbuf && !(kb.t[j] > R.t_curr)));
       const uint32_t avail = cnt - skip;
       if (!complete && avail < k) break;  // the next round reaches past the buffer
       const uint32_t n = avail < k ? avail : k;
+      // this round's entries, entry e in lane e
+      const int pos = (int)(skip + lane);
+      const int src = pos & 31;
+      float et = __shfl_sync(kFull, kb.t[0], src);
+      uint32_t ep = __shfl_sync(kFull, kb.p[0], src);
+#pragma unroll
+      for (int j = 1; j < NB; ++j) {
+        const float xt = __shfl_sync(kFull, kb.t[j], src);
+        const uint32_t xp = __shfl_sync(kFull, kb.p[j], src);
+        if ((pos >> 5) == j) {
+          et = xt;
+          ep = xp;
+        }
+      }
       if (CKPT) {
         uint32_t rec = 0;
         if (lane == 0) rec = atomicAdd(ck.pool_next, 1u);
@@ -128,36 +152,34 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
             r[2] = ck_head;
             r[3] = n;
           }
-          uint32_t v = __shfl_sync(kFull, bp, (int)((skip + lane) & 31u));
-          if (lane < ck.kc) r[kCkptHeader + lane] = lane < n ? v : kInvalid;
+          if (lane < ck.kc) r[kCkptHeader + lane] = lane < n ? ep : kInvalid;
           ck_head = rec;
         }
       }
       ++R.step;
       st.rounds += lane == 0 ? 1u : 0u;
-      float new_t = n == k ? __shfl_sync(kFull, bt, (int)(skip + k - 1)) + 1e-4f : t_max;
-      // lanes skip..skip+n-1 hold this round's entries
-      const bool mine = lane >= skip && lane < skip + n;
+      float new_t = n == k ? kbuf_t_at(kb, (int)(skip + k - 1)) + 1e-4f : t_max;
+      const bool mine = lane < n;
       float alpha = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
       bool contrib = false;
       if (mine) {
-        Shade sd = load_shade(V.s.shade, bp);
+        Shade sd = load_shade(V.s.shade, ep);
         alpha = response(sd, R.o, R.d) * sd.opacity;
         contrib = V.u.alpha_min < alpha;
         if (contrib) {
           V3 dir = vnorm(vsub(sd.mu, R.o));
           float c[3];
-          sh_radiance(V.s.sh, bp, dir, V.u.deg, c);
+          sh_radiance(V.s.sh, ep, dir, V.u.deg, c);
           c0 = c[0] > 0.f ? c[0] : 0.f;
           c1 = c[1] > 0.f ? c[1] : 0.f;
           c2 = c[2] > 0.f ? c[2] : 0.f;
         }
         if (RECORD) {
-          uint32_t e = R.n_entries + (lane - skip);
+          uint32_t e = R.n_entries + lane;
           if (e < ho.max_entries) {
             size_t at = (size_t)slot * ho.max_entries + e;
-            ho.pidx[at] = bp;
-            ho.t[at] = bt;
+            ho.pidx[at] = ep;
+            ho.t[at] = et;
             ho.alpha[at] = alpha;
           }
         }
@@ -167,12 +189,11 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
       st.contributing += lane == 0 ? __popc(cmask) : 0u;
       // front-to-back accumulation in entry order
       for (uint32_t e = 0; e < n; ++e) {
-        const int src = (int)(skip + e);
-        float a = __shfl_sync(kFull, alpha, src);
-        float x0 = __shfl_sync(kFull, c0, src);
-        float x1 = __shfl_sync(kFull, c1, src);
-        float x2 = __shfl_sync(kFull, c2, src);
-        if ((cmask >> src) & 1u) {
+        float a = __shfl_sync(kFull, alpha, (int)e);
+        float x0 = __shfl_sync(kFull, c0, (int)e);
+        float x1 = __shfl_sync(kFull, c1, (int)e);
+        float x2 = __shfl_sync(kFull, c2, (int)e);
+        if ((cmask >> e) & 1u) {
           float ta = R.T * a;
           R.L0 = R.L0 + ta * x0;
           R.L1 = R.L1 + ta * x1;
@@ -199,7 +220,7 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
 // Persistent kernel: each warp takes one pixel slot at a time from a global
 // counter (slot = 32 * tile + position in the 8x4 tile, views back to back),
 // so neighbouring pixels run on neighbouring warps at the same time.
-template <bool RECORD, bool CKPT>
+template <bool RECORD, bool CKPT, int NB>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_trace8(const ViewDev* __restrict__ views, uint32_t n_views,
                                                                   uint32_t total_tiles, DevCounters* ctr,
                                                                   const __grid_constant__ FaceTable F,
@@ -233,7 +254,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_trace8(const ViewDev
       if (px >= V.w || py >= V.h) continue;
     }
     const ViewDev& V = views[vi];
-    float4 r = trace_ray_warp<RECORD, CKPT>(V, F, W, px, py, st, status, lane, ho, item, ck);
+    float4 r = trace_ray_warp<RECORD, CKPT, NB>(V, F, W, px, py, st, status, lane, ho, item, ck);
     if (lane == 0) {
       if (RECORD) {
         if (ho.rgba) ho.rgba[item] = r;
@@ -248,9 +269,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_trace8(const ViewDev
 
 uint32_t kmax_for(uint32_t k) { return k <= 8 ? 8u : (k <= 16 ? 16u : 32u); }
 
-Err launch_trace(const ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
-                  const FaceTable& faces, const LaunchShape& shape, int num_sms, cudaStream_t stream,
-                  uint64_t* launches, ViewDev* d_views, const Ckpt* ckpt) {
+void apply_shape(ViewDev* views, uint32_t n_views, const LaunchShape& shape) {
+  for (uint32_t i = 0; i < n_views; ++i) {
+    uint32_t kb = std::min(kMaxKbuf, std::max(shape.kbuf, views[i].u.k));
+    views[i].kbuf = std::max(1u, kb);
+    views[i].leaf_batch = std::min(32u, std::max(1u, shape.leaf_batch));
+  }
+}
+
+Err launch_trace(ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
+                 const FaceTable& faces, const LaunchShape& shape, int num_sms, cudaStream_t stream,
+                 uint64_t* launches, ViewDev* d_views, const Ckpt* ckpt) {
+  apply_shape(views, n_views, shape);
   GT_CUDA_TRY(cudaMemcpyAsync(d_views, views, sizeof(ViewDev) * n_views, cudaMemcpyHostToDevice, stream));
   uint32_t block = kWarpsPerBlock * 32;
   uint32_t grid = (uint32_t)num_sms * std::max(1u, shape.blocks_per_sm);
@@ -258,12 +288,26 @@ Err launch_trace(const ViewDev* views, uint32_t n_views, uint32_t total_tiles, D
   uint64_t max_grid = (warps_needed + kWarpsPerBlock - 1) / kWarpsPerBlock;
   if (grid > max_grid) grid = (uint32_t)std::max<uint64_t>(1, max_grid);
   HitOut ho{};
+  // buffer slots per lane: enough for the widest k-buffer of the batch
+  uint32_t kmax = 1;
+  for (uint32_t i = 0; i < n_views; ++i) kmax = std::max(kmax, views[i].kbuf);
+  const uint32_t nb = (kmax + 31u) / 32u;
+  const Ckpt ck = ckpt ? *ckpt : Ckpt{};
+  const void* fn;
   if (ckpt)
-    k_trace8<false, true><<<grid, block, 0, stream>>>(d_views, n_views, total_tiles, counters, faces, nullptr, 0u, ho,
-                                                      *ckpt);
+    fn = nb <= 1 ? (const void*)k_trace8<false, true, 1>
+                 : nb == 2 ? (const void*)k_trace8<false, true, 2>
+                           : nb == 3 ? (const void*)k_trace8<false, true, 3> : (const void*)k_trace8<false, true, 4>;
   else
-    k_trace8<false, false><<<grid, block, 0, stream>>>(d_views, n_views, total_tiles, counters, faces, nullptr, 0u, ho,
-                                                       Ckpt{});
+    fn = nb <= 1 ? (const void*)k_trace8<false, false, 1>
+                 : nb == 2 ? (const void*)k_trace8<false, false, 2>
+                           : nb == 3 ? (const void*)k_trace8<false, false, 3> : (const void*)k_trace8<false, false, 4>;
+  const ViewDev* dv = d_views;
+  const uint32_t* no_pix = nullptr;
+  uint32_t zero = 0;
+  void* args[] = {(void*)&dv, (void*)&n_views, (void*)&total_tiles, (void*)&counters, (void*)&faces,
+                  (void*)&no_pix, (void*)&zero, (void*)&ho, (void*)&ck};
+  GT_CUDA_TRY(cudaLaunchKernel(fn, dim3(grid), dim3(block), args, 0, stream));
   ++*launches;
   GT_CUDA_TRY(cudaGetLastError());
   return Err{};
@@ -277,7 +321,7 @@ Err launch_trace_hits(const ViewDev& view, ViewDev* d_views, const uint32_t* pix
   GT_CUDA_TRY(cudaMemcpyAsync(d_views, &view, sizeof(ViewDev), cudaMemcpyHostToDevice, stream));
   HitOut ho{out_pidx, out_t, out_alpha, out_count, out_rounds, out_rgba, max_entries};
   uint32_t grid = std::min<uint32_t>((n_pix + kWarpsPerBlock - 1) / kWarpsPerBlock, 148u * 8u);
-  k_trace8<true, false><<<grid, kWarpsPerBlock * 32, 0, stream>>>(d_views, 1, 0, counters, faces, pixels, n_pix, ho,
+  k_trace8<true, false, 1><<<grid, kWarpsPerBlock * 32, 0, stream>>>(d_views, 1, 0, counters, faces, pixels, n_pix, ho,
                                                                   Ckpt{});
   ++*launches;
   GT_CUDA_TRY(cudaGetLastError());

@@ -30,6 +30,7 @@ struct WarpScratch {
   float st[kWarpStack];
   uint32_t leafq[kLeafQueue];
   float leaft[kLeafQueue];
+  uint32_t pop[4];  // nodes taken by the current pop (lanes 8s..8s+7 test pop[s])
 };
 
 struct HitOut {
@@ -83,22 +84,86 @@ __device__ __forceinline__ void warp_sort_prefix(float& key, uint32_t& val, uint
   }
 }
 
-// Inserts (t, p) into the warp k-buffer (lane i = i-th closest, ascending in
-// (t, particle index)).  Entries greater than the hit form a suffix.
-__device__ __forceinline__ void warp_insert(float& bt, uint32_t& bp, float t, uint32_t p, uint32_t lane) {
-  bool after = t < bt || (t == bt && p < bp);
-  uint32_t m = __ballot_sync(kFull, after);
-  if (m) {
-    int pos = __ffs(m) - 1;
-    float ut = __shfl_up_sync(kFull, bt, 1);
-    uint32_t up = __shfl_up_sync(kFull, bp, 1);
-    if ((int)lane > pos) {
-      bt = ut;
-      bp = up;
-    }
-    if ((int)lane == pos) {
-      bt = t;
-      bp = p;
+// Warp k-buffer of 32*NB entries ascending in (t, particle index): entry
+// 32*j + lane lives in lane `lane`, slot j.  Unused entries are (t_max,
+// kInvalid), which sort after every hit.
+template <int NB>
+struct KBuf {
+  float t[NB];
+  uint32_t p[NB];
+};
+
+template <int NB>
+__device__ __forceinline__ void kbuf_init(KBuf<NB>& b, float t_max) {
+#pragma unroll
+  for (int j = 0; j < NB; ++j) {
+    b.t[j] = t_max;
+    b.p[j] = kInvalid;
+  }
+}
+
+// Value of entry idx (warp-uniform idx < 32*NB), broadcast to all lanes.
+// (One shuffle per slot: selecting the slot first with a runtime index made
+// the compiler move the whole buffer to local memory.)
+template <int NB>
+__device__ __forceinline__ float kbuf_t_at(const KBuf<NB>& b, int idx) {
+  float v = __shfl_sync(kFull, b.t[0], idx & 31);
+#pragma unroll
+  for (int j = 1; j < NB; ++j) {
+    const float x = __shfl_sync(kFull, b.t[j], idx & 31);
+    v = (idx >> 5) == j ? x : v;
+  }
+  return v;
+}
+
+// Inserts (t, p): entries greater than the hit form a suffix that moves up
+// by one position (the last entry drops out).
+template <int NB>
+__device__ __forceinline__ void kbuf_insert(KBuf<NB>& b, float t, uint32_t p, uint32_t lane) {
+  bool moved = false;  // warp-uniform: the hit went into an earlier slot
+  float ct = 0.f;      // lane 31's entry of the previous slot, before the move
+  uint32_t cp = 0;
+#pragma unroll
+  for (int j = 0; j < NB; ++j) {
+    if (moved) {
+      float ut = __shfl_up_sync(kFull, b.t[j], 1);
+      uint32_t up = __shfl_up_sync(kFull, b.p[j], 1);
+      if (j + 1 < NB) {
+        const float nt = __shfl_sync(kFull, b.t[j], 31);
+        const uint32_t np = __shfl_sync(kFull, b.p[j], 31);
+        if (lane == 0) {
+          ut = ct;
+          up = cp;
+        }
+        ct = nt;
+        cp = np;
+      } else if (lane == 0) {
+        ut = ct;
+        up = cp;
+      }
+      b.t[j] = ut;
+      b.p[j] = up;
+    } else {
+      const bool after = t < b.t[j] || (t == b.t[j] && p < b.p[j]);
+      const uint32_t m = __ballot_sync(kFull, after);
+      if (m) {
+        const int pos = __ffs(m) - 1;
+        if (j + 1 < NB) {
+          ct = __shfl_sync(kFull, b.t[j], 31);
+          cp = __shfl_sync(kFull, b.p[j], 31);
+        }
+        const float ut = __shfl_up_sync(kFull, b.t[j], 1);
+        const uint32_t up = __shfl_up_sync(kFull, b.p[j], 1);
+        if ((int)lane > pos) {
+          b.t[j] = ut;
+          b.p[j] = up;
+        }
+        if ((int)lane == pos) {
+          b.t[j] = t;
+          b.p[j] = p;
+        }
+        moved = true;
+      }
     }
   }
 }
@@ -107,18 +172,21 @@ __device__ __forceinline__ void warp_insert(float& bt, uint32_t& bp, float t, ui
 enum TraverseMode { kCollect = 0, kClosestAny = 1, kCountFront = 2 };
 
 // Warp-cooperative traversal from the root with interval (tlo, t_max).
-//   kCollect:    the 32 closest front-face hits go into (bt, bp)
-//   kClosestAny: the closest hit of any facing goes into lane 0 of (bt, bp)
-//   kCountFront: every front-face hit is counted into *count
-// Far bound of the box tests: the buffer's last entry (kCollect), its first
-// entry (kClosestAny) or t_max (kCountFront).
-template <int MODE>
+//   kCollect:    the closest front-face hits go into the k-buffer kb
+//   kClosestAny: the closest hit of any facing goes into entry 0 of kb
+//   kCountFront: every front-face hit is counted into st.anyhits
+// Far bound of the box tests: entry kbuf-1 of the buffer (kCollect; the
+// entries past it are not exact), entry 0 (kClosestAny) or t_max
+// (kCountFront).  leaf_batch: queued leaves that trigger a batch of proxy
+// tests (<= 32).
+template <int MODE, int NB>
 __device__ __forceinline__ void traverse8(const SceneDev& S, const FaceTable& F, WarpScratch& W, V3 o, V3 d,
-                                          const BoxRay& br, float tlo, float t_max, float& bt, uint32_t& bp,
-                                          uint32_t* count, RayStats& st, uint32_t& status, uint32_t lane) {
+                                          const BoxRay& br, float tlo, float t_max, KBuf<NB>& kb,
+                                          RayStats& st, uint32_t& status, uint32_t lane,
+                                          int kbuf = 32 * NB, int leaf_batch = 32) {
   if (S.n_kept == 0) return;
   const uint32_t lt_mask = (1u << lane) - 1u;
-  const int cull_lane = MODE == kClosestAny ? 0 : 31;
+  const int cull = MODE == kClosestAny ? 0 : kbuf - 1;  // the entry that bounds the search
   int sp = 0, nq = 0;
   if (lane == 0) {
     W.snode[0] = 0;
@@ -126,7 +194,7 @@ __device__ __forceinline__ void traverse8(const SceneDev& S, const FaceTable& F,
   }
   sp = 1;
   __syncwarp();
-  float thi = MODE == kCountFront ? t_max : __shfl_sync(kFull, bt, cull_lane);
+  float thi = MODE == kCountFront ? t_max : kbuf_t_at(kb, cull);
   uint32_t iters = 0;
   const uint32_t max_iters = 4u * S.n_kept + 64u;
   while (true) {
@@ -134,26 +202,33 @@ __device__ __forceinline__ void traverse8(const SceneDev& S, const FaceTable& F,
       status |= kStatusVisitCap;
       return;
     }
-    // pop up to 4 nodes still in range (kept in registers: no indexed array)
-    uint32_t pn0 = 0, pn1 = 0, pn2 = 0, pn3 = 0;
+    // pop: lanes 0..7 read the top 8 stack entries at once and the first
+    // (top-most) entries still in range are taken, up to 4 in all, through a
+    // 4-slot array in shared memory; out-of-range entries above the last one
+    // taken are dropped (the far bound only shrinks).  __fns is avoided: it is
+    // a software loop and made this step slower than a serial pop.
     int np = 0;
     while (np < 4 && sp > 0) {
-      --sp;
-      float t = W.st[sp];
-      uint32_t n = W.snode[sp];
-      if (t <= thi) {
-        pn3 = pn2;
-        pn2 = pn1;
-        pn1 = pn0;
-        pn0 = n;
-        ++np;
+      const int avail = sp < 8 ? sp : 8;
+      bool ok = false;
+      uint32_t en = 0;
+      if ((int)lane < avail) {
+        const float et = W.st[sp - 1 - (int)lane];
+        en = W.snode[sp - 1 - (int)lane];
+        ok = et <= thi;
       }
+      const uint32_t okm = __ballot_sync(kFull, ok);
+      const int r = np + __popc(okm & lt_mask);
+      if (ok && r < 4) W.pop[r] = en;
+      const uint32_t m4 = __ballot_sync(kFull, ok && r == 3);
+      sp -= m4 ? __ffs(m4) : avail;
+      np = np + __popc(okm) < 4 ? np + __popc(okm) : 4;
     }
     __syncwarp();
     if (np > 0) {
       const int slot = (int)(lane >> 3);
       const bool valid = slot < np;
-      uint32_t node = slot == 0 ? pn0 : slot == 1 ? pn1 : slot == 2 ? pn2 : pn3;
+      const uint32_t node = W.pop[slot];
       float tnear = CUDART_INF_F;
       uint32_t ref = kInvalid;
       bool hit = false;
@@ -187,22 +262,34 @@ __device__ __forceinline__ void traverse8(const SceneDev& S, const FaceTable& F,
           status |= kStatusStackOverflow;
           return;
         }
-        // gather the m hit children into lanes 0..m-1, then sort that segment
-        const uint32_t src = (int)lane < m ? __fns(imask, 0, (int)lane + 1) : lane;
-        float key = __shfl_sync(kFull, tnear, src);
-        uint32_t val = __shfl_sync(kFull, ref, src);
-        if ((int)lane >= m) key = CUDART_INF_F;
-        if (m > 1) warp_sort_prefix(key, val, lane, m);
-        if ((int)lane < m) {
-          W.snode[sp + m - 1 - (int)lane] = val;
-          W.st[sp + m - 1 - (int)lane] = key;
+        // the m hit children are written to stack slots sp..sp+m-1 in lane
+        // order, then read back into lanes 0..m-1, sorted and stored far-to-near
+        if (hit && !leaf) {
+          const int r = __popc(imask & lt_mask);
+          W.snode[sp + r] = ref;
+          W.st[sp + r] = tnear;
+        }
+        __syncwarp();
+        if (m > 1) {
+          float key = CUDART_INF_F;
+          uint32_t val = 0;
+          if ((int)lane < m) {
+            key = W.st[sp + (int)lane];
+            val = W.snode[sp + (int)lane];
+          }
+          warp_sort_prefix(key, val, lane, m);
+          __syncwarp();
+          if ((int)lane < m) {
+            W.snode[sp + m - 1 - (int)lane] = val;
+            W.st[sp + m - 1 - (int)lane] = key;
+          }
         }
         sp += m;
       }
       __syncwarp();
     }
     const bool drain = sp == 0;
-    if (nq >= 32 || (drain && nq > 0)) {
+    if (nq >= leaf_batch || (drain && nq > 0)) {
       const int nb = nq < 32 ? nq : 32;
       uint32_t j = 0;
       bool have = (int)lane < nb;
@@ -266,9 +353,9 @@ __device__ __forceinline__ void traverse8(const SceneDev& S, const FaceTable& F,
             h4 = h5;
             --nh;
           }
-          warp_insert(bt, bp, t, pp, lane);
+          kbuf_insert(kb, t, pp, lane);
         }
-        thi = __shfl_sync(kFull, bt, cull_lane);
+        thi = kbuf_t_at(kb, cull);
       }
     }
     if (sp == 0 && nq == 0) break;

@@ -68,7 +68,8 @@ class BatchItem(C.Structure):
 
 class TuneResult(C.Structure):
     _fields_ = [("block_threads", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("tile_w", C.c_uint32),
-                ("tile_h", C.c_uint32), ("best_ms", C.c_float), ("default_ms", C.c_float)]
+                ("tile_h", C.c_uint32), ("best_ms", C.c_float), ("default_ms", C.c_float),
+                ("kbuf", C.c_uint32), ("leaf_batch", C.c_uint32)]
 
 
 assert C.sizeof(Uniforms) == 112
@@ -94,6 +95,7 @@ SIGNATURES = [
                                  C.POINTER(BwdOpts), C.POINTER(RenderStats)]),
     ("gt_l2_loss", _i32, [_vp, _vp, _vp, _u64, _vp, C.POINTER(C.c_double)]),
     ("gt_autotune", _i32, [_vp, _vp, C.POINTER(Uniforms), _u32, _u32, C.POINTER(TuneResult)]),
+    ("gt_set_tune", _i32, [_vp, _vp, C.POINTER(Uniforms), _u32, _u32, C.POINTER(TuneResult)]),
     ("gt_autotune_reset", _i32, [_vp]),
     ("gt_device_alloc", _i32, [_vp, _u64, C.POINTER(_vp)]),
     ("gt_device_free", _i32, [_vp, _vp]),

@@ -219,6 +219,13 @@ class Context:
                                          C.byref(r)))
         return {name: getattr(r, name) for name, _ in r._fields_}
 
+    def set_tune(self, scene: "Scene", uniforms, width: int, height: int, blocks_per_sm: int = 4,
+                 kbuf: int = 32, leaf_batch: int = 32):
+        """Installs a launch shape for this (scene, k, image size) bucket."""
+        r = L.TuneResult(128, blocks_per_sm, 8, 4, 0.0, 0.0, kbuf, leaf_batch)
+        self.check(self._lib.gt_set_tune(self._h, scene.handle, C.byref(_uniforms(uniforms)), width, height,
+                                         C.byref(r)))
+
     # ----------------------------------------------------------- helpers
     def device_alloc(self, nbytes: int) -> int:
         p = C.c_void_p()
