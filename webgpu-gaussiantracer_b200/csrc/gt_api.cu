@@ -548,7 +548,12 @@ extern "C" gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items
   API_CUDA(ctx, cudaEventRecord(ctx->ring[2 * slot], ctx->stream));
   // One graph per batch shape: counter reset + the persistent kernel.
   LaunchShape shape = shape_for(ctx, items[0].scene, items[0].w, items[0].h, items[0].u.k);
-  auto key = std::make_tuple(count, total_tiles, kmax, shape.blocks_per_sm);
+  // the view table is rebuilt on every call: it takes the shape's k-buffer
+  // size and leaf batch here, and the graph's kernel matches its slot count
+  apply_shape(ctx->h_views, count, shape);
+  uint32_t kb_max = 1;
+  for (uint32_t q = 0; q < count; ++q) kb_max = std::max(kb_max, ctx->h_views[q].kbuf);
+  auto key = std::make_tuple(count, total_tiles, kmax, shape.blocks_per_sm, (kb_max + 31u) / 32u);
   auto it = ctx->graphs.find(key);
   if (it == ctx->graphs.end()) {
     GraphEntry g;

@@ -64,7 +64,8 @@ struct gt_context {
   uint64_t ring_head = 0, ring_tail = 0;
   uint64_t launches = 0;
   std::map<std::tuple<uint64_t, uint32_t, uint32_t, uint32_t>, gt_tune_result> tune;
-  std::map<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t>, gt::GraphEntry> graphs;
+  // batch graphs by (views, tiles, k bucket, blocks per SM, k-buffer slots)
+  std::map<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t, uint32_t>, gt::GraphEntry> graphs;
   std::set<gt_scene*> scenes;  // live scenes; destroyed with the context
   gt::CkptStore ckpt;
 };

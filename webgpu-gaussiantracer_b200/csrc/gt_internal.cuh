@@ -120,7 +120,7 @@ constexpr uint32_t kMaxKbuf = 128;  // up to four buffer entries per lane
 
 struct LaunchShape {
   uint32_t block_threads = 128;
-  uint32_t blocks_per_sm = 4;
+  uint32_t blocks_per_sm = 8;
   uint32_t tile_w = 8, tile_h = 4;  // pixel tile of the work order (tile_w*tile_h == 32)
   uint32_t kbuf = 64;               // k-buffer entries (raised to k when k is larger; <= kMaxKbuf)
   uint32_t leaf_batch = 32;         // leaf queue size that triggers proxy tests

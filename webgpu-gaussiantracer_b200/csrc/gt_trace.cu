@@ -220,8 +220,12 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
 // Persistent kernel: each warp takes one pixel slot at a time from a global
 // counter (slot = 32 * tile + position in the 8x4 tile, views back to back),
 // so neighbouring pixels run on neighbouring warps at the same time.
+// 8 resident blocks (32 warps per SM, 64 registers a thread) beat 4 blocks
+// without spills by 12% on the 1M-Gaussian 1080p view: the kernel is bound by
+// dependent latencies, and more warps hide them better than the spill loads
+// cost (measured 4/5/6/8/10/12/16 blocks: 111/105/104/98/112/121/140 ms).
 template <bool RECORD, bool CKPT, int NB>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_trace8(const ViewDev* __restrict__ views, uint32_t n_views,
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) k_trace8(const ViewDev* __restrict__ views, uint32_t n_views,
                                                                   uint32_t total_tiles, DevCounters* ctr,
                                                                   const __grid_constant__ FaceTable F,
                                                                   const uint32_t* pixels, uint32_t n_pix,
