@@ -60,6 +60,9 @@ enum {
 #define GT_FLAG_ACCUMULATE     0x8u  /* backward: add into dL_dparams         */
 #define GT_FLAG_CHECKPOINT     0x10u /* render: keep the round checkpoint in the context;
                                         backward: reuse it when the views match  */
+#define GT_FLAG_FAST_BUILD     0x20u /* scene: Morton-prefix (LBVH) hierarchy instead
+                                        of surface-area clustering: builds faster,
+                                        traces slower (scenes rebuilt every step) */
 
 /* -------------------------------------------------------- opaque handles */
 typedef struct gt_context gt_context;
@@ -147,9 +150,12 @@ gt_status gt_last_error(const gt_context* ctx, char* buf, size_t len);
  *   alpha_min     proxy cut: particle i gets a proxy iff opacity > alpha_min;
  *                 its icosahedron is scaled by sqrt(2 ln(opacity/alpha_min))
  *                 (src/main.ts:79-87).  A double, like the JS number it replaces.
- *   flags         GT_FLAG_INPUT_DEVICE if `packed` is a device pointer
- * The build (proxy transforms, Morton codes, radix sort, hierarchy, refit)
- * runs on the GPU.  n == 0 gives an empty scene that renders black. */
+ *   flags         GT_FLAG_INPUT_DEVICE if `packed` is a device pointer,
+ *                 GT_FLAG_FAST_BUILD for the Karras LBVH hierarchy
+ * The build (proxy transforms, Morton codes, radix sort, binary hierarchy by
+ * PLOC clustering or LBVH, 8-wide collapse) runs on the GPU.  Any hierarchy
+ * gives the same images: only the traversal cost differs.  n == 0 gives an
+ * empty scene that renders black. */
 gt_status gt_scene_create(gt_context* ctx, const void* packed, uint64_t n,
                           uint32_t stride_bytes, double alpha_min,
                           uint32_t flags, gt_scene** out);

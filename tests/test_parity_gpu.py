@@ -241,3 +241,36 @@ def test_tuned_shapes_are_bit_exact(ctx, k):
     with pytest.raises(RuntimeError):
         ctx.set_tune(g, v.uniforms, w, h, kbuf=129)
     ctx._lib.gt_autotune_reset(ctx._h)
+
+
+@pytest.mark.gpu
+def test_hierarchies_give_identical_images(ctx):
+    """The PLOC and LBVH hierarchies change the traversal order only."""
+    pg = small_scene(n=5000, seed=37)
+    w, h = 56, 40
+    for k in (3, 16):
+        v = view(w, h, k=k)
+        a = ctx.render(Scene(ctx, pg.gaussiansBuffer, 0.01), v.uniforms, w, h)
+        b = ctx.render(Scene(ctx, pg.gaussiansBuffer, 0.01, fast_build=True), v.uniforms, w, h)
+        np.testing.assert_array_equal(a, b)
+        ref, _ = oracle.Scene(pg.gaussiansBuffer, 0.01, "f32").render(v.uniforms, w, h)
+        np.testing.assert_array_equal(a.reshape(-1, 4), ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [2, 3, 40])
+def test_clustering_with_coincident_particles(ctx, n):
+    """Identical particles tie in every merge distance; the build must still
+    finish and render what the oracle renders."""
+    pg = small_scene(n=1, seed=38)
+    rec = np.repeat(pg.gaussiansBuffer[:1], n, axis=0)
+    rec[:, 0:3] = 0.0    # at the origin
+    rec[:, 4:7] = 0.3    # scales (activated)
+    rec[:, 12] = 0.9     # opacity well above alpha_min
+    w, h = 24, 20
+    v = view(w, h, pos=(0.0, 0.0, 3.0), k=4)
+    s = Scene(ctx, rec, 0.01)
+    assert s.info()["n_kept"] == n
+    img = ctx.render(s, v.uniforms, w, h)
+    ref, _ = oracle.Scene(rec, 0.01, "f32").render(v.uniforms, w, h)
+    np.testing.assert_array_equal(img.reshape(-1, 4), ref)

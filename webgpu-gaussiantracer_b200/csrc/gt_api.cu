@@ -297,7 +297,8 @@ extern "C" gt_status gt_scene_create(gt_context* ctx, const void* packed, uint64
   s->stride = stride_bytes;
   s->alpha_min = alpha_min;
   cudaEventRecord(ctx->call0, ctx->stream);
-  Err e = build_scene(dev, n, stride_bytes, alpha_min, ctx->stream, &s->b, &ctx->launches);
+  Err e = build_scene(dev, n, stride_bytes, alpha_min, ctx->stream, &s->b, &ctx->launches,
+                      (flags & GT_FLAG_FAST_BUILD) != 0);
   cudaEventRecord(ctx->call1, ctx->stream);
   cudaStreamSynchronize(ctx->stream);
   if (tmp) cudaFree(tmp);

@@ -327,7 +327,7 @@ __global__ void k_scan_add(uint32_t* out, uint64_t n, const uint32_t* tile_offse
 
 // Exclusive scan of n uint32 values (in may equal out).  Temporaries are
 // stream-ordered allocations.
-static Err scan_exclusive(const uint32_t* in, uint32_t* out, uint64_t n, cudaStream_t st, uint64_t* launches) {
+Err scan_exclusive(const uint32_t* in, uint32_t* out, uint64_t n, cudaStream_t st, uint64_t* launches) {
   if (n == 0) return Err{};
   uint64_t tiles = (n + kScanTile - 1) / kScanTile;
   if (tiles == 1) {
@@ -754,7 +754,7 @@ void free_scene(SceneBuffers* b) {
 static inline unsigned grid_for(uint64_t n, unsigned block) { return (unsigned)((n + block - 1) / block); }
 
 Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride, double alpha_min, cudaStream_t st,
-                SceneBuffers* out, uint64_t* launches) {
+                SceneBuffers* out, uint64_t* launches, bool fast_build) {
   SceneBuffers b;
   b.n_sh = std::min<uint32_t>(16u, (stride - 64u) / 16u);
   const uint8_t* packed = static_cast<const uint8_t*>(packed_dev);
@@ -833,10 +833,16 @@ Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride, double alph
                                           leaf_box);
   ++*launches;
   if (m > 1) {
-    k_karras<<<grid_for(n_int, B), B, 0, st>>>(keys, (int)m, b.nodes, parent_int, parent_leaf);
-    k_refit<<<grid_for(m, B), B, 0, st>>>(m, leaf_box, ibox, b.nodes, parent_int, parent_leaf, arrive);
+    if (fast_build) {
+      k_karras<<<grid_for(n_int, B), B, 0, st>>>(keys, (int)m, b.nodes, parent_int, parent_leaf);
+      k_refit<<<grid_for(m, B), B, 0, st>>>(m, leaf_box, ibox, b.nodes, parent_int, parent_leaf, arrive);
+      *launches += 2;
+    } else {
+      Err pe = build_ploc(leaf_box, m, st, b.nodes, ibox, parent_int, parent_leaf, launches);
+      if (pe.code != GT_OK) return pe;
+    }
     k_depth<<<grid_for(m, B), B, 0, st>>>(m, parent_int, parent_leaf, depth);
-    *launches += 3;
+    *launches += 1;
     // structural check: refcount over [internal 0..m-2 | leaves 0..m-1]
     uint32_t* refc = nullptr;
     GT_CUDA_TRY(cudaMallocAsync(&refc, (size_t)(2 * m - 1) * 4, st));

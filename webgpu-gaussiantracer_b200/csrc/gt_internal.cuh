@@ -159,8 +159,16 @@ struct SceneBuffers {
   float scene_mag = 0;
   uint64_t bytes = 0;
 };
+// fast_build: Karras LBVH (a few ms for 1M proxies); otherwise PLOC
+// clustering (slower to build, faster to trace).
 Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride_bytes, double alpha_min,
-                cudaStream_t stream, SceneBuffers* out, uint64_t* launches);
+                cudaStream_t stream, SceneBuffers* out, uint64_t* launches, bool fast_build = false);
+// Binary hierarchy over m leaves in Morton order by PLOC (gt_ploc.cu): root 0,
+// node format and parent links as the Karras build plus refit produce them.
+Err build_ploc(const float* leaf_box, uint32_t m, cudaStream_t st, float4* nodes, float* ibox, uint32_t* parent_int,
+               uint32_t* parent_leaf, uint64_t* launches);
+// Exclusive prefix sum of n words (gt_build.cu).
+Err scan_exclusive(const uint32_t* in, uint32_t* out, uint64_t n, cudaStream_t st, uint64_t* launches);
 void free_scene(SceneBuffers* b);
 
 // Round checkpoint written by the forward pass of gt_backward.  Each traced

@@ -26,6 +26,7 @@ GT_FLAG_OUTPUT_DEVICE = 0x2
 GT_FLAG_ASYNC = 0x4
 GT_FLAG_ACCUMULATE = 0x8
 GT_FLAG_CHECKPOINT = 0x10
+GT_FLAG_FAST_BUILD = 0x20
 
 STATUS_NAMES = {GT_OK: "GT_OK", GT_ERR_INVALID_ARG: "GT_ERR_INVALID_ARG", GT_ERR_OOM: "GT_ERR_OOM",
                 GT_ERR_CUDA: "GT_ERR_CUDA", GT_ERR_DEVICE_TIMEOUT: "GT_ERR_DEVICE_TIMEOUT",

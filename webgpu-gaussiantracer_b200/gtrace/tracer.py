@@ -276,20 +276,22 @@ class Scene:
     """Proxies + BVH + shading records of one packed particle buffer, on the GPU."""
 
     def __init__(self, ctx: Context, packed: np.ndarray, alpha_min: float, device_ptr: int | None = None,
-                 n: int | None = None, stride: int | None = None):
+                 n: int | None = None, stride: int | None = None, fast_build: bool = False):
+        """fast_build: Karras LBVH hierarchy (quicker build, slower traversal)."""
         self.ctx = ctx
         self._lib = ctx._lib
         h = C.c_void_p()
+        fb = L.GT_FLAG_FAST_BUILD if fast_build else 0
         if device_ptr is not None:
             self.n = int(n)
             ctx.check(self._lib.gt_scene_create(ctx.handle, C.c_void_p(device_ptr), self.n, int(stride),
-                                                float(alpha_min), L.GT_FLAG_INPUT_DEVICE, C.byref(h)))
+                                                float(alpha_min), L.GT_FLAG_INPUT_DEVICE | fb, C.byref(h)))
         else:
             arr = np.ascontiguousarray(packed, dtype=np.float32)
             self.n = arr.shape[0]
             stride = arr.shape[1] * 4 if arr.ndim == 2 and self.n else 320
             ctx.check(self._lib.gt_scene_create(ctx.handle, arr.ctypes.data_as(C.c_void_p) if self.n else None,
-                                                self.n, stride, float(alpha_min), 0, C.byref(h)))
+                                                self.n, stride, float(alpha_min), fb, C.byref(h)))
         self._h = h
         self.alpha_min = alpha_min
         ctx._scenes.add(self)
