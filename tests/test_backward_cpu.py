@@ -1,5 +1,6 @@
 """CPU check of the adjoint formulas: the oracle's FP64 analytic gradient
-against central finite differences of its FP64 render (h = 1e-4).
+against central finite differences of its FP64 render (h = 1e-4) on 256
+randomly chosen (particle, parameter) pairs.
 
 Samples whose +h and -h renders differ in any hit sequence or in which
 entries pass alpha_min straddle a discontinuity of the piecewise-smooth
@@ -49,8 +50,9 @@ def test_fp64_adjoint_matches_central_differences(seed):
                            zip(base_hits["pidx"][q, :min(base_hits["count"][q], 128)],
                                base_hits["alpha"][q, :min(base_hits["count"][q], 128)]) if a > 0.01})
     assert len(contributing) > 10
-    picks = [(p, i) for p in rng.choice(contributing, size=min(12, len(contributing)), replace=False)
-             for i in rng.choice(59, size=5, replace=False)]
+    # 128 (particle, parameter) pairs per seed: 256 over both seeds
+    pairs = [(int(p), int(i)) for p in contributing for i in range(59)]
+    picks = [pairs[q] for q in rng.choice(len(pairs), size=min(128, len(pairs)), replace=False)]
     hstep = 1e-4
     checked = rejected = 0
     errs = []

@@ -159,3 +159,30 @@ def test_gradient_with_wide_kbuffer(ctx, mode):
     ctx._lib.gt_autotune_reset(ctx._h)
     assert info["used_mode"] == mode
     _check(got, _ref_grad(rec, 0.01, v.uniforms, w, h, g))
+
+
+def test_differentiable_config_subset(ctx):
+    """The differentiable configuration on a 2,048-Gaussian subset of its
+    200k scene (200x200 view of the same camera, k = 8): the full gradient
+    of the L2 loss against the perturbed-scene target, CUDA against the FP64
+    adjoint on the same entry lists."""
+    from gtrace import synth
+    from gtrace.uniforms import unpack_uniforms
+    raw, amin, v0 = synth.clusters_200k_config()
+    sub = {k: np.asarray(a)[:2048] for k, a in raw.items()}
+    rec = synth.pack(sub).gaussiansBuffer
+    tgt_rec = synth.pack(synth.perturb(sub, synth.SEED_BASE + 33)).gaussiansBuffer
+    w, h = 200, 200
+    v = synth.view(w, h, (0.0, 0.0, 12.0), k=8, alpha_min=amin)
+    s, t = Scene(ctx, rec, amin), Scene(ctx, tgt_rec, amin)
+    img = ctx.render(s, v.uniforms, w, h)
+    target = ctx.render(t, v.uniforms, w, h)
+    g = 2.0 * (img - target)
+    g[..., 3] = 0.0
+    got, info = ctx.backward(s, v.uniforms, w, h, g.astype(np.float32))
+    _, hits = oracle.Scene(rec, amin, "f32").render(v.uniforms, w, h, max_entries=256)
+    ref = oracle.backward_lists(oracle.Scene(rec, amin, "f64"), v.uniforms, w, h, hits,
+                                g.reshape(-1, 4).astype(np.float64),
+                                alpha_min=unpack_uniforms(v.uniforms)["alpha_min"])
+    _check(got, ref)
+    assert np.abs(got).sum() > 0

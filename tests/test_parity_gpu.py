@@ -274,3 +274,55 @@ def test_clustering_with_coincident_particles(ctx, n):
     img = ctx.render(s, v.uniforms, w, h)
     ref, _ = oracle.Scene(rec, 0.01, "f32").render(v.uniforms, w, h)
     np.testing.assert_array_equal(img.reshape(-1, 4), ref)
+
+
+def test_clusters_1m_stratified_subset(ctx):
+    """1M clustered Gaussians at 1920x1080, k = 16: every 8th pixel in x and y
+    (32,400 rays) bit-exact against the oracle's float build, hit sequences
+    of every 64th of those equal, and the subset's RMSE against the FP64
+    render below 1e-4."""
+    pg, amin, v = synth.clusters_1m_config()
+    w, h = v.width, v.height
+    g = Scene(ctx, pg.gaussiansBuffer, amin)
+    img = ctx.render(g, v.uniforms, w, h).reshape(-1, 4)
+    ys, xs = np.meshgrid(np.arange(0, h, 8), np.arange(0, w, 8), indexing="ij")
+    pix = (ys * w + xs).ravel().astype(np.uint32)
+    o = oracle.Scene(pg.gaussiansBuffer, amin, "f32")
+    ref, _ = o.render(v.uniforms, w, h, pixels=pix)
+    np.testing.assert_array_equal(img[pix].view(np.uint32), ref.view(np.uint32))
+    sub = pix[::64]
+    got = ctx.render_hits(g, v.uniforms, w, h, sub, max_entries=512)
+    _, ref_h = o.render(v.uniforms, w, h, pixels=sub, max_entries=512)
+    _assert_hits_equal(got, ref_h, 512)
+    del o
+    r64, _ = oracle.Scene(pg.gaussiansBuffer, amin, "f64").render(v.uniforms, w, h, pixels=pix)
+    rmse = float(np.sqrt(np.mean((img[pix, :3] - r64[:, :3]) ** 2)))
+    assert rmse < 1e-4, rmse
+
+
+def test_batched_config_shape(ctx):
+    """The batched configuration's structure at 2% of its Gaussian counts:
+    8 scenes, 64 views of uneven sizes, per-scene alpha_min; one batched
+    launch equals the 64 single renders bit for bit."""
+    scenes_raw, views = synth.batched_scenes_config(scale=0.02)
+    scenes = [Scene(ctx, synth.pack(r).gaussiansBuffer, a) for r, a in scenes_raw]
+    items = [(scenes[s], synth.view(w, h, pos, k=16, alpha_min=scenes_raw[s][1]).uniforms, w, h)
+             for s, w, h, pos in views]
+    outs, st = ctx.render_batch(items)
+    assert st["rays"] == sum(w * h for _, w, h, _ in views)
+    for (sc, u, w, h), out in zip(items, outs):
+        np.testing.assert_array_equal(out, ctx.render(sc, u, w, h))
+
+
+@pytest.mark.parametrize("n_pix", [1, 7, 507])
+def test_render_hits_any_pixel_count(ctx, n_pix):
+    """Pixel lists of any length (the per-pixel output parts of the call's
+    device buffer each start on their own aligned boundary)."""
+    pg = small_scene(n=2048, seed=12)
+    g, o = _both(ctx, pg.gaussiansBuffer, 0.01)
+    w, h = 40, 30
+    v = view(w, h, k=5)
+    pix = np.random.default_rng(n_pix).integers(0, w * h, size=n_pix).astype(np.uint32)
+    got = ctx.render_hits(g, v.uniforms, w, h, pix, max_entries=33)
+    _, ref = o.render(v.uniforms, w, h, pixels=pix, max_entries=33)
+    _assert_hits_equal(got, ref, 33)

@@ -416,16 +416,22 @@ extern "C" gt_status gt_render_hits(gt_context* ctx, const gt_scene* scene, cons
     return fail(ctx, GT_ERR_INVALID_ARG, "NULL output buffer");
   API_CUDA(ctx, cudaSetDevice(ctx->device));
   size_t me = std::max<uint32_t>(max_entries, 1);
-  size_t bytes = (size_t)n_pix * (4 + me * 12 + 4 + 4 + 16);
+  // one allocation cut into parts that each start on a 256-byte boundary
+  // (the float4 part needs 16; n_pix is arbitrary)
+  auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t o_rgba = 0, o_pix = up(o_rgba + (size_t)n_pix * 16), o_pidx = up(o_pix + (size_t)n_pix * 4);
+  const size_t o_t = up(o_pidx + (size_t)n_pix * me * 4), o_alpha = up(o_t + (size_t)n_pix * me * 4);
+  const size_t o_count = up(o_alpha + (size_t)n_pix * me * 4), o_rounds = up(o_count + (size_t)n_pix * 4);
+  const size_t bytes = o_rounds + (size_t)n_pix * 4;
   uint8_t* buf = nullptr;
   API_CUDA(ctx, cudaMalloc(&buf, bytes));
-  uint32_t* d_pix = reinterpret_cast<uint32_t*>(buf);
-  float4* d_rgba = reinterpret_cast<float4*>(buf + (size_t)n_pix * 4);
-  uint32_t* d_pidx = reinterpret_cast<uint32_t*>(buf + (size_t)n_pix * 20);
-  float* d_t = reinterpret_cast<float*>(buf + (size_t)n_pix * (20 + 4 * me));
-  float* d_alpha = reinterpret_cast<float*>(buf + (size_t)n_pix * (20 + 8 * me));
-  uint32_t* d_count = reinterpret_cast<uint32_t*>(buf + (size_t)n_pix * (20 + 12 * me));
-  uint32_t* d_rounds = reinterpret_cast<uint32_t*>(buf + (size_t)n_pix * (24 + 12 * me));
+  float4* d_rgba = reinterpret_cast<float4*>(buf + o_rgba);
+  uint32_t* d_pix = reinterpret_cast<uint32_t*>(buf + o_pix);
+  uint32_t* d_pidx = reinterpret_cast<uint32_t*>(buf + o_pidx);
+  float* d_t = reinterpret_cast<float*>(buf + o_t);
+  float* d_alpha = reinterpret_cast<float*>(buf + o_alpha);
+  uint32_t* d_count = reinterpret_cast<uint32_t*>(buf + o_count);
+  uint32_t* d_rounds = reinterpret_cast<uint32_t*>(buf + o_rounds);
   ViewDev v = make_view(scene, *u, w, h, nullptr, 0);
   gt_status rc = ensure_views(ctx, 1);
   if (rc != GT_OK) {

@@ -618,12 +618,14 @@ gt_status backward_impl(gt_context* ctx, const BwdView* views, uint32_t count, c
 }
 
 gt_status check_bwd_view(gt_context* ctx, const gt_scene* s, const gt_uniforms* u, uint32_t w, uint32_t h,
-                         const float* dL) {
+                         const float* dL, uint32_t flags) {
   if (!s || s->ctx != ctx) return api_fail(ctx, GT_ERR_INVALID_ARG, "scene is NULL or from another context");
   gt_status st = api_check_uniforms(ctx, u);
   if (st != GT_OK) return st;
   if (u->debug_mode != 0) return api_fail(ctx, GT_ERR_INVALID_ARG, "backward needs debug_mode 0");
   if (!dL) return api_fail(ctx, GT_ERR_INVALID_ARG, "dL_drgba is NULL");
+  if ((flags & GT_FLAG_INPUT_DEVICE) && ((uintptr_t)dL % 16) != 0)  // read as float4
+    return api_fail(ctx, GT_ERR_INVALID_ARG, "device dL_drgba must be 16-byte aligned");
   if (w == 0 || h == 0 || (uint64_t)w * h > (1ull << 31)) return api_fail(ctx, GT_ERR_INVALID_ARG, "bad image size");
   return GT_OK;
 }
@@ -634,7 +636,7 @@ extern "C" gt_status gt_backward(gt_context* ctx, const gt_scene* scene, const g
                                  const float* dL_drgba, float* dL_dparams, uint32_t flags, gt_bwd_opts* opts,
                                  gt_render_stats* stats) {
   if (!ctx) return api_fail(nullptr, GT_ERR_INVALID_ARG, "context is NULL");
-  gt_status st = check_bwd_view(ctx, scene, u, w, h, dL_drgba);
+  gt_status st = check_bwd_view(ctx, scene, u, w, h, dL_drgba, flags);
   if (st != GT_OK) return st;
   if (!dL_dparams && scene->n > 0) return api_fail(ctx, GT_ERR_INVALID_ARG, "dL_dparams is NULL");
   if (flags & GT_FLAG_ASYNC) return api_fail(ctx, GT_ERR_INVALID_ARG, "gt_backward is synchronous");
@@ -651,7 +653,8 @@ extern "C" gt_status gt_backward_batch(gt_context* ctx, const gt_batch_item* ite
   if (flags & GT_FLAG_ASYNC) return api_fail(ctx, GT_ERR_INVALID_ARG, "gt_backward_batch is synchronous");
   std::vector<BwdView> v(count);
   for (uint32_t i = 0; i < count; ++i) {
-    gt_status st = check_bwd_view(ctx, items[i].scene, &items[i].u, items[i].w, items[i].h, items[i].dL_drgba);
+    gt_status st =
+        check_bwd_view(ctx, items[i].scene, &items[i].u, items[i].w, items[i].h, items[i].dL_drgba, flags);
     if (st != GT_OK) return st;
     uint32_t s = 0;
     while (s < n_scenes && scenes[s] != items[i].scene) ++s;
