@@ -63,6 +63,13 @@ enum {
 #define GT_FLAG_FAST_BUILD     0x20u /* scene: Morton-prefix (LBVH) hierarchy instead
                                         of surface-area clustering: builds faster,
                                         traces slower (scenes rebuilt every step) */
+#define GT_FLAG_ANTIALIAS      0x40u /* render: progressive anti-aliasing, the
+                                        reference's `antialiasing` path
+                                        (src/GS_shader.ts:54,281-308, a constant
+                                        false there): one jittered sample per pixel,
+                                        seeded by (pixel, u.accumulated_frames) and
+                                        blended into the previous contents of
+                                        out_rgba (replaced when frames == 0) */
 
 /* -------------------------------------------------------- opaque handles */
 typedef struct gt_context gt_context;
@@ -162,6 +169,46 @@ gt_status gt_scene_create(gt_context* ctx, const void* packed, uint64_t n,
 gt_status gt_scene_destroy(gt_scene* scene);
 gt_status gt_scene_get_info(const gt_scene* scene, gt_scene_info* info);
 
+/* ========================================================= PLY ingest
+ * Native replacement of PackedGaussians (src/GS_ply.ts:39-253): the 3DGS
+ * PLY header is decoded on the host with the reference loader's rules
+ * (decodeHeader :58-111, readRawVertex :113-132: 50-byte header chunks,
+ * "element vertex" count, "property <type> <name>" in JavaScript object-key
+ * order, float and uchar properties read, others skipped), and the vertex
+ * rows are activated (:225-235: scale = exp, quaternion / its norm,
+ * opacity = sigmoid, in double) and packed into the 320-byte std430 records
+ * (:199-207; 64 + 16 (deg+1)^2 bytes for lower SH degrees) on the GPU.
+ * The header must be ASCII.  A missing float/uchar property, an SH degree
+ * outside 0..3 or a body shorter than the header says is GT_ERR_INVALID_ARG
+ * (the reference packs NaN or throws a RangeError there).  The PLY buffer is
+ * always a host buffer. */
+typedef struct gt_ply_info {
+  uint64_t n_vertices;    /* "element vertex" count                              */
+  uint64_t data_offset;   /* byte offset of the vertex data (one past end_header) */
+  uint32_t sh_degree;     /* 0..3, from the number of f_rest_* properties         */
+  uint32_t record_stride; /* bytes per packed record: 64 + 16 (sh_degree+1)^2     */
+  uint32_t row_bytes;     /* bytes per vertex row as the reference reads it       */
+  uint32_t n_properties;  /* distinct property names in the header                */
+  float ingest_ms;        /* device time of upload + activation/packing           */
+  uint32_t _pad;
+} gt_ply_info;
+
+/* Decodes the header only (host, no device work).  Errors are reported by
+ * gt_last_error(NULL, ...). */
+gt_status gt_ply_parse_header(const void* ply, uint64_t len, gt_ply_info* info);
+/* Writes PackedGaussians.gaussiansBuffer: n_vertices * record_stride bytes
+ * into out_packed (host, or device with GT_FLAG_OUTPUT_DEVICE, 16-byte
+ * aligned); out_bytes is its capacity. */
+gt_status gt_ply_pack(gt_context* ctx, const void* ply, uint64_t len, void* out_packed,
+                      uint64_t out_bytes, uint32_t flags, gt_ply_info* info);
+/* loadGaussianSplatting + PackedGaussians + gaussianSceneToBvh in one call:
+ * the packed records never leave the device.  flags: GT_FLAG_FAST_BUILD. */
+gt_status gt_scene_create_from_ply(gt_context* ctx, const void* ply, uint64_t len, double alpha_min,
+                                   uint32_t flags, gt_scene** out, gt_ply_info* info);
+/* The same from a file path (read with stdio). */
+gt_status gt_scene_create_from_ply_file(gt_context* ctx, const char* path, double alpha_min,
+                                        uint32_t flags, gt_scene** out, gt_ply_info* info);
+
 /* ============================================================= render */
 
 /* Renders one view.  Replaces traceRays (webrtx/src/pass_encoder.ts:35-65),
@@ -172,7 +219,9 @@ gt_status gt_scene_get_info(const gt_scene* scene, gt_scene_info* info);
  *   w, h       image size; any value >= 1 (the reference needs multiples of 8)
  *   out_rgba   w*h*4 floats, pixel (x, y) at index 4*(w*y + x); RGB = radiance,
  *              A = 1 (src/GS_shader.ts:300-301)
- *   flags      GT_FLAG_OUTPUT_DEVICE, GT_FLAG_ASYNC
+ *   flags      GT_FLAG_OUTPUT_DEVICE, GT_FLAG_ASYNC, GT_FLAG_ANTIALIAS (out_rgba
+ *              then also holds the running average of the earlier frames),
+ *              GT_FLAG_CHECKPOINT (not with GT_FLAG_ANTIALIAS)
  *   stats      optional (NULL allowed); not filled for asynchronous calls */
 gt_status gt_render(gt_context* ctx, const gt_scene* scene, const gt_uniforms* u,
                     uint32_t w, uint32_t h, float* out_rgba, uint32_t flags,
@@ -191,6 +240,24 @@ gt_status gt_render_hits(gt_context* ctx, const gt_scene* scene, const gt_unifor
                          uint32_t max_entries, uint32_t* out_pidx, float* out_t,
                          float* out_alpha, uint32_t* out_count, uint32_t* out_rounds,
                          float* out_rgba);
+
+/* ============================================================ display
+ * The reference's tone-map render pass (src/toneMapper.ts:15-24, a full-screen
+ * fragment shader into an 8-bit swap-chain texture) as a headless RGBA8
+ * buffer: byte 4i..4i+3 = R, G, B, 255 of pixel i, each channel clamped to
+ * [0, 1] and rounded from c * 255 (unorm8).  exposure is 1.66 in the
+ * reference.  exp and the 1/2.2 power use this library's deterministic
+ * routines, so the bytes are reproducible. */
+#define GT_TONEMAP_HDR            0u /* the shader's active line: vec4(hdr, 1)          */
+#define GT_TONEMAP_EXPOSURE       1u /* 1 - exp(-exposure hdr)                          */
+#define GT_TONEMAP_EXPOSURE_GAMMA 2u /* (1 - exp(-exposure hdr))^(1/2.2), the commented  */
+                                     /* gamma line                                       */
+/* rgba: n_pixels * 4 floats (host, or device with GT_FLAG_INPUT_DEVICE,
+ * 16-byte aligned); out_rgba8: n_pixels * 4 bytes (host, or device with
+ * GT_FLAG_OUTPUT_DEVICE, 4-byte aligned).  GT_FLAG_ASYNC needs both on the
+ * device. */
+gt_status gt_tonemap(gt_context* ctx, const float* rgba, uint64_t n_pixels, uint32_t mode, float exposure,
+                     uint8_t* out_rgba8, uint32_t flags);
 
 /* ============================================================ backward
  * No counterpart in the reference (it has no training path, README.md:69). */
@@ -250,7 +317,7 @@ gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items, uint32_t 
  *   - at most 256 views per call; larger counts are rejected with
  *     GT_ERR_INVALID_ARG;
  *   - the launch's scratch (tile counter, statistics, device view table,
- *     about 56 KB) lives in one fixed array in the library's device image;
+ *     about 60 KB) lives in one fixed array in the library's device image;
  *     every GPU that loads the library holds a copy until the process exits;
  *   - the first call on a device looks up that array's address (do it before
  *     any stream capture);

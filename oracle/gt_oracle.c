@@ -78,104 +78,216 @@ double or_log(double x) {
 
 /* ------------------------------------------------------------------------
  * PLY ingest: restatement of PackedGaussians (src/GS_ply.ts:58-253).
- *   header: "element vertex N", "property <type> <name>" (float | uchar),
- *           data starts one byte after "end_header" (:103)
- *   per vertex, in header order: float -> f32 LE, uchar -> byte/255 (:120-128)
+ *   header (decodeHeader, :58-111): 50-byte chunks are read until the text
+ *           holds "end_header" (a file ending inside that chunk throws); the
+ *           '\n'-split, trimmed lines of those chunks are scanned up to a line
+ *           equal to "end_header": "element vertex" -> count (first digit
+ *           run, last line wins), "property" -> (type, name) = groups 2, 3 of
+ *           the first match of (\w+)\s+(\w+)\s+(\w+); names in JS object-key
+ *           order (array-index names ascending first, then insertion order; a
+ *           repeated name keeps its place, takes the later type;
+ *           "__proto__" adds nothing); data one byte after "end_header" (:103)
+ *   per vertex, in key order: float -> f32 LE, uchar -> byte/255, other
+ *           types not read and 0 bytes (:120-128)
  *   activation (in double, :225-235): scale = exp, quaternion / its norm,
  *           opacity = 1/(1+exp(-x))
  *   SH order (:188-196): sh[0] = f_dc_0..2; sh[i+1].rgb = f_rest_{rgb*n+i},
- *           n = #f_rest / 3
+ *           n = #f_rest / 3; degree 0..3 (:136-148)
  *   std430 packing (src/GS_packing.ts:146-174,233-245): position @0,
  *           scale @16, rotation @32, opacity @48, sh[j] @64+16j;
  *           record size rounded up to 16.
+ * Non-ASCII headers, missing float/uchar properties and short bodies are
+ * errors (the reference packs NaN or throws there).
  * ---------------------------------------------------------------------- */
-#define OR_MAX_PROPS 256
+#define OR_MAX_PROPS 1024
+#define OR_NAME 64
+typedef struct {
+  char name[OR_NAME];
+  int kind; /* 1 float, 0 uchar, -1 other */
+  int is_index;
+  unsigned long long index;
+  int order; /* insertion order */
+} or_prop;
+
+static int or_js_space(int c) { return c == ' ' || c == '\t' || c == '\n' || c == '\v' || c == '\f' || c == '\r'; }
+static int or_js_word(int c) {
+  return (c >= 'a' && c <= 'z') || (c >= 'A' && c <= 'Z') || (c >= '0' && c <= '9') || c == '_';
+}
+
+/* (\w+)\s+(\w+)\s+(\w+): leftmost match; returns 1 and the spans of groups 2, 3 */
+static int or_prop_match(const char* s, size_t L, size_t* t0, size_t* t1, size_t* n0, size_t* n1) {
+  for (size_t i = 0; i < L; ++i) {
+    if (!or_js_word((unsigned char)s[i])) continue;
+    size_t a = i;
+    while (a < L && or_js_word((unsigned char)s[a])) ++a;
+    size_t b = a;
+    while (b < L && or_js_space((unsigned char)s[b])) ++b;
+    if (b > a && b < L && or_js_word((unsigned char)s[b])) {
+      size_t c = b;
+      while (c < L && or_js_word((unsigned char)s[c])) ++c;
+      size_t d = c;
+      while (d < L && or_js_space((unsigned char)s[d])) ++d;
+      if (d > c && d < L && or_js_word((unsigned char)s[d])) {
+        size_t e = d;
+        while (e < L && or_js_word((unsigned char)s[e])) ++e;
+        *t0 = b;
+        *t1 = c;
+        *n0 = d;
+        *n1 = e;
+        return 1;
+      }
+    }
+    i = a; /* the loop's ++i moves past the non-word character at a */
+  }
+  return 0;
+}
+
+static int or_array_index(const char* nm, unsigned long long* v) {
+  size_t l = strlen(nm);
+  if (l == 0 || l > 10) return 0;
+  for (size_t i = 0; i < l; ++i)
+    if (nm[i] < '0' || nm[i] > '9') return 0;
+  if (nm[0] == '0' && l > 1) return 0;
+  unsigned long long x = strtoull(nm, NULL, 10);
+  if (x >= 4294967295ull) return 0;
+  *v = x;
+  return 1;
+}
+
+static int or_prop_cmp(const void* pa, const void* pb) {
+  const or_prop* a = (const or_prop*)pa;
+  const or_prop* b = (const or_prop*)pb;
+  if (a->is_index != b->is_index) return a->is_index ? -1 : 1;
+  if (a->is_index) return a->index < b->index ? -1 : (a->index > b->index ? 1 : 0);
+  return a->order - b->order;
+}
+
 int or_ply_to_aos(const uint8_t* bytes, size_t len, uint32_t* n_out, uint32_t* deg_out,
                   uint32_t* stride_out, float* aos) {
-  const char* end_tag = "end_header";
-  size_t hdr_end = 0;
-  for (size_t i = 0; i + 10 <= len; ++i) {
-    if (memcmp(bytes + i, end_tag, 10) == 0) {
-      hdr_end = i + 10 + 1;
+  size_t pos = (size_t)-1;
+  for (size_t i = 0; i + 10 <= len; ++i)
+    if (memcmp(bytes + i, "end_header", 10) == 0) {
+      pos = i;
       break;
     }
-  }
-  if (hdr_end == 0 || hdr_end > len) return 1;
-  char names[OR_MAX_PROPS][32];
-  int is_float[OR_MAX_PROPS];
-  int np = 0;
-  uint64_t nvert = 0;
-  size_t pos = 0;
-  while (pos < hdr_end) {
-    size_t e = pos;
-    while (e < hdr_end && bytes[e] != '\n') ++e;
-    char line[256];
-    size_t l = e - pos < 255 ? e - pos : 255;
-    memcpy(line, bytes + pos, l);
-    line[l] = 0;
-    /* trim */
-    char* p = line;
-    while (*p == ' ' || *p == '\t' || *p == '\r') ++p;
-    size_t pl = strlen(p);
-    while (pl && (p[pl - 1] == ' ' || p[pl - 1] == '\r' || p[pl - 1] == '\t')) p[--pl] = 0;
-    if (strncmp(p, "element vertex", 14) == 0) {
-      const char* q = p;
-      while (*q && (*q < '0' || *q > '9')) ++q;
-      nvert = strtoull(q, NULL, 10);
-    } else if (strncmp(p, "property", 8) == 0) {
-      char a[64], t[64], nm[64];
-      if (sscanf(p, "%63s %63s %63s", a, t, nm) == 3) {
+  if (pos == (size_t)-1) return 1;
+  const size_t chunk_end = (pos + 10 + 49) / 50 * 50;
+  if (chunk_end > len) return 1;
+  for (size_t i = 0; i < pos; ++i)
+    if (bytes[i] >= 0x80) return 1;
+  const size_t hdr_end = pos + 11;
+  or_prop* props = (or_prop*)calloc(OR_MAX_PROPS, sizeof(or_prop));
+  if (!props) return 7;
+  int np = 0, next_order = 0;
+  unsigned long long nvert = 0;
+  int nvert_ok = 1;
+  size_t ls = 0;
+  for (;;) {
+    size_t le = ls;
+    while (le < chunk_end && bytes[le] != '\n') ++le;
+    size_t a = ls, b = le;
+    while (a < b && or_js_space(bytes[a])) ++a;
+    while (b > a && or_js_space(bytes[b - 1])) --b;
+    const char* p = (const char*)bytes + a;
+    const size_t pl = b - a;
+    if (pl >= 14 && memcmp(p, "element vertex", 14) == 0) {
+      size_t d = 0;
+      while (d < pl && !(p[d] >= '0' && p[d] <= '9')) ++d;
+      if (d < pl) {
+        size_t e = d;
+        while (e < pl && p[e] >= '0' && p[e] <= '9') ++e;
+        while (d + 1 < e && p[d] == '0') ++d; /* leading zeros */
+        if (e - d > 12) {
+          nvert_ok = 0;
+        } else {
+          char num[16];
+          memcpy(num, p + d, e - d);
+          num[e - d] = 0;
+          nvert = strtoull(num, NULL, 10);
+          nvert_ok = 1;
+        }
+      }
+    } else if (pl >= 8 && memcmp(p, "property", 8) == 0) {
+      size_t t0 = 0, t1 = 0, n0 = 0, n1 = 0;
+      if (or_prop_match(p, pl, &t0, &t1, &n0, &n1) && n1 - n0 < OR_NAME && !(n1 - n0 == 9 && !memcmp(p + n0, "__proto__", 9))) {
+        char nm[OR_NAME];
+        memcpy(nm, p + n0, n1 - n0);
+        nm[n1 - n0] = 0;
+        int kind = (t1 - t0 == 5 && !memcmp(p + t0, "float", 5)) ? 1 : ((t1 - t0 == 5 && !memcmp(p + t0, "uchar", 5)) ? 0 : -1);
         int idx = -1;
         for (int i = 0; i < np; ++i)
-          if (strcmp(names[i], nm) == 0) idx = i;
+          if (strcmp(props[i].name, nm) == 0) idx = i;
         if (idx < 0) {
-          if (np >= OR_MAX_PROPS) return 2;
+          if (np >= OR_MAX_PROPS) {
+            free(props);
+            return 2;
+          }
           idx = np++;
-          snprintf(names[idx], sizeof names[idx], "%s", nm);
+          snprintf(props[idx].name, OR_NAME, "%s", nm);
+          props[idx].order = next_order++;
+          props[idx].is_index = or_array_index(nm, &props[idx].index);
         }
-        is_float[idx] = strcmp(t, "float") == 0 ? 1 : (strcmp(t, "uchar") == 0 ? 0 : -1);
+        props[idx].kind = kind;
+      } else if (n1 - n0 >= OR_NAME) {
+        free(props);
+        return 2;
       }
-    } else if (strcmp(p, "end_header") == 0) {
+    } else if (pl == 10 && memcmp(p, "end_header", 10) == 0) {
       break;
     }
-    pos = e + 1;
+    if (le >= chunk_end) break;
+    ls = le + 1;
   }
+  if (!nvert_ok || nvert >= (1ull << 31)) {
+    free(props);
+    return 2;
+  }
+  qsort(props, (size_t)np, sizeof(or_prop), or_prop_cmp);
+  char names[OR_MAX_PROPS][OR_NAME];
+  int is_float[OR_MAX_PROPS];
+  for (int i = 0; i < np; ++i) {
+    memcpy(names[i], props[i].name, OR_NAME);
+    is_float[i] = props[i].kind;
+  }
+  free(props);
   int n_rest = 0;
   for (int i = 0; i < np; ++i)
     if (strncmp(names[i], "f_rest_", 7) == 0) ++n_rest;
-  int per_color = n_rest / 3;
-  double degf = sqrt((double)per_color + 1.0) - 1.0;
+  double per_color_d = (double)n_rest / 3.0;
+  double degf = sqrt(per_color_d + 1.0) - 1.0;
+  if (!(degf == 0.0 || degf == 1.0 || degf == 2.0 || degf == 3.0)) return 3;
   int deg = (int)degf;
-  if ((double)deg != degf || deg < 0 || deg > 3) return 3;
+  int per_color = n_rest / 3;
   int n_sh = (deg + 1) * (deg + 1);
   /* struct: 64 bytes of header fields + n_sh vec3 at stride 16, size rounded to 16 */
   uint32_t stride = 64u + 16u * (uint32_t)n_sh;
-  *n_out = (uint32_t)nvert;
-  *deg_out = (uint32_t)deg;
-  *stride_out = stride;
-  if (!aos) return 0;
-  /* bytes per vertex */
-  size_t vbytes = 0;
-  for (int i = 0; i < np; ++i) vbytes += is_float[i] == 1 ? 4 : (is_float[i] == 0 ? 1 : 0);
-  if (hdr_end + vbytes * nvert > len) return 4;
+  /* every required property must be read (float or uchar) */
   int ix[14];
   const char* want[14] = {"x", "y", "z", "scale_0", "scale_1", "scale_2", "rot_0",
                           "rot_1", "rot_2", "rot_3", "opacity", "f_dc_0", "f_dc_1", "f_dc_2"};
   for (int w = 0; w < 14; ++w) {
     ix[w] = -1;
     for (int i = 0; i < np; ++i)
-      if (strcmp(names[i], want[w]) == 0) ix[w] = i;
+      if (strcmp(names[i], want[w]) == 0 && is_float[i] >= 0) ix[w] = i;
     if (ix[w] < 0) return 5;
   }
   int rest_ix[45];
-  for (int r = 0; r < n_rest && r < 45; ++r) {
+  for (int r = 0; r < 3 * per_color && r < 45; ++r) {
     char nm[32];
     snprintf(nm, sizeof nm, "f_rest_%d", r);
     rest_ix[r] = -1;
     for (int i = 0; i < np; ++i)
-      if (strcmp(names[i], nm) == 0) rest_ix[r] = i;
+      if (strcmp(names[i], nm) == 0 && is_float[i] >= 0) rest_ix[r] = i;
     if (rest_ix[r] < 0) return 6;
   }
+  /* bytes per vertex */
+  size_t vbytes = 0;
+  for (int i = 0; i < np; ++i) vbytes += is_float[i] == 1 ? 4 : (is_float[i] == 0 ? 1 : 0);
+  if (nvert > 0 && (len - hdr_end) / vbytes < nvert) return 4;
+  *n_out = (uint32_t)nvert;
+  *deg_out = (uint32_t)deg;
+  *stride_out = stride;
+  if (!aos) return 0;
   double* v = (double*)malloc(sizeof(double) * (size_t)np);
   if (!v) return 7;
   const uint8_t* data = bytes + hdr_end;
@@ -213,6 +325,57 @@ int or_ply_to_aos(const uint8_t* bytes, size_t len, uint32_t* n_out, uint32_t* d
       for (int c = 0; c < 3; ++c) rec[16 + 4 * (i + 1) + c] = (float)v[rest_ix[c * per_color + i]];
   }
   free(v);
+  return 0;
+}
+
+/* ------------------------------------------------------------------------
+ * Anti-aliasing jitter (src/GS_shader.ts:6-31): getNewSeed is numPermutation
+ * rounds of the TEA block cipher (Wheeler and Needham 1994) with the
+ * reference's constants; rng is an LCG step whose low 24 bits are scaled to
+ * [0, 1).
+ * ---------------------------------------------------------------------- */
+uint32_t or_new_seed(uint32_t p1, uint32_t p2, uint32_t rounds) {
+  uint32_t s0 = 0, v0 = p1, v1 = p2;
+  for (uint32_t r = 0; r < rounds; ++r) {
+    s0 += 0x9e3779b9u;
+    v0 += ((v1 << 4) + 0xa341316cu) ^ (v1 + s0) ^ ((v1 >> 5) + 0xc8013ea4u);
+    v1 += ((v0 << 4) + 0xad90777du) ^ (v0 + s0) ^ ((v0 >> 5) + 0x7e95761eu);
+  }
+  return v0;
+}
+
+float or_rng(uint32_t* seed) {
+  *seed = 1664525u * *seed + 1013904223u;
+  return (float)(*seed & 0x00FFFFFFu) / (float)0x01000000;
+}
+
+/* ------------------------------------------------------------------------
+ * Tone map (src/toneMapper.ts:15-24) into unorm8 RGBA: mode 0 shows hdr as
+ * the reference's fragment shader does, mode 1 applies 1 - exp(-exposure
+ * hdr), mode 2 also the 1/2.2 power (written as exp(log(x) / 2.2) with the
+ * deterministic routines above); unorm8 clamps to [0, 1] and rounds c * 255
+ * to nearest (ties to even); NaN gives 0.
+ * ---------------------------------------------------------------------- */
+static uint8_t or_unorm8(float c) {
+  if (!(c > 0.0f)) return 0;
+  if (c >= 1.0f) return 255;
+  return (uint8_t)nearbyintf(c * 255.0f);
+}
+
+static float or_tone(float hdr, uint32_t mode, float exposure) {
+  if (mode == 0) return hdr;
+  float ldr = 1.0f - or_expf(-(exposure * hdr));
+  if (mode == 1) return ldr;
+  if (!(ldr > 0.0f)) return ldr;
+  return or_expf((float)(or_log((double)ldr) / 2.2));
+}
+
+int or_tonemap(const float* rgba, uint64_t n, uint32_t mode, float exposure, uint8_t* out) {
+  if (mode > 2) return 1;
+  for (uint64_t i = 0; i < n; ++i) {
+    for (int c = 0; c < 3; ++c) out[4 * i + c] = or_unorm8(or_tone(rgba[4 * i + c], mode, exposure));
+    out[4 * i + 3] = 255;
+  }
   return 0;
 }
 

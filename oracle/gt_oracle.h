@@ -48,6 +48,17 @@ typedef struct or_hits {
 int or_ply_to_aos(const uint8_t* bytes, size_t len, uint32_t* n, uint32_t* sh_degree,
                   uint32_t* stride, float* aos);
 
+/* Progressive anti-aliasing restatement: renders the full image with the
+ * jittered samples of (pixel, uniforms.accumulatedFrames) and blends it into
+ * accum (w*h*4), src/GS_shader.ts:275-308 with antialiasing = true. */
+int or_render_accum_f32(const or_scene_f32* s, const void* uniforms, uint32_t w, uint32_t h,
+                        int threads, float* accum);
+/* getNewSeed and rng of src/GS_shader.ts:6-31. */
+uint32_t or_new_seed(uint32_t p1, uint32_t p2, uint32_t rounds);
+float or_rng(uint32_t* seed);
+/* Tone map of src/toneMapper.ts:15-24 into unorm8 RGBA (modes 0..2). */
+int or_tonemap(const float* rgba, uint64_t n, uint32_t mode, float exposure, uint8_t* out);
+
 /* Deterministic elementary functions shared by the float oracle and the CUDA
  * tracer's specification (exposed for their unit tests). */
 float or_expf(float x);

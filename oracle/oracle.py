@@ -56,6 +56,14 @@ def lib():
             r = getattr(L, f"or_render_{sfx}")
             r.restype = i32
             r.argtypes = [vp, vp, u32, u32, vp, u32, i32, i32, vp, C.POINTER(OrHits)]
+        L.or_render_accum_f32.restype = i32
+        L.or_render_accum_f32.argtypes = [vp, vp, u32, u32, i32, vp]
+        L.or_new_seed.restype = u32
+        L.or_new_seed.argtypes = [u32, u32, u32]
+        L.or_rng.restype = C.c_float
+        L.or_rng.argtypes = [C.POINTER(u32)]
+        L.or_tonemap.restype = i32
+        L.or_tonemap.argtypes = [vp, u64, u32, C.c_float, vp]
         L.or_backward_f64.restype = i32
         L.or_backward_f64.argtypes = [vp, vp, u32, u32, vp, u32, vp, i32, vp]
         L.or_backward_lists_f64.restype = i32
@@ -127,6 +135,18 @@ class Scene:
         rec["node_visits"] = int(hits.node_visits)
         return out, rec
 
+    def render_accum(self, uniforms, w: int, h: int, accum: np.ndarray, threads: int = 0) -> np.ndarray:
+        """Progressive anti-aliasing step: blends the jittered render of
+        frame ``accumulated_frames`` into ``accum`` (w*h x 4 float32, in place)."""
+        if self.precision != "f32":
+            raise ValueError("the anti-aliasing restatement is the float build")
+        u = np.frombuffer(bytes(uniforms), dtype=np.uint8).copy()
+        assert accum.dtype == np.float32 and accum.flags.c_contiguous and accum.size == w * h * 4
+        rc = lib().or_render_accum_f32(self._h, _ptr(u), w, h, threads, _ptr(accum))
+        if rc != 0:
+            raise RuntimeError(f"oracle accumulate failed ({rc})")
+        return accum
+
     def backward(self, uniforms, w: int, h: int, dL_drgba: np.ndarray, pixels=None, threads: int = 0):
         if self.precision != "f64":
             raise ValueError("the oracle adjoint is FP64")
@@ -180,6 +200,26 @@ def ply_to_aos(data: bytes) -> np.ndarray:
     if rc != 0:
         raise ValueError(f"oracle PLY parse failed ({rc})")
     return out
+
+
+def tonemap(rgba: np.ndarray, mode: int, exposure: float = 1.66) -> np.ndarray:
+    """unorm8 RGBA of an RGBA-f32 image (src/toneMapper.ts:15-24), shape (n, 4)."""
+    a = np.ascontiguousarray(rgba, dtype=np.float32).reshape(-1, 4)
+    out = np.zeros((a.shape[0], 4), dtype=np.uint8)
+    rc = lib().or_tonemap(_ptr(a), a.shape[0], mode, exposure, _ptr(out))
+    if rc != 0:
+        raise ValueError(f"oracle tone map failed ({rc})")
+    return out
+
+
+def new_seed(p1: int, p2: int, rounds: int = 8) -> int:
+    return int(lib().or_new_seed(p1, p2, rounds))
+
+
+def rng(seed: int):
+    s = C.c_uint32(seed)
+    v = float(lib().or_rng(C.byref(s)))
+    return v, int(s.value)
 
 
 def expf(x: float) -> float:

@@ -100,7 +100,6 @@ static gt_status ensure_staging(gt_context* ctx, size_t bytes) {
 
 static SceneDev scene_dev(const gt_scene* s) {
   SceneDev d;
-  d.nodes = s->b.nodes;
   d.nodes8 = s->b.nodes8;
   d.w2o = s->b.w2o;
   d.leaf_pidx = s->b.leaf_pidx;
@@ -363,6 +362,9 @@ extern "C" gt_status gt_render(gt_context* ctx, const gt_scene* scene, const gt_
     return fail(ctx, GT_ERR_INVALID_ARG, "GT_FLAG_ASYNC needs a device output buffer");
   if ((flags & GT_FLAG_OUTPUT_DEVICE) && ((uintptr_t)out_rgba % 16) != 0)
     return fail(ctx, GT_ERR_INVALID_ARG, "device out_rgba must be 16-byte aligned");
+  const bool aa = (flags & GT_FLAG_ANTIALIAS) != 0;
+  if (aa && (flags & GT_FLAG_CHECKPOINT))
+    return fail(ctx, GT_ERR_INVALID_ARG, "GT_FLAG_ANTIALIAS renders are not checkpointed");
   API_CUDA(ctx, cudaSetDevice(ctx->device));
   size_t bytes = (size_t)w * h * sizeof(float4);
   float4* out = reinterpret_cast<float4*>(out_rgba);
@@ -370,6 +372,9 @@ extern "C" gt_status gt_render(gt_context* ctx, const gt_scene* scene, const gt_
     st = ensure_staging(ctx, bytes);
     if (st != GT_OK) return st;
     out = ctx->staging;
+    // the running average of the earlier frames is blended on the device
+    if (aa && u->accumulated_frames != 0)
+      API_CUDA(ctx, cudaMemcpyAsync(out, out_rgba, bytes, cudaMemcpyHostToDevice, ctx->stream));
   }
   if (flags & GT_FLAG_CHECKPOINT) {
     if (flags & GT_FLAG_ASYNC) return fail(ctx, GT_ERR_INVALID_ARG, "a checkpointing render is synchronous");
@@ -387,6 +392,7 @@ extern "C" gt_status gt_render(gt_context* ctx, const gt_scene* scene, const gt_
   st = ensure_views(ctx, 1);
   if (st != GT_OK) return st;
   ViewDev v = make_view(scene, *u, w, h, out, 0);
+  v.u.aa = aa ? 1u : 0u;
   API_CUDA(ctx, cudaEventRecord(ctx->call0, ctx->stream));
   API_CUDA(ctx, cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), ctx->stream));
   uint64_t slot = ring_slot(ctx);
@@ -482,6 +488,9 @@ extern "C" gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items
   if (!items) return fail(ctx, GT_ERR_INVALID_ARG, "items is NULL");
   if ((flags & GT_FLAG_ASYNC) && !(flags & GT_FLAG_OUTPUT_DEVICE))
     return fail(ctx, GT_ERR_INVALID_ARG, "GT_FLAG_ASYNC needs device output buffers");
+  const bool aa = (flags & GT_FLAG_ANTIALIAS) != 0;
+  if (aa && (flags & GT_FLAG_CHECKPOINT))
+    return fail(ctx, GT_ERR_INVALID_ARG, "GT_FLAG_ANTIALIAS renders are not checkpointed");
   API_CUDA(ctx, cudaSetDevice(ctx->device));
   size_t staging = 0;
   uint32_t kmax = 8, total_tiles = 0;
@@ -548,7 +557,11 @@ extern "C" gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items
     const gt_batch_item& it = items[i];
     float4* out = (flags & GT_FLAG_OUTPUT_DEVICE) ? reinterpret_cast<float4*>(it.out_rgba) : ctx->staging + offs[i];
     ctx->h_views[q] = make_view(it.scene, it.u, it.w, it.h, out, total_tiles);
+    ctx->h_views[q].u.aa = aa ? 1u : 0u;
     total_tiles += ctx->h_views[q].n_tiles;
+    if (aa && it.u.accumulated_frames != 0 && !(flags & GT_FLAG_OUTPUT_DEVICE))
+      API_CUDA(ctx, cudaMemcpyAsync(out, it.out_rgba, (size_t)it.w * it.h * sizeof(float4), cudaMemcpyHostToDevice,
+                                    ctx->stream));
   }
   API_CUDA(ctx, cudaEventRecord(ctx->call0, ctx->stream));
   uint64_t slot = ring_slot(ctx);

@@ -861,6 +861,11 @@ Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride, double alph
     Err ce = collapse_bvh8(b.nodes, leaf_box, m, st, &b.nodes8, &b.n_nodes8, launches);
     if (ce.code != GT_OK) return ce;
     b.bytes += (uint64_t)b.n_nodes8 * 16 * sizeof(float4);
+    // traversal reads only the 8-wide nodes: the binary hierarchy goes
+    GT_CUDA_TRY(cudaStreamSynchronize(st));
+    cudaFree(b.nodes);
+    b.nodes = nullptr;
+    b.bytes -= (uint64_t)std::max<uint32_t>(n_int, 1) * 4 * sizeof(float4);
   }
   float rb[6];
   uint32_t bo[8];

@@ -99,17 +99,55 @@ __device__ __forceinline__ double det_log(double x) {
 }
 
 // Ray generation (src/GS_shader.ts:275-285).
+// Per-pixel seed of the reference's progressive anti-aliasing
+// (getNewSeed, src/GS_shader.ts:9-23): 8 rounds of the TEA block cipher
+// (Wheeler and Needham 1994) keyed by the reference's four constants.
+__device__ __forceinline__ uint32_t aa_seed(uint32_t p1, uint32_t p2) {
+  uint32_t s0 = 0, v0 = p1, v1 = p2;
+#pragma unroll
+  for (int r = 0; r < 8; ++r) {
+    s0 += 0x9e3779b9u;
+    v0 += ((v1 << 4) + 0xa341316cu) ^ (v1 + s0) ^ ((v1 >> 5) + 0xc8013ea4u);
+    v1 += ((v0 << 4) + 0xad90777du) ^ (v0 + s0) ^ ((v0 >> 5) + 0x7e95761eu);
+  }
+  return v0;
+}
+
+// rng (src/GS_shader.ts:25-29): LCG step, low 24 bits scaled to [0, 1).
+__device__ __forceinline__ float aa_rng(uint32_t& seed) {
+  seed = 1664525u * seed + 1013904223u;
+  return (float)(seed & 0x00FFFFFFu) * (1.0f / 16777216.0f);
+}
+
+// Ray generation (src/GS_shader.ts:275-285): camera basis from the columns
+// of toWorld; the pixel sample is the centre, or with anti-aliasing the
+// jitter (rng(seed), rng(seed)) of seed = getNewSeed(W*y + x, frames, 8).
 __device__ __forceinline__ void ray_gen(const RayUniforms& u, uint32_t w, uint32_t h, uint32_t px, uint32_t py,
                                         V3& o, V3& d) {
   V3 cx = mk(-u.tw[0], -u.tw[1], -u.tw[2]);
   V3 cy = mk(u.tw[4], u.tw[5], u.tw[6]);
   V3 cz = mk(-u.tw[8], -u.tw[9], -u.tw[10]);
   o = mk(u.tw[12], u.tw[13], u.tw[14]);
-  float nx = __fdiv_rn((float)px + 0.5f, (float)w) * 2.0f - 1.0f;
-  float ny = __fdiv_rn((float)py + 0.5f, (float)h) * 2.0f - 1.0f;
+  float jx = 0.5f, jy = 0.5f;
+  if (u.aa) {
+    uint32_t seed = aa_seed(w * py + px, u.frames);
+    jx = aa_rng(seed);
+    jy = aa_rng(seed);
+  }
+  float nx = __fdiv_rn((float)px + jx, (float)w) * 2.0f - 1.0f;
+  float ny = __fdiv_rn((float)py + jy, (float)h) * 2.0f - 1.0f;
   float ax = nx * u.asp[0], ay = ny * u.asp[1];
   V3 v = mk((ax * cx.x + ay * cy.x) + cz.x, (ax * cx.y + ay * cy.y) + cz.y, (ax * cx.z + ay * cy.z) + cz.z);
   d = vnorm(v);
+}
+
+// Progressive average (src/GS_shader.ts:302-308): frame 0 replaces the
+// pixel, frame f > 0 blends mix(old, new, 1 / (f + 1)) = old (1 - a) + new a.
+__device__ __forceinline__ float4 aa_blend(float4 old, float4 nw, uint32_t frames) {
+  if (frames == 0) return make_float4(nw.x, nw.y, nw.z, 1.0f);
+  const float a = __fdiv_rn(1.0f, __uint2float_rn(frames) + 1.0f);
+  const float b = 1.0f - a;
+  return make_float4(old.x * b + nw.x * a, old.y * b + nw.y * a, old.z * b + nw.z * a, 1.0f);
 }
 
 // intersect_triangle_branchless0 (webrtx/src/glsl/intersect.glsl:73-92):

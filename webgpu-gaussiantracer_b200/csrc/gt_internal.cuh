@@ -62,7 +62,6 @@ struct DevCounters {
 // Scene as the kernels see it.  Records of kept proxies are in BVH leaf
 // order j; shading records are indexed by particle index p.
 struct SceneDev {
-  const float4* nodes;      // 4 float4 per internal node (see gt_build.cu)
   const float4* nodes8;     // 16 float4 per 8-wide node (see gt_build.cu)
   const float4* w2o;        // 3 float4 per leaf: world-to-object 4x3 column-major
   const uint32_t* leaf_pidx;// particle index of leaf j
@@ -81,6 +80,8 @@ struct RayUniforms {
   float asp[2];
   float t_min, t_max, T_min, alpha_min;
   uint32_t k, deg, early_stop, debug;
+  uint32_t frames;  // accumulated_frames
+  uint32_t aa;      // 1: jittered pixel sample, blended into the previous image
 };
 
 inline RayUniforms to_ray_uniforms(const gt_uniforms& u) {
@@ -96,6 +97,8 @@ inline RayUniforms to_ray_uniforms(const gt_uniforms& u) {
   r.deg = u.sh_degree_max;
   r.early_stop = u.early_stop;
   r.debug = u.debug_mode;
+  r.frames = u.accumulated_frames;
+  r.aa = 0;
   return r;
 }
 
@@ -143,7 +146,7 @@ struct Err {
 
 // Scene build (gt_build.cu).
 struct SceneBuffers {
-  float4* nodes = nullptr;
+  float4* nodes = nullptr;   // binary hierarchy: only during the build
   float4* nodes8 = nullptr;  // 8-wide nodes: 8 child records of 2 float4
   uint32_t n_nodes8 = 0;
   float4* w2o = nullptr;

@@ -263,7 +263,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) k_trace8(const ViewDev
       if (RECORD) {
         if (ho.rgba) ho.rgba[item] = r;
       } else {
-        V.out[(size_t)py * V.w + px] = r;
+        float4* dst = V.out + (size_t)py * V.w + px;
+        *dst = V.u.aa ? aa_blend(*dst, r, V.u.frames) : r;
       }
       ++rays;
     }

@@ -27,6 +27,11 @@ GT_FLAG_ASYNC = 0x4
 GT_FLAG_ACCUMULATE = 0x8
 GT_FLAG_CHECKPOINT = 0x10
 GT_FLAG_FAST_BUILD = 0x20
+GT_FLAG_ANTIALIAS = 0x40
+
+GT_TONEMAP_HDR = 0
+GT_TONEMAP_EXPOSURE = 1
+GT_TONEMAP_EXPOSURE_GAMMA = 2
 
 STATUS_NAMES = {GT_OK: "GT_OK", GT_ERR_INVALID_ARG: "GT_ERR_INVALID_ARG", GT_ERR_OOM: "GT_ERR_OOM",
                 GT_ERR_CUDA: "GT_ERR_CUDA", GT_ERR_DEVICE_TIMEOUT: "GT_ERR_DEVICE_TIMEOUT",
@@ -73,6 +78,15 @@ class TuneResult(C.Structure):
                 ("kbuf", C.c_uint32), ("leaf_batch", C.c_uint32)]
 
 
+class PlyInfo(C.Structure):
+    _fields_ = [("n_vertices", C.c_uint64), ("data_offset", C.c_uint64), ("sh_degree", C.c_uint32),
+                ("record_stride", C.c_uint32), ("row_bytes", C.c_uint32), ("n_properties", C.c_uint32),
+                ("ingest_ms", C.c_float), ("_pad", C.c_uint32)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_ if not name.startswith("_")}
+
+
 assert C.sizeof(Uniforms) == 112
 
 # (name, restype, argtypes) of every symbol include/gtrace.h declares
@@ -85,6 +99,11 @@ SIGNATURES = [
     ("gt_scene_create", _i32, [_vp, _vp, _u64, _u32, C.c_double, _u32, C.POINTER(_vp)]),
     ("gt_scene_destroy", _i32, [_vp]),
     ("gt_scene_get_info", _i32, [_vp, C.POINTER(SceneInfo)]),
+    ("gt_ply_parse_header", _i32, [_vp, _u64, C.POINTER(PlyInfo)]),
+    ("gt_ply_pack", _i32, [_vp, _vp, _u64, _vp, _u64, _u32, C.POINTER(PlyInfo)]),
+    ("gt_scene_create_from_ply", _i32, [_vp, _vp, _u64, C.c_double, _u32, C.POINTER(_vp), C.POINTER(PlyInfo)]),
+    ("gt_scene_create_from_ply_file", _i32, [_vp, C.c_char_p, C.c_double, _u32, C.POINTER(_vp),
+                                             C.POINTER(PlyInfo)]),
     ("gt_render", _i32, [_vp, _vp, C.POINTER(Uniforms), _u32, _u32, _vp, _u32, C.POINTER(RenderStats)]),
     ("gt_render_hits", _i32, [_vp, _vp, C.POINTER(Uniforms), _u32, _u32, _vp, _u32, _u32, _vp, _vp, _vp, _vp, _vp,
                               _vp]),
@@ -94,6 +113,7 @@ SIGNATURES = [
     ("gt_render_batch_noalloc", _i32, [_vp, C.POINTER(BatchItem), _u32, _u32, C.POINTER(RenderStats)]),
     ("gt_backward_batch", _i32, [_vp, C.POINTER(BatchItem), _u32, C.POINTER(_vp), C.POINTER(_vp), _u32, _u32,
                                  C.POINTER(BwdOpts), C.POINTER(RenderStats)]),
+    ("gt_tonemap", _i32, [_vp, _vp, _u64, _u32, C.c_float, _vp, _u32]),
     ("gt_l2_loss", _i32, [_vp, _vp, _vp, _u64, _vp, C.POINTER(C.c_double)]),
     ("gt_autotune", _i32, [_vp, _vp, C.POINTER(Uniforms), _u32, _u32, C.POINTER(TuneResult)]),
     ("gt_set_tune", _i32, [_vp, _vp, C.POINTER(Uniforms), _u32, _u32, C.POINTER(TuneResult)]),

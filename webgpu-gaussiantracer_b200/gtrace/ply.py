@@ -34,28 +34,63 @@ class PlyError(ValueError):
     """Raised for a file the reference's loader could not read either."""
 
 
+_JS_SPACE = " \t\n\v\f\r"
+_PROPERTY_RE = re.compile(r"([A-Za-z0-9_]+)[ \t\n\v\f\r]+([A-Za-z0-9_]+)[ \t\n\v\f\r]+([A-Za-z0-9_]+)")
+
+
+def _array_index(name: str):
+    """The value of a canonical array-index key ("0", or digits without a
+    leading zero below 2^32 - 1), else None: such keys of a JS object come
+    first, in ascending order."""
+    if not name or not name.isascii() or not name.isdigit() or (len(name) > 1 and name[0] == "0"):
+        return None
+    v = int(name)
+    return v if v < 4294967295 else None
+
+
 def _decode_header(buf: bytes):
-    """Returns (vertex_count, [(name, type)], data_offset) (src/GS_ply.ts:58-111)."""
-    end = buf.find(b"end_header")
-    if end < 0:
+    """Returns (vertex_count, [(name, type)], data_offset) (src/GS_ply.ts:58-111).
+
+    The reference reads the header in 50-byte chunks until the text holds
+    ``end_header`` (a file that ends inside that chunk makes its 50-byte view
+    throw), scans the trimmed lines of those chunks up to a line equal to
+    ``end_header``, and keeps ``propertyTypes`` as a JS object: array-index
+    names first in ascending order, then the others in first-insertion order,
+    a repeated name keeping its place with the later type, ``__proto__``
+    creating no entry.  The body starts one byte past the first
+    ``end_header``.  The header must be ASCII here (the reference takes byte
+    offsets from UTF-8-decoded text, which only agree for ASCII)."""
+    pos = buf.find(b"end_header")
+    if pos < 0:
         raise PlyError("PLY header has no end_header")
-    text = buf[:end + len(b"end_header")].decode("latin-1")
+    chunk_end = (pos + 10 + 49) // 50 * 50
+    if chunk_end > len(buf):
+        raise PlyError("the file ends inside the 50-byte header chunk that holds end_header")
+    if any(b >= 0x80 for b in buf[:pos]):
+        raise PlyError("the PLY header is not ASCII")
+    text = buf[:chunk_end].decode("latin-1")
     count = 0
-    props: list[tuple[str, str]] = []
+    named: dict[str, str] = {}
+    indexed: dict[int, tuple[str, str]] = {}
     for raw in text.split("\n"):
-        line = raw.strip()
+        line = raw.strip(_JS_SPACE)
         if line.startswith("element vertex"):
-            m = re.search(r"\d+", line)
+            m = re.search(r"[0-9]+", line)
             if m:
                 count = int(m.group(0))
         elif line.startswith("property"):
-            m = re.match(r"(\w+)\s+(\w+)\s+(\w+)", line)
-            if m:
+            m = _PROPERTY_RE.search(line)
+            if m and m.group(3) != "__proto__":
                 name, typ = m.group(3), m.group(2)
-                props = [p for p in props if p[0] != name] + [(name, typ)]
+                idx = _array_index(name)
+                if idx is not None:
+                    indexed[idx] = (name, typ)
+                else:
+                    named[name] = typ  # a dict keeps the first insertion's place
         elif line == "end_header":
             break
-    return count, props, end + len(b"end_header") + 1
+    props = [indexed[i] for i in sorted(indexed)] + list(named.items())
+    return count, props, pos + 10 + 1
 
 
 def _sh_feature_order(n_rest: int) -> list[str]:
@@ -102,20 +137,23 @@ class PackedGaussians:
         degree = int(degree)
         self.numGaussians = count
         self.sphericalHarmonicsDegree = degree
-        dtype = []
-        for name, typ in props:
-            if typ not in ("float", "uchar"):
-                # the reference skips other types without advancing its read offset
-                raise PlyError(f"property type {typ} is not read by the reference loader")
-            dtype.append((name, _PLY_TYPES[typ]))
+        if count >= 2 ** 31:
+            raise PlyError("at most 2^31 - 1 vertices")
+        # the reference reads float and uchar properties and skips other types
+        # without advancing its read offset (src/GS_ply.ts:120-128)
+        dtype = [(name, _PLY_TYPES[typ]) for name, typ in props if typ in ("float", "uchar")]
+        readable = {name for name, _ in dtype}
+        required = (["x", "y", "z", "scale_0", "scale_1", "scale_2", "rot_0", "rot_1", "rot_2", "rot_3", "opacity"]
+                    + _sh_feature_order(n_rest))
+        for name in required:
+            if name not in readable:
+                raise PlyError(f"missing float/uchar vertex property {name}")
         dt = np.dtype(dtype)
-        if offset + dt.itemsize * count > len(buf):
+        if count and offset + dt.itemsize * count > len(buf):
             raise PlyError("PLY vertex data is shorter than the header says")
         rows = np.frombuffer(buf, dtype=dt, count=count, offset=offset)
 
         def col(name: str) -> np.ndarray:
-            if name not in dt.names:
-                raise PlyError(f"missing property {name}")
             v = rows[name].astype(np.float64)
             if dt[name] == np.dtype("u1"):
                 v = v / 255.0
@@ -124,7 +162,9 @@ class PackedGaussians:
         pos = np.stack([col("x"), col("y"), col("z")], axis=1)
         scale = np.exp(np.stack([col("scale_0"), col("scale_1"), col("scale_2")], axis=1))
         q = np.stack([col(f"rot_{i}") for i in range(4)], axis=1)
-        q = q / np.sqrt((q ** 2).sum(axis=1, keepdims=True))
+        # ((q0^2 + q1^2) + q2^2) + q3^2, the JS expression's order
+        norm = np.sqrt(((q[:, 0] * q[:, 0] + q[:, 1] * q[:, 1]) + q[:, 2] * q[:, 2]) + q[:, 3] * q[:, 3])
+        q = q / norm[:, None]
         opacity = 1.0 / (1.0 + np.exp(-col("opacity")))
         n_sh = (degree + 1) ** 2
         order = _sh_feature_order(n_rest)

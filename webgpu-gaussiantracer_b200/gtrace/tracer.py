@@ -79,16 +79,21 @@ class Context:
 
     # ------------------------------------------------------------- render
     def render(self, scene: "Scene", uniforms, width: int, height: int, out: np.ndarray | None = None,
-               stats: bool = False, checkpoint: bool = False):
+               stats: bool = False, checkpoint: bool = False, antialias: bool = False):
         """Renders one view to a host array of shape (height, width, 4).
-        checkpoint=True keeps the round checkpoint for a following backward."""
+        checkpoint=True keeps the round checkpoint for a following backward.
+        antialias=True takes the jittered sample of frame
+        ``uniforms.accumulated_frames`` and blends it into ``out`` (the
+        reference's progressive average; frame 0 replaces it)."""
         u = _uniforms(uniforms)
         if out is None:
+            if antialias and u.accumulated_frames != 0:
+                raise ValueError("antialias frames after the first blend into `out`: pass it")
             out = np.empty((height, width, 4), dtype=np.float32)
         if out.dtype != np.float32 or not out.flags.c_contiguous or out.size != width * height * 4:
             raise ValueError("out must be a C-contiguous float32 array of width*height*4 values")
         st = L.RenderStats()
-        flags = L.GT_FLAG_CHECKPOINT if checkpoint else 0
+        flags = (L.GT_FLAG_CHECKPOINT if checkpoint else 0) | (L.GT_FLAG_ANTIALIAS if antialias else 0)
         self.check(self._lib.gt_render(self._h, scene.handle, C.byref(u), width, height,
                                        out.ctypes.data_as(C.c_void_p), flags, C.byref(st)))
         return (out, st.as_dict()) if stats else out
@@ -226,6 +231,32 @@ class Context:
         self.check(self._lib.gt_set_tune(self._h, scene.handle, C.byref(_uniforms(uniforms)), width, height,
                                          C.byref(r)))
 
+    # ------------------------------------------------------------ display
+    def tonemap(self, rgba: np.ndarray, mode: int = L.GT_TONEMAP_HDR, exposure: float = 1.66) -> np.ndarray:
+        """The reference's tone-map pass (src/toneMapper.ts:15-24) into a
+        headless RGBA8 image of the same height and width."""
+        a = np.ascontiguousarray(rgba, dtype=np.float32)
+        if a.size % 4:
+            raise ValueError("rgba holds 4 floats per pixel")
+        n = a.size // 4
+        out = np.zeros(a.shape[:-1] + (4,) if a.ndim > 1 and a.shape[-1] == 4 else (n, 4), dtype=np.uint8)
+        self.check(self._lib.gt_tonemap(self._h, a.ctypes.data_as(C.c_void_p), n, mode, exposure,
+                                        out.ctypes.data_as(C.c_void_p), 0))
+        return out
+
+    # --------------------------------------------------------- PLY ingest
+    def pack_ply(self, data: bytes):
+        """Native ``PackedGaussians(arrayBuffer).gaussiansBuffer``: the PLY
+        blob decoded, activated and packed on the GPU.  Returns the records as
+        a float32 array of shape (n, record_stride / 4) and the header info."""
+        buf = np.frombuffer(bytes(data), dtype=np.uint8)
+        info = ply_header(buf)
+        out = np.zeros((info["n_vertices"], info["record_stride"] // 4), dtype=np.float32)
+        pi = L.PlyInfo()
+        self.check(self._lib.gt_ply_pack(self._h, buf.ctypes.data_as(C.c_void_p), buf.size,
+                                         out.ctypes.data_as(C.c_void_p), out.nbytes, 0, C.byref(pi)))
+        return out, pi.as_dict()
+
     # ----------------------------------------------------------- helpers
     def device_alloc(self, nbytes: int) -> int:
         p = C.c_void_p()
@@ -296,6 +327,32 @@ class Scene:
         self.alpha_min = alpha_min
         ctx._scenes.add(self)
 
+    @classmethod
+    def from_ply(cls, ctx: Context, source, alpha_min: float, fast_build: bool = False) -> "Scene":
+        """Builds a scene straight from a 3DGS PLY (bytes, or a file path as
+        str): loadGaussianSplatting + PackedGaussians + gaussianSceneToBvh,
+        with decoding, activation and packing done natively.  The header info
+        is kept in ``ply_info``."""
+        self = cls.__new__(cls)
+        self.ctx = ctx
+        self._lib = ctx._lib
+        h = C.c_void_p()
+        pi = L.PlyInfo()
+        fb = L.GT_FLAG_FAST_BUILD if fast_build else 0
+        if isinstance(source, str):
+            ctx.check(self._lib.gt_scene_create_from_ply_file(ctx.handle, source.encode(), float(alpha_min), fb,
+                                                              C.byref(h), C.byref(pi)))
+        else:
+            buf = np.frombuffer(bytes(source), dtype=np.uint8)
+            ctx.check(self._lib.gt_scene_create_from_ply(ctx.handle, buf.ctypes.data_as(C.c_void_p), buf.size,
+                                                         float(alpha_min), fb, C.byref(h), C.byref(pi)))
+        self._h = h
+        self.n = int(pi.n_vertices)
+        self.alpha_min = alpha_min
+        self.ply_info = pi.as_dict()
+        ctx._scenes.add(self)
+        return self
+
     @property
     def handle(self):
         if not self._h:
@@ -319,6 +376,19 @@ class Scene:
             self.close()
         except Exception:
             pass
+
+
+def ply_header(data) -> dict:
+    """Header of a 3DGS PLY blob as the native loader decodes it (no GPU
+    work): n_vertices, data_offset, sh_degree, record_stride, row_bytes,
+    n_properties."""
+    lib = L.load()
+    buf = np.frombuffer(bytes(data), dtype=np.uint8) if not isinstance(data, np.ndarray) else data
+    pi = L.PlyInfo()
+    L.check(lib.gt_ply_parse_header(buf.ctypes.data_as(C.c_void_p), buf.size, C.byref(pi)), None)
+    d = pi.as_dict()
+    d.pop("ingest_ms")
+    return d
 
 
 def gaussian_scene_to_bvh(ctx: Context, gs_data: PackedGaussians, alpha_min: float,

@@ -11,6 +11,12 @@
 //   gt.traceRays(ctx, scene, uniformData /* the 112-byte ArrayBuffer */, width, height,
 //                pixels /* Float32Array(width*height*4) */);
 //
+// or loads the PLY natively and shows the frame without WebGPU:
+//
+//   const scene = gt.createSceneFromPly(ctx, plyArrayBuffer, alpha_min);
+//   gt.traceRays(ctx, scene, uniformData, width, height, pixels, /*antialias=*/false);
+//   gt.toneMap(ctx, pixels, imageData.data /* Uint8ClampedArray */, 0, 1.66);
+//
 // Only plain N-API (node_api.h) is used.  Errors become JS exceptions carrying
 // gt_last_error().  Build with binding.gyp next to this file (node-gyp).
 #include <node_api.h>
@@ -126,10 +132,59 @@ napi_value DestroyScene(napi_env env, napi_callback_info info) {
   return nullptr;
 }
 
-// traceRays(ctx, scene, uniforms(112 bytes), width, height, pixels(Float32Array w*h*4))
+// createSceneFromPly(ctx, plyArrayBuffer, alphaMin): loadGaussianSplatting +
+// PackedGaussians + gaussianSceneToBvh, decoded and packed natively.
+napi_value CreateSceneFromPly(napi_env env, napi_callback_info info) {
+  napi_value argv[3];
+  if (!get_args(env, info, 3, argv)) return nullptr;
+  gt_context* ctx = get_external<gt_context>(env, argv[0]);
+  void* data = nullptr;
+  size_t len = 0;
+  if (!ctx || !get_bytes(env, argv[1], &data, &len)) return throw_error(env, "createSceneFromPly: bad arguments");
+  double alpha_min = 0.0;
+  napi_get_value_double(env, argv[2], &alpha_min);
+  gt_scene* scene = nullptr;
+  gt_ply_info pi;
+  gt_status st = gt_scene_create_from_ply(ctx, data, len, alpha_min, 0, &scene, &pi);
+  if (st != GT_OK) return throw_status(env, ctx, st);
+  napi_value out;
+  napi_create_external(env, scene, nullptr, nullptr, &out);
+  return out;
+}
+
+// toneMap(ctx, pixels(Float32Array w*h*4), rgba8(Uint8ClampedArray w*h*4), mode, exposure):
+// the display pass of src/toneMapper.ts; rgba8 can back a canvas ImageData.
+napi_value ToneMap(napi_env env, napi_callback_info info) {
+  napi_value argv[5];
+  if (!get_args(env, info, 5, argv)) return nullptr;
+  gt_context* ctx = get_external<gt_context>(env, argv[0]);
+  void *pix = nullptr, *out = nullptr;
+  size_t plen = 0, olen = 0;
+  if (!ctx || !get_bytes(env, argv[1], &pix, &plen) || !get_bytes(env, argv[2], &out, &olen))
+    return throw_error(env, "toneMap: bad arguments");
+  double exposure = 1.66;
+  napi_get_value_double(env, argv[4], &exposure);
+  const uint64_t n = plen / 16;
+  if (n * 4 > olen) return throw_error(env, "toneMap: output buffer too small");
+  gt_status st = gt_tonemap(ctx, static_cast<const float*>(pix), n, get_u32(env, argv[3]), (float)exposure,
+                            static_cast<uint8_t*>(out), 0);
+  if (st != GT_OK) return throw_status(env, ctx, st);
+  return nullptr;
+}
+
+// traceRays(ctx, scene, uniforms(112 bytes), width, height, pixels(Float32Array w*h*4)[, antialias])
+// With antialias true the pixels keep the running average of the frames
+// (uniforms.accumulatedFrames counts them), as the reference's shader does
+// when its `antialiasing` constant is true.
 napi_value TraceRays(napi_env env, napi_callback_info info) {
-  napi_value argv[6];
-  if (!get_args(env, info, 6, argv)) return nullptr;
+  napi_value argv[7];
+  size_t argc = 7;
+  if (napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr) != napi_ok || argc < 6) {
+    napi_throw_type_error(env, nullptr, "wrong number of arguments");
+    return nullptr;
+  }
+  bool antialias = false;
+  if (argc >= 7) napi_get_value_bool(env, argv[6], &antialias);
   gt_context* ctx = get_external<gt_context>(env, argv[0]);
   gt_scene* scene = get_external<gt_scene>(env, argv[1]);
   void *ub = nullptr, *pix = nullptr;
@@ -141,7 +196,8 @@ napi_value TraceRays(napi_env env, napi_callback_info info) {
   if ((uint64_t)w * h * 16 > plen) return throw_error(env, "traceRays: pixel buffer too small");
   gt_uniforms u;
   memcpy(&u, ub, sizeof u);
-  gt_status st = gt_render(ctx, scene, &u, w, h, static_cast<float*>(pix), 0, nullptr);
+  gt_status st = gt_render(ctx, scene, &u, w, h, static_cast<float*>(pix), antialias ? GT_FLAG_ANTIALIAS : 0u,
+                           nullptr);
   if (st != GT_OK) return throw_status(env, ctx, st);
   return nullptr;
 }
@@ -176,7 +232,9 @@ napi_value Init(napi_env env, napi_value exports) {
       {"destroyContext", nullptr, DestroyContext, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"createScene", nullptr, CreateScene, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"destroyScene", nullptr, DestroyScene, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"createSceneFromPly", nullptr, CreateSceneFromPly, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"traceRays", nullptr, TraceRays, nullptr, nullptr, nullptr, napi_default, nullptr},
+      {"toneMap", nullptr, ToneMap, nullptr, nullptr, nullptr, napi_default, nullptr},
       {"backward", nullptr, Backward, nullptr, nullptr, nullptr, napi_default, nullptr},
   };
   napi_define_properties(env, exports, sizeof props / sizeof props[0], props);
