@@ -196,7 +196,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewD
   __shared__ WarpScratch scratch[kWarpsPerBlock];
   const uint32_t lane = threadIdx.x & 31;
   WarpScratch& W = scratch[threadIdx.x >> 5];
-  RayStats st = {0, 0, 0, 0, 0, 0};
+  RayStats& st = W.stats;
+  if (lane == 0) st = RayStats{0, 0, 0, 0, 0, 0};
+  __syncwarp();
   uint32_t status = 0, rays = 0;
   const uint32_t total = total_tiles * 32u;
   while (true) {
@@ -282,9 +284,11 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewD
         }
       }
       if (contrib) entry_gradient(V.s, p, sd, o, d, Tme, alpha, resp, q, craw, ga, g, V.u.deg, V.grad);
-      st.rounds += lane == 0 ? 1u : 0u;
-      st.entries += lane == 0 ? (uint32_t)n : 0u;
-      st.contributing += lane == 0 ? (uint32_t)__popc(cmask) : 0u;
+      if (lane == 0) {
+        ++st.rounds;
+        st.entries += (unsigned)n;
+        st.contributing += (unsigned)__popc(cmask);
+      }
     }
   }
   flush_stats(ctr, st, rays, status);

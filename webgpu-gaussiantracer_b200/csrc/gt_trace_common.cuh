@@ -11,8 +11,10 @@ namespace gt {
 
 constexpr int kTileW = 8, kTileH = 4;
 
+// Work counters of one warp, kept in its shared scratch (not in registers)
+// and updated by lane 0 with warp totals.
 struct RayStats {
-  uint32_t rounds, entries, contributing, proxy_tests, node_visits, anyhits;
+  unsigned long long rounds, entries, contributing, proxy_tests, node_visits, anyhits;
 };
 
 // Box-test state of a ray: inverse direction, origin times inverse direction
@@ -127,7 +129,8 @@ __device__ __forceinline__ void proxy_test(const FaceTable& F, const float4* w2o
       const float mg = __fmaf_rn(trange, fabsf(dn), mbase);
       if (num >= __fmaf_rn(tlo, dn, mg) || num <= __fmaf_rn(thi, dn, -mg)) continue;
       float t;
-      if (tri_test(F, f, oo, tlo, od, thi, dn, t) && front_facing(F, f, W, d)) on_hit(t, f);
+      if (tri_test(F, f, oo, tlo, od, thi, dn, t) && front_facing(F, f, load_affine(w2o + 3 * (size_t)j), d))
+        on_hit(t, f);
     } else {
       // grazing pair: both faces go to the exact test
 #pragma unroll 1
@@ -135,7 +138,8 @@ __device__ __forceinline__ void proxy_test(const FaceTable& F, const float4* w2o
         const int f = c ? F.pb[pair] : fa;
         const float dn = c ? -dna : dna;
         float t;
-        if (tri_test(F, f, oo, tlo, od, thi, dn, t) && front_facing(F, f, W, d)) on_hit(t, f);
+        if (tri_test(F, f, oo, tlo, od, thi, dn, t) && front_facing(F, f, load_affine(w2o + 3 * (size_t)j), d))
+          on_hit(t, f);
       }
     }
   }
@@ -145,24 +149,19 @@ __device__ __forceinline__ void proxy_test(const FaceTable& F, const float4* w2o
 // a tie with the k-th hit
 __device__ __forceinline__ float next_up(float x) { return nextafterf(x, CUDART_INF_F); }
 
-__device__ __forceinline__ void flush_stats(DevCounters* ctr, RayStats& st, uint32_t rays, uint32_t status) {
-  unsigned long long v[7] = {rays, st.rounds, st.entries, st.contributing, st.proxy_tests, st.node_visits, st.anyhits};
-#pragma unroll
-  for (int i = 0; i < 7; ++i) {
-    unsigned long long x = v[i];
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xFFFFFFFFu, x, off);
-    v[i] = x;
-  }
+// Adds a warp's counters to the launch totals.  `rays` is counted by lane 0;
+// `st` is the warp's shared counter block.
+__device__ __forceinline__ void flush_stats(DevCounters* ctr, const RayStats& st, uint32_t rays, uint32_t status) {
   uint32_t s = __reduce_or_sync(0xFFFFFFFFu, status);
+  __syncwarp();
   if ((threadIdx.x & 31) == 0) {
-    atomicAdd(&ctr->rays, v[0]);
-    atomicAdd(&ctr->rounds, v[1]);
-    atomicAdd(&ctr->entries, v[2]);
-    atomicAdd(&ctr->contributing, v[3]);
-    atomicAdd(&ctr->proxy_tests, v[4]);
-    atomicAdd(&ctr->node_visits, v[5]);
-    atomicAdd(&ctr->anyhits, v[6]);
+    atomicAdd(&ctr->rays, (unsigned long long)rays);
+    atomicAdd(&ctr->rounds, st.rounds);
+    atomicAdd(&ctr->entries, st.entries);
+    atomicAdd(&ctr->contributing, st.contributing);
+    atomicAdd(&ctr->proxy_tests, st.proxy_tests);
+    atomicAdd(&ctr->node_visits, st.node_visits);
+    atomicAdd(&ctr->anyhits, st.anyhits);
     if (s) atomicOr(&ctr->status, s);
   }
 }

@@ -31,6 +31,10 @@ struct WarpScratch {
   uint32_t leafq[kLeafQueue];
   float leaft[kLeafQueue];
   uint32_t pop[4];  // nodes taken by the current pop (lanes 8s..8s+7 test pop[s])
+  float hq[kMaxHitsPerProxy][32];  // hits of each lane's proxy, column per lane
+  RayStats stats;                  // the warp's work counters (lane 0 writes)
+  float rs[4];                     // warp-uniform ray state parked during a traversal
+  uint32_t ru[8];
 };
 
 struct HitOut {
@@ -244,7 +248,7 @@ __device__ __forceinline__ void traverse8(const SceneDev& S, const FaceTable& F,
         hit = ref != kInvalid && tn <= tf;
         tnear = tn;
       }
-      st.node_visits += (lane & 7) == 0 && valid ? 1u : 0u;
+      if (lane == 0) st.node_visits += (unsigned)np;
       const bool leaf = (ref & kLeafBit) != 0;
       const uint32_t lmask = __ballot_sync(kFull, hit && leaf);
       const uint32_t imask = __ballot_sync(kFull, hit && !leaf);
@@ -314,19 +318,15 @@ __device__ __forceinline__ void traverse8(const SceneDev& S, const FaceTable& F,
         __syncwarp();
       }
       nq -= nb;
-      // one proxy per lane; its hits are kept in a register queue h0..h5
-      float h0 = 0.f, h1 = 0.f, h2 = 0.f, h3 = 0.f, h4 = 0.f, h5 = 0.f;
+      // one proxy per lane; its hits go to the lane's column of the hit queue
+      // in shared memory (registers are the kernel's scarcest resource)
       int nh = 0;
+      const uint32_t tested = __ballot_sync(kFull, have);
+      if (lane == 0) st.proxy_tests += (unsigned)__popc(tested);
       if (have) {
-        ++st.proxy_tests;
         const float tb = MODE == kCountFront ? t_max : fminf(next_up(thi), t_max);
         proxy_test<MODE != kClosestAny>(F, S.w2o, j, o, d, tlo, tb, [&](float t, int) {
-          h5 = h4;
-          h4 = h3;
-          h3 = h2;
-          h2 = h1;
-          h1 = h0;
-          h0 = t;
+          if (nh < kMaxHitsPerProxy) W.hq[nh][lane] = t;
           ++nh;
         });
         if (nh > kMaxHitsPerProxy) {
@@ -334,25 +334,19 @@ __device__ __forceinline__ void traverse8(const SceneDev& S, const FaceTable& F,
           nh = kMaxHitsPerProxy;
         }
       }
-      if (MODE == kCountFront) {
-        st.anyhits += nh;
-      } else {
-        uint32_t p = nh ? __ldg(S.leaf_pidx + j) : 0u;
-        st.anyhits += nh;
+      const uint32_t found = __reduce_add_sync(kFull, (uint32_t)nh);
+      if (lane == 0) st.anyhits += found;
+      if (MODE != kCountFront && found) {
+        __syncwarp();
+        const uint32_t p = nh ? __ldg(S.leaf_pidx + j) : 0u;
         while (true) {
-          uint32_t pend = __ballot_sync(kFull, nh > 0);
+          const uint32_t pend = __ballot_sync(kFull, nh > 0);
           if (!pend) break;
-          int src = __ffs(pend) - 1;
-          float t = __shfl_sync(kFull, h0, src);
-          uint32_t pp = __shfl_sync(kFull, p, src);
-          if ((int)lane == src) {
-            h0 = h1;
-            h1 = h2;
-            h2 = h3;
-            h3 = h4;
-            h4 = h5;
-            --nh;
-          }
+          const int src = __ffs(pend) - 1;
+          const int slot = __shfl_sync(kFull, nh, src) - 1;
+          const float t = W.hq[slot][src];
+          const uint32_t pp = __shfl_sync(kFull, p, src);
+          if ((int)lane == src) --nh;
           kbuf_insert(kb, t, pp, lane);
         }
         thi = kbuf_t_at(kb, cull);
