@@ -106,6 +106,38 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+def init_ranks():
+    """One process per GPU (torchrun): rank, world size, local rank and the
+    gloo process group used for the barrier and the max over ranks (the path
+    has no data exchange).  The short timeout ends a run whose ranks wait on a
+    rank that never arrives."""
+    import datetime
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
+    return rank, world, local, dist
+
+
+def max_over_ranks(dist, x: float) -> float:
+    """The largest value of x over all ranks (x itself without a process group)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_mrays(world: int, rays_per_rank: int, slowest_s: float) -> float:
+    """Mrays/s of the whole job: every rank traces the same view (replicas),
+    the job takes as long as its slowest rank."""
+    return world * rays_per_rank / slowest_s / 1e6
+
+
 def make_workload(name: str):
     from gtrace import synth
     if name == "clusters-1m-1080p":
@@ -127,13 +159,14 @@ def make_workload(name: str):
     return pg, amin, v, desc
 
 
-def cpu_port_throughput(pg, amin, v, budget_s: float, threads: int = 0):
+def cpu_port_throughput(pg, amin, v, budget_s: float, threads: int = 0, scene=None):
     """Times the CPU restatement of the reference algorithm (oracle, per-round
     k-buffer traversal) on stratified pixel subsets; returns Mrays/s and the
-    sample description.  Scene preparation is not timed."""
+    sample description.  Scene preparation (skipped when `scene` is given) is
+    not timed."""
     from oracle import oracle
     t0 = time.perf_counter()
-    s = oracle.Scene(pg.gaussiansBuffer, amin, "f32")
+    s = scene if scene is not None else oracle.Scene(pg.gaussiansBuffer, amin, "f32")
     prep = time.perf_counter() - t0
     w, h = v.width, v.height
     stride = 8
@@ -305,19 +338,14 @@ def main():
     ap.add_argument("--workload", default="clusters-1m-1080p")
     ap.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU baseline work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-step-budget", type=float, default=0.0,
+                    help="--impl reference: seconds of CPU work per step (0: 60 s spread over the steps)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched and forward+backward measurements")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    rank, world, local, dist = init_ranks()
 
     pg, amin, v, desc = make_workload(args.workload)
     w, h = v.width, v.height
@@ -329,10 +357,13 @@ def main():
             if dist:
                 dist.destroy_process_group()
             return
+        from oracle import oracle
+        ref_scene = oracle.Scene(pg.gaussiansBuffer, amin, "f32")
         vals = []
         sample = None
         for i in range(args.warmup + args.steps):
-            mr, n, stride, dt, prep = cpu_port_throughput(pg, amin, v, budget_s=max(2.0, 60.0 / (args.steps + 3)))
+            budget = args.ref_step_budget if args.ref_step_budget > 0 else max(2.0, 60.0 / (args.steps + 3))
+            mr, n, stride, dt, prep = cpu_port_throughput(pg, amin, v, budget_s=budget, scene=ref_scene)
             sample = f"{n} pixels (every {stride}th pixel in x and y) of the {w}x{h} view"
             if i >= args.warmup:
                 vals.append(mr)
@@ -373,13 +404,8 @@ def main():
         ms = ctx.timer_stop()
     n_launch = ctx.launch_count() - n_launch0
     ktimes = ctx.kernel_times()
-    ms_step = ms / args.steps
-    if dist:
-        import torch
-        t = torch.tensor([ms_step], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_step = float(t.item())
-    value = world * rays / (ms_step * 1e-3) / 1e6
+    ms_step = max_over_ranks(dist, ms / args.steps)
+    value = whole_job_mrays(world, rays, ms_step * 1e-3)
 
     # end to end: host output buffer (pinned), copy inside the timed region
     host = ctx.host_alloc(rays * 16, np.float32, (h, w, 4))
@@ -390,13 +416,8 @@ def main():
     t0 = time.perf_counter()
     for _ in range(args.steps):
         ctx.render(scene, v.uniforms, w, h, out=host)
-    e2e_s = (time.perf_counter() - t0) / args.steps
-    if dist:
-        import torch
-        t = torch.tensor([e2e_s], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e = world * rays / e2e_s / 1e6
+    e2e_s = max_over_ranks(dist, (time.perf_counter() - t0) / args.steps)
+    e2e = whole_job_mrays(world, rays, e2e_s)
     checksum = float(np.float64(host[..., :3]).sum())
     ctx.host_free(host)
     ctx.device_free(out_dev)
