@@ -367,6 +367,16 @@ gt_status gt_set_tune(gt_context* ctx, const gt_scene* scene, const gt_uniforms*
 /* Drops every cached tuning result of the context. */
 gt_status gt_autotune_reset(gt_context* ctx);
 
+/* ======================================================== loop limits
+ * No counterpart in the reference.  Every device loop of the trace kernels is
+ * bounded: traversal steps (4 n + 64 per traversal), stack entries (256 per
+ * warp) and rounds per ray (2^22).  A ray that reaches a bound stops, and the
+ * call returns GT_ERR_DEVICE_TIMEOUT (steps, rounds) or GT_ERR_STACK_OVERFLOW
+ * (stack) with the context still usable.  gt_set_limits lowers the bounds (0
+ * restores a default) so that callers and tests can exercise that path
+ * without a fault; it drops the context's captured batch graphs. */
+gt_status gt_set_limits(gt_context* ctx, uint32_t max_steps, uint32_t stack_entries, uint32_t max_rounds);
+
 /* ====================================================== device helpers
  * For callers without a CUDA binding of their own (the N-API addon, the
  * benchmark): plain device buffers on the context's GPU, and CUDA-event

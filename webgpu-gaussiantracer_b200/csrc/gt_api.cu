@@ -606,6 +606,22 @@ extern "C" gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items
   return finish_call(ctx, stats, slot);
 }
 
+// ======================================================== loop limits
+extern "C" gt_status gt_set_limits(gt_context* ctx, uint32_t max_steps, uint32_t stack_entries,
+                                   uint32_t max_rounds) {
+  if (!ctx) return fail(nullptr, GT_ERR_INVALID_ARG, "context is NULL");
+  if (stack_entries > (uint32_t)kWarpStack)
+    return fail(ctx, GT_ERR_INVALID_ARG, "stack_entries must be at most 256");
+  if (max_rounds > kMaxRounds) return fail(ctx, GT_ERR_INVALID_ARG, "max_rounds must be at most 2^22");
+  API_CUDA(ctx, cudaSetDevice(ctx->device));
+  API_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->faces.lim_steps = max_steps ? max_steps : 0xFFFFFFFFu;
+  ctx->faces.lim_stack = stack_entries ? stack_entries : (uint32_t)kWarpStack;
+  ctx->faces.lim_rounds = max_rounds ? max_rounds : kMaxRounds;
+  drop_graphs(ctx);  // captured launches hold the table by value
+  return GT_OK;
+}
+
 // =============================================================== tuning
 extern "C" gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const gt_uniforms* u, uint32_t w,
                                  uint32_t h, gt_tune_result* result) {

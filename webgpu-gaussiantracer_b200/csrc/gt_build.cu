@@ -109,6 +109,9 @@ void make_face_table(FaceTable* F) {
     }
   }
   F->npairs = q;
+  F->lim_steps = 0xFFFFFFFFu;
+  F->lim_stack = kWarpStack;
+  F->lim_rounds = kMaxRounds;
 }
 static_assert(sizeof(kIcoIdx) == 60 * sizeof(int), "table size");
 

@@ -24,6 +24,7 @@ constexpr uint32_t kMaxDepth = 120;        // deepest BVH the build accepts
 constexpr uint32_t kInvalid = 0xFFFFFFFFu; // empty k-buffer slot (uint(-1))
 constexpr uint32_t kLeafBit = 0x80000000u; // child reference: leaf flag
 constexpr uint32_t kMaxRounds = 1u << 22;          // round cap per ray
+constexpr int kWarpStack = 256;                    // traversal stack entries per warp
 
 // device status word bits
 constexpr uint32_t kStatusStackOverflow = 1u;
@@ -46,6 +47,14 @@ struct FaceTable {
   float c[20];     // plane offsets n . p0 (pre-check only)
   int pa[10], pb[10];  // antipodal face pairs: n[pb[q]] == -n[pa[q]] bit for bit
   int npairs;          // 10 (checked when the context is created)
+  // Device loop limits of the trace kernels (this table is a kernel
+  // parameter, so they cost no registers).  gt_set_limits lowers them to
+  // exercise the failure path: a traversal past lim_steps steps, a stack
+  // past lim_stack entries or a ray past lim_rounds rounds stops and sets a
+  // status bit that the host turns into an error.
+  uint32_t lim_steps;   // traversal steps per traversal (after 4 n_kept + 64)
+  uint32_t lim_stack;   // stack entries per warp (<= kWarpStack)
+  uint32_t lim_rounds;  // rounds per ray
 };
 void make_face_table(FaceTable* ft);
 

@@ -235,7 +235,7 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
       }
       R.n_entries += n;
       R.t_curr = new_t;
-      if (R.step >= kMaxRounds && wray_more(V, R)) {
+      if (R.step >= F.lim_rounds && wray_more(V, R)) {
         status |= kStatusRoundCap;
         R.t_curr = t_max;
       }

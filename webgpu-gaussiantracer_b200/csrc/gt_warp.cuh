@@ -20,7 +20,6 @@
 namespace gt {
 
 constexpr int kWarpsPerBlock = 4;
-constexpr int kWarpStack = 256;  // stack entries per warp
 constexpr int kLeafQueue = 96;   // leaf queue entries per warp (<= 63 in use)
 constexpr int kMaxHitsPerProxy = 6;
 constexpr uint32_t kFull = 0xFFFFFFFFu;
@@ -200,7 +199,7 @@ __device__ __forceinline__ void traverse8(const SceneDev& S, const FaceTable& F,
   __syncwarp();
   float thi = MODE == kCountFront ? t_max : kbuf_t_at(kb, cull);
   uint32_t iters = 0;
-  const uint32_t max_iters = 4u * S.n_kept + 64u;
+  const uint32_t max_iters = min(4u * S.n_kept + 64u, F.lim_steps);
   while (true) {
     if (++iters > max_iters) {
       status |= kStatusVisitCap;
@@ -262,7 +261,7 @@ __device__ __forceinline__ void traverse8(const SceneDev& S, const FaceTable& F,
       }
       if (imask) {
         const int m = __popc(imask);
-        if (sp + m > kWarpStack) {
+        if (sp + m > (int)F.lim_stack) {
           status |= kStatusStackOverflow;
           return;
         }

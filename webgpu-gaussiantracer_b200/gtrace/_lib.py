@@ -118,6 +118,7 @@ SIGNATURES = [
     ("gt_autotune", _i32, [_vp, _vp, C.POINTER(Uniforms), _u32, _u32, C.POINTER(TuneResult)]),
     ("gt_set_tune", _i32, [_vp, _vp, C.POINTER(Uniforms), _u32, _u32, C.POINTER(TuneResult)]),
     ("gt_autotune_reset", _i32, [_vp]),
+    ("gt_set_limits", _i32, [_vp, _u32, _u32, _u32]),
     ("gt_device_alloc", _i32, [_vp, _u64, C.POINTER(_vp)]),
     ("gt_device_free", _i32, [_vp, _vp]),
     ("gt_host_alloc", _i32, [_vp, _u64, C.POINTER(_vp)]),
