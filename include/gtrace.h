@@ -166,6 +166,17 @@ gt_status gt_last_error(const gt_context* ctx, char* buf, size_t len);
 gt_status gt_scene_create(gt_context* ctx, const void* packed, uint64_t n,
                           uint32_t stride_bytes, double alpha_min,
                           uint32_t flags, gt_scene** out);
+/* gt_scene_create with the activated values in double precision beside the
+ * packed records: `activated` holds 8 doubles per particle, opacity, scale
+ * x y z, rotation w x y z, exactly the numbers of gaussianData
+ * (src/GS_ply.ts:225-235) that the reference builds its proxies from
+ * (src/main.ts:72-94: the opacity cut, s = sqrt(2 ln(o / alpha_min)), the
+ * rotation and the scale).  The proxies are then built from them, as the
+ * reference's are; shading still reads the packed binary32 records, as the
+ * reference's shader does.  NULL gives gt_scene_create.  A host pointer
+ * unless GT_FLAG_INPUT_DEVICE (then both buffers are device pointers). */
+gt_status gt_scene_create_ex(gt_context* ctx, const void* packed, uint64_t n, uint32_t stride_bytes,
+                             double alpha_min, const double* activated, uint32_t flags, gt_scene** out);
 gt_status gt_scene_destroy(gt_scene* scene);
 gt_status gt_scene_get_info(const gt_scene* scene, gt_scene_info* info);
 

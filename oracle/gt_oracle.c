@@ -163,7 +163,7 @@ static int or_prop_cmp(const void* pa, const void* pb) {
 }
 
 int or_ply_to_aos(const uint8_t* bytes, size_t len, uint32_t* n_out, uint32_t* deg_out,
-                  uint32_t* stride_out, float* aos) {
+                  uint32_t* stride_out, float* aos, double* act64) {
   size_t pos = (size_t)-1;
   for (size_t i = 0; i + 10 <= len; ++i)
     if (memcmp(bytes + i, "end_header", 10) == 0) {
@@ -310,16 +310,19 @@ int or_ply_to_aos(const uint8_t* bytes, size_t len, uint32_t* n_out, uint32_t* d
     rec[0] = (float)v[ix[0]];
     rec[1] = (float)v[ix[1]];
     rec[2] = (float)v[ix[2]];
-    rec[4] = (float)exp(v[ix[3]]);
-    rec[5] = (float)exp(v[ix[4]]);
-    rec[6] = (float)exp(v[ix[5]]);
+    double a8[8];
+    a8[0] = 1.0 / (1.0 + exp(-v[ix[10]]));
+    for (int c = 0; c < 3; ++c) a8[1 + c] = exp(v[ix[3 + c]]);
     double q0 = v[ix[6]], q1 = v[ix[7]], q2 = v[ix[8]], q3 = v[ix[9]];
     double nrm = sqrt(q0 * q0 + q1 * q1 + q2 * q2 + q3 * q3);
-    rec[8] = (float)(q0 / nrm);
-    rec[9] = (float)(q1 / nrm);
-    rec[10] = (float)(q2 / nrm);
-    rec[11] = (float)(q3 / nrm);
-    rec[12] = (float)(1.0 / (1.0 + exp(-v[ix[10]])));
+    a8[4] = q0 / nrm;
+    a8[5] = q1 / nrm;
+    a8[6] = q2 / nrm;
+    a8[7] = q3 / nrm;
+    if (act64) memcpy(act64 + 8 * g, a8, sizeof a8);
+    for (int c = 0; c < 3; ++c) rec[4 + c] = (float)a8[1 + c];
+    for (int c = 0; c < 4; ++c) rec[8 + c] = (float)a8[4 + c];
+    rec[12] = (float)a8[0];
     for (int c = 0; c < 3; ++c) rec[16 + c] = (float)v[ix[11 + c]];
     for (int i = 0; i < per_color; ++i)
       for (int c = 0; c < 3; ++c) rec[16 + 4 * (i + 1) + c] = (float)v[rest_ix[c * per_color + i]];

@@ -44,9 +44,12 @@ typedef struct or_hits {
 } or_hits;
 
 /* PLY ingest restatement of PackedGaussians (src/GS_ply.ts:58-253).
- * Returns 0 on success.  With aos == NULL only n/sh_degree/stride are set. */
+ * Returns 0 on success.  With aos == NULL only n/sh_degree/stride are set.
+ * act64 (optional, with aos): the activated values in double, 8 per vertex:
+ * opacity, scale xyz, rotation wxyz (gaussianData, before the binary32
+ * rounding of the packed records). */
 int or_ply_to_aos(const uint8_t* bytes, size_t len, uint32_t* n, uint32_t* sh_degree,
-                  uint32_t* stride, float* aos);
+                  uint32_t* stride, float* aos, double* act64);
 
 /* Progressive anti-aliasing restatement: renders the full image with the
  * jittered samples of (pixel, uniforms.accumulatedFrames) and blends it into
@@ -68,6 +71,13 @@ or_scene_f32* or_scene_create_f32(const float* aos, uint64_t n, uint32_t stride_
                                   double alpha_min);
 or_scene_f64* or_scene_create_f64(const float* aos, uint64_t n, uint32_t stride_bytes,
                                   double alpha_min);
+/* As or_scene_create_* with the activated values in double (8 per particle:
+ * opacity, scale xyz, rotation wxyz): the opacity cut and the proxies use
+ * them, as src/main.ts:72-94 uses the JS numbers; NULL = the packed values. */
+or_scene_f32* or_scene_create_ex_f32(const float* aos, uint64_t n, uint32_t stride_bytes,
+                                     double alpha_min, const double* act64);
+or_scene_f64* or_scene_create_ex_f64(const float* aos, uint64_t n, uint32_t stride_bytes,
+                                     double alpha_min, const double* act64);
 void or_scene_destroy_f32(or_scene_f32* s);
 void or_scene_destroy_f64(or_scene_f64* s);
 uint64_t or_scene_kept_f32(const or_scene_f32* s);

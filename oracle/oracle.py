@@ -41,11 +41,14 @@ def lib():
         L.or_log.restype = C.c_double
         L.or_log.argtypes = [C.c_double]
         L.or_ply_to_aos.restype = i32
-        L.or_ply_to_aos.argtypes = [vp, C.c_size_t, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32), vp]
+        L.or_ply_to_aos.argtypes = [vp, C.c_size_t, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32), vp, vp]
         for sfx in ("f32", "f64"):
             f = getattr(L, f"or_scene_create_{sfx}")
             f.restype = vp
             f.argtypes = [vp, u64, u32, C.c_double]
+            f = getattr(L, f"or_scene_create_ex_{sfx}")
+            f.restype = vp
+            f.argtypes = [vp, u64, u32, C.c_double, vp]
             getattr(L, f"or_scene_destroy_{sfx}").argtypes = [vp]
             k = getattr(L, f"or_scene_kept_{sfx}")
             k.restype = u64
@@ -79,14 +82,18 @@ def _ptr(a):
 class Scene:
     """Oracle scene in float ("f32": the bit-exact specification) or double."""
 
-    def __init__(self, packed: np.ndarray, alpha_min: float, precision: str = "f32"):
+    def __init__(self, packed: np.ndarray, alpha_min: float, precision: str = "f32", activated=None):
+        """activated: optional (n, 8) float64 opacity, scale xyz, rotation
+        wxyz, from which the proxies are built (as the reference builds them)."""
         L = lib()
         self.precision = precision
         self._aos = np.ascontiguousarray(packed, dtype=np.float32)
         n = self._aos.shape[0]
         stride = self._aos.shape[1] * 4 if n else 320
         self.n = n
-        self._h = getattr(L, f"or_scene_create_{precision}")(_ptr(self._aos), n, stride, alpha_min)
+        self._act = None if activated is None else np.ascontiguousarray(activated, dtype=np.float64).reshape(n, 8)
+        self._h = getattr(L, f"or_scene_create_ex_{precision}")(_ptr(self._aos), n, stride, alpha_min,
+                                                                _ptr(self._act))
         if not self._h:
             raise RuntimeError("oracle scene creation failed")
 
@@ -188,18 +195,21 @@ def backward_lists(scene: "Scene", uniforms, w: int, h: int, hits: dict, dL_drgb
     return out[:, :scene.n]
 
 
-def ply_to_aos(data: bytes) -> np.ndarray:
+def ply_to_aos(data: bytes, activations: bool = False):
+    """Packed records of a PLY blob; with activations=True also the (n, 8)
+    float64 activated values (opacity, scale xyz, rotation wxyz)."""
     L = lib()
     buf = np.frombuffer(data, dtype=np.uint8)
     n, deg, stride = C.c_uint32(), C.c_uint32(), C.c_uint32()
-    rc = L.or_ply_to_aos(_ptr(buf), len(data), C.byref(n), C.byref(deg), C.byref(stride), None)
+    rc = L.or_ply_to_aos(_ptr(buf), len(data), C.byref(n), C.byref(deg), C.byref(stride), None, None)
     if rc != 0:
         raise ValueError(f"oracle PLY parse failed ({rc})")
     out = np.zeros((n.value, stride.value // 4), dtype=np.float32)
-    rc = L.or_ply_to_aos(_ptr(buf), len(data), C.byref(n), C.byref(deg), C.byref(stride), _ptr(out))
+    act = np.zeros((n.value, 8), dtype=np.float64)
+    rc = L.or_ply_to_aos(_ptr(buf), len(data), C.byref(n), C.byref(deg), C.byref(stride), _ptr(out), _ptr(act))
     if rc != 0:
         raise ValueError(f"oracle PLY parse failed ({rc})")
-    return out
+    return (out, act) if activations else out
 
 
 def tonemap(rgba: np.ndarray, mode: int, exposure: float = 1.66) -> np.ndarray:

@@ -63,3 +63,17 @@ def test_mirror_matches_oracle_large():
     ties = P.check_activation(pg.gaussiansBuffer, aos, P.exact_words(pg))
     assert ties <= 2
 
+
+
+def test_oracle_activations_match_mirror():
+    """The double activations behind the packed records (the values the
+    reference builds its proxies from) agree between the oracle's loader and
+    the mirror to an ulp of exp, and round to the packed words."""
+    blob = P.standard(3000, 3, seed=77)
+    pg = ply.PackedGaussians(blob)
+    aos, act = oracle.ply_to_aos(blob, activations=True)
+    mirror = pg.activations()
+    assert act.shape == mirror.shape == (3000, 8)
+    assert np.all(np.abs(act - mirror) <= 2 * np.spacing(np.abs(mirror)))
+    assert np.array_equal(act[:, 4:].astype(np.float32), aos[:, 8:12])
+    assert np.array_equal(act[:, 0].astype(np.float32), aos[:, 12])

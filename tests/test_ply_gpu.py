@@ -57,17 +57,26 @@ def test_pack_large_unaligned(ctx):
 
 
 def test_scene_from_ply_renders_like_packed(ctx):
+    """A PLY scene's proxies come from the double activations (as the
+    reference's do): the same image as gt_scene_create_ex with the oracle's
+    activations, and as the oracle's scene built from them."""
     blob = ply.write_ply(synth.raw_small(n=6000, seed=synth.SEED_BASE + 5))
-    packed = oracle.ply_to_aos(blob)
+    packed, act = oracle.ply_to_aos(blob, activations=True)
     v = synth.view(128, 96, (0.0, 0.0, 4.0), k=6)
     a = Scene.from_ply(ctx, blob, 0.01)
-    b = Scene(ctx, packed, 0.01)
+    b = Scene(ctx, packed, 0.01, activated=act)
     assert a.n == 6000 and a.ply_info["sh_degree"] == 3
     ia = ctx.render(a, v.uniforms, v.width, v.height)
     ib = ctx.render(b, v.uniforms, v.width, v.height)
     assert np.array_equal(ia.view(np.uint32), ib.view(np.uint32))
-    ref, _ = oracle.Scene(packed, 0.01, "f32").render(v.uniforms, v.width, v.height)
+    ref, _ = oracle.Scene(packed, 0.01, "f32", activated=act).render(v.uniforms, v.width, v.height)
     assert np.array_equal(ia.reshape(-1, 4).view(np.uint32), ref.view(np.uint32))
+    # the mirror's gaussianData gives the same proxies
+    c = Scene(ctx, ply.PackedGaussians(blob).gaussiansBuffer, 0.01,
+              activated=ply.PackedGaussians(blob).activations())
+    ic = ctx.render(c, v.uniforms, v.width, v.height)
+    assert np.array_equal(ia.view(np.uint32), ic.view(np.uint32))
+    c.close()
     with tempfile.TemporaryDirectory() as d:
         path = os.path.join(d, "scene.ply")
         with open(path, "wb") as fh:
@@ -91,9 +100,41 @@ def test_lower_degree_scene(ctx):
     blob = ply.write_ply(raw1, sh_degree=1)
     s = Scene.from_ply(ctx, blob, 0.01)
     assert s.ply_info["record_stride"] == 128
-    packed = oracle.ply_to_aos(blob)
+    packed, act = oracle.ply_to_aos(blob, activations=True)
     v = synth.view(96, 64, (0.0, 0.0, 4.0), k=6)
     img = ctx.render(s, v.uniforms, v.width, v.height)
-    ref, _ = oracle.Scene(packed, 0.01, "f32").render(v.uniforms, v.width, v.height)
+    ref, _ = oracle.Scene(packed, 0.01, "f32", activated=act).render(v.uniforms, v.width, v.height)
     assert np.array_equal(img.reshape(-1, 4).view(np.uint32), ref.view(np.uint32))
     s.close()
+
+
+def test_opacity_cut_in_double_like_the_reference(ctx):
+    """The reference cuts proxies on the double opacity (src/main.ts:79). With
+    alpha_min between a Gaussian's double opacity and its binary32 rounding,
+    the Gaussian keeps its proxy from a PLY (or with gt_scene_create_ex) and
+    loses it with gt_scene_create on the packed records.  Its proxy's hits
+    then take k-buffer slots in the rounds of the rays through it, as in the
+    reference, and the image equals the oracle's built the same way."""
+    x = np.float32(-4.6)
+    while True:  # a binary32 logit whose double opacity rounds down to binary32
+        o = 1.0 / (1.0 + np.exp(-np.float64(x)))
+        if np.float64(np.float32(o)) < o:
+            break
+        x = np.nextafter(x, np.float32(0))
+    alpha_min = (float(np.float32(o)) + o) / 2.0
+    raw = synth.raw_small(n=400, seed=synth.SEED_BASE + 8)
+    raw["opacity_logit"][:50] = x
+    blob = ply.write_ply(raw)
+    pg = ply.PackedGaussians(blob)
+    assert (pg.gaussianData["opacity"][:50] > alpha_min).all()
+    assert (pg.gaussiansBuffer[:50, 12].astype(np.float64) < alpha_min).all()
+    a = Scene.from_ply(ctx, blob, alpha_min)
+    b = Scene(ctx, pg.gaussiansBuffer, alpha_min)
+    assert a.info()["n_kept"] == b.info()["n_kept"] + 50
+    packed, act = oracle.ply_to_aos(blob, activations=True)
+    v = synth.view(80, 60, (0.0, 0.0, 4.0), k=3)
+    img = ctx.render(a, v.uniforms, v.width, v.height)
+    ref, _ = oracle.Scene(packed, alpha_min, "f32", activated=act).render(v.uniforms, v.width, v.height)
+    assert np.array_equal(img.reshape(-1, 4).view(np.uint32), ref.view(np.uint32))
+    a.close()
+    b.close()

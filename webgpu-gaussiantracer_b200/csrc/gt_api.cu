@@ -269,6 +269,11 @@ extern "C" gt_status gt_last_error(const gt_context* ctx, char* buf, size_t len)
 // ================================================================ scene
 extern "C" gt_status gt_scene_create(gt_context* ctx, const void* packed, uint64_t n, uint32_t stride_bytes,
                                      double alpha_min, uint32_t flags, gt_scene** out) {
+  return gt_scene_create_ex(ctx, packed, n, stride_bytes, alpha_min, nullptr, flags, out);
+}
+
+extern "C" gt_status gt_scene_create_ex(gt_context* ctx, const void* packed, uint64_t n, uint32_t stride_bytes,
+                                        double alpha_min, const double* activated, uint32_t flags, gt_scene** out) {
   if (!ctx) return fail(nullptr, GT_ERR_INVALID_ARG, "context is NULL");
   if (!out) return fail(ctx, GT_ERR_INVALID_ARG, "out is NULL");
   *out = nullptr;
@@ -290,6 +295,20 @@ extern "C" gt_status gt_scene_create(gt_context* ctx, const void* packed, uint64
     }
     dev = tmp;
   }
+  const double* act = activated;
+  double* act_tmp = nullptr;
+  if (n > 0 && activated && !(flags & GT_FLAG_INPUT_DEVICE)) {
+    cudaError_t e = cudaMalloc(&act_tmp, n * 8 * sizeof(double));
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(act_tmp, activated, n * 8 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) {
+      cudaFree(act_tmp);
+      cudaFree(tmp);
+      return fail(ctx, e == cudaErrorMemoryAllocation ? GT_ERR_OOM : GT_ERR_CUDA,
+                  std::string("upload of the activated values: ") + cudaGetErrorString(e));
+    }
+    act = act_tmp;
+  }
   gt_scene* s = new gt_scene();
   s->ctx = ctx;
   s->n = n;
@@ -297,10 +316,11 @@ extern "C" gt_status gt_scene_create(gt_context* ctx, const void* packed, uint64
   s->alpha_min = alpha_min;
   cudaEventRecord(ctx->call0, ctx->stream);
   Err e = build_scene(dev, n, stride_bytes, alpha_min, ctx->stream, &s->b, &ctx->launches,
-                      (flags & GT_FLAG_FAST_BUILD) != 0);
+                      (flags & GT_FLAG_FAST_BUILD) != 0, act);
   cudaEventRecord(ctx->call1, ctx->stream);
   cudaStreamSynchronize(ctx->stream);
   if (tmp) cudaFree(tmp);
+  if (act_tmp) cudaFree(act_tmp);
   if (e.code != GT_OK) {
     free_scene(&s->b);
     delete s;

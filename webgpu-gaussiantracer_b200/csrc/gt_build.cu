@@ -124,10 +124,36 @@ struct IcoVerts {
 // with R = wgpu-matrix mat3.fromQuat([x, y, z, w]) evaluated in double and
 // rounded to binary32 (Float32Array), s*scale rounded to binary32, and each
 // column entry the binary32 product of the two.
-__device__ __forceinline__ void proxy_o2w(const float* rec, double alpha_min, float M[12]) {
-  double o = (double)rec[12];
+// The activated values the proxy is built from: opacity, scale xyz and
+// rotation wxyz.  The reference builds its proxies from the JS numbers of
+// gaussianData (double); when the caller supplies them (act64, 8 doubles per
+// particle in that order) they are used, else the packed binary32 values.
+struct Act64 {
+  double o, s[3], q[4];
+};
+__device__ __forceinline__ Act64 activation(const float* rec, const double* act64, uint64_t i) {
+  Act64 a;
+  if (act64) {
+    const double* p = act64 + 8 * i;
+    a.o = p[0];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) a.s[c] = p[1 + c];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) a.q[c] = p[4 + c];
+  } else {
+    a.o = rec[12];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) a.s[c] = rec[4 + c];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) a.q[c] = rec[8 + c];
+  }
+  return a;
+}
+
+__device__ __forceinline__ void proxy_o2w(const float* rec, const Act64& A, double alpha_min, float M[12]) {
+  double o = A.o;
   double s = __dsqrt_rn(__dmul_rn(2.0, det_log(__ddiv_rn(o, alpha_min))));
-  double w = rec[8], x = rec[9], y = rec[10], z = rec[11];
+  double w = A.q[0], x = A.q[1], y = A.q[2], z = A.q[3];
   double x2 = x + x, y2 = y + y, z2 = z + z;
   double xx = x * x2, yx = y * x2, yy = y * y2;
   double zx = z * x2, zy = z * y2, zz = z * z2;
@@ -135,7 +161,7 @@ __device__ __forceinline__ void proxy_o2w(const float* rec, double alpha_min, fl
   double R[9] = {1.0 - yy - zz, yx + wz, zx - wy, yx - wz, 1.0 - xx - zz, zy + wx, zx + wy, zy - wx, 1.0 - xx - yy};
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    float Sc = __double2float_rn(__dmul_rn(s, (double)rec[4 + c]));
+    float Sc = __double2float_rn(__dmul_rn(s, A.s[c]));
 #pragma unroll
     for (int r = 0; r < 3; ++r) M[3 * c + r] = __double2float_rn(R[3 * c + r]) * Sc;
   }
@@ -165,10 +191,11 @@ __device__ __forceinline__ const float* record(const uint8_t* packed, uint64_t i
 }
 
 __global__ void k_keep_flags(const uint8_t* packed, uint64_t n, uint32_t stride, double alpha_min,
-                             uint32_t* flags) {
+                             const double* act64, uint32_t* flags) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  flags[i] = ((double)record(packed, i, stride)[12] > alpha_min) ? 1u : 0u;
+  const double o = act64 ? act64[8 * i] : (double)record(packed, i, stride)[12];
+  flags[i] = (o > alpha_min) ? 1u : 0u;
 }
 
 // float min/max through order-preserving integer maps (for atomics)
@@ -181,7 +208,7 @@ __device__ __forceinline__ float ord2f(uint32_t u) {
 }
 
 __global__ void k_proxy_boxes(const uint8_t* packed, uint64_t n, uint32_t stride, double alpha_min,
-                              const uint32_t* flags, const uint32_t* slots, const IcoVerts iv, float* box,
+                              const double* act64, const uint32_t* flags, const uint32_t* slots, const IcoVerts iv, float* box,
                               uint32_t* kept_pidx, uint32_t* bounds_ord) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   float cmin[3] = {CUDART_INF_F, CUDART_INF_F, CUDART_INF_F}, cmax[3] = {-CUDART_INF_F, -CUDART_INF_F, -CUDART_INF_F};
@@ -189,7 +216,7 @@ __global__ void k_proxy_boxes(const uint8_t* packed, uint64_t n, uint32_t stride
   if (i < n && flags[i]) {
     const float* rec = record(packed, i, stride);
     float M[12];
-    proxy_o2w(rec, alpha_min, M);
+    proxy_o2w(rec, activation(rec, act64, i), alpha_min, M);
     Affine A;
 #pragma unroll
     for (int q = 0; q < 12; ++q) A.m[q] = M[q];
@@ -484,15 +511,16 @@ __global__ void k_karras(const uint32_t* keys, int n, float4* nodes, uint32_t* p
 }
 
 // Leaf records in leaf order: world-to-object map, particle index, box.
-__global__ void k_leaves(const uint8_t* packed, uint32_t stride, double alpha_min, const uint32_t* sorted_slots,
-                         uint32_t m, const uint32_t* kept_pidx, const float* box_by_slot, float4* w2o,
+__global__ void k_leaves(const uint8_t* packed, uint32_t stride, double alpha_min, const double* act64,
+                         const uint32_t* sorted_slots, uint32_t m, const uint32_t* kept_pidx, const float* box_by_slot, float4* w2o,
                          uint32_t* leaf_pidx, float* leaf_box) {
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= m) return;
   uint32_t slot = sorted_slots[j];
   uint32_t p = kept_pidx[slot];
   float M[12], W[12];
-  proxy_o2w(record(packed, p, stride), alpha_min, M);
+  const float* rec = record(packed, p, stride);
+  proxy_o2w(rec, activation(rec, act64, p), alpha_min, M);
   affine_inverse(M, W);
   w2o[3 * (size_t)j] = make_float4(W[0], W[1], W[2], W[3]);
   w2o[3 * (size_t)j + 1] = make_float4(W[4], W[5], W[6], W[7]);
@@ -757,7 +785,7 @@ void free_scene(SceneBuffers* b) {
 static inline unsigned grid_for(uint64_t n, unsigned block) { return (unsigned)((n + block - 1) / block); }
 
 Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride, double alpha_min, cudaStream_t st,
-                SceneBuffers* out, uint64_t* launches, bool fast_build) {
+                SceneBuffers* out, uint64_t* launches, bool fast_build, const double* act64) {
   SceneBuffers b;
   b.n_sh = std::min<uint32_t>(16u, (stride - 64u) / 16u);
   const uint8_t* packed = static_cast<const uint8_t*>(packed_dev);
@@ -776,7 +804,7 @@ Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride, double alph
   GT_CUDA_TRY(cudaMallocAsync(&slots, n * 4, st));
   GT_CUDA_TRY(cudaMallocAsync(&bounds, 8 * 4, st));
   const unsigned B = 256;
-  k_keep_flags<<<grid_for(n, B), B, 0, st>>>(packed, n, stride, alpha_min, flags);
+  k_keep_flags<<<grid_for(n, B), B, 0, st>>>(packed, n, stride, alpha_min, act64, flags);
   ++*launches;
   GT_CUDA_TRY(cudaGetLastError());
   Err e = scan_exclusive(flags, slots, n, st, launches);
@@ -809,7 +837,8 @@ Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride, double alph
   }
   IcoVerts iv;
   ico_vertices(iv.v);
-  k_proxy_boxes<<<grid_for(n, B), B, 0, st>>>(packed, n, stride, alpha_min, flags, slots, iv, box, kept_pidx, bounds);
+  k_proxy_boxes<<<grid_for(n, B), B, 0, st>>>(packed, n, stride, alpha_min, act64, flags, slots, iv, box, kept_pidx,
+                                              bounds);
   ++*launches;
   k_morton<<<grid_for(m, B), B, 0, st>>>(box, m, bounds, keys, vals);
   ++*launches;
@@ -832,7 +861,7 @@ Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride, double alph
   GT_CUDA_TRY(cudaMallocAsync(&depth, 4, st));
   GT_CUDA_TRY(cudaMemsetAsync(arrive, 0, (size_t)std::max<uint32_t>(n_int, 1) * 4, st));
   GT_CUDA_TRY(cudaMemsetAsync(depth, 0, 4, st));
-  k_leaves<<<grid_for(m, B), B, 0, st>>>(packed, stride, alpha_min, vals, m, kept_pidx, box, b.w2o, b.leaf_pidx,
+  k_leaves<<<grid_for(m, B), B, 0, st>>>(packed, stride, alpha_min, act64, vals, m, kept_pidx, box, b.w2o, b.leaf_pidx,
                                           leaf_box);
   ++*launches;
   if (m > 1) {

@@ -172,9 +172,13 @@ struct SceneBuffers {
   uint64_t bytes = 0;
 };
 // fast_build: Karras LBVH (a few ms for 1M proxies); otherwise PLOC
-// clustering (slower to build, faster to trace).
+// clustering (slower to build, faster to trace).  act64 (device, optional):
+// the activated values in double, 8 per particle (opacity, scale xyz,
+// rotation wxyz), from which the proxies are then built, as the reference
+// builds them from its JS numbers; shading always uses the packed records.
 Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride_bytes, double alpha_min,
-                cudaStream_t stream, SceneBuffers* out, uint64_t* launches, bool fast_build = false);
+                cudaStream_t stream, SceneBuffers* out, uint64_t* launches, bool fast_build = false,
+                const double* act64 = nullptr);
 // Binary hierarchy over m leaves in Morton order by PLOC (gt_ploc.cu): root 0,
 // node format and parent links as the Karras build plus refit produce them.
 Err build_ploc(const float* leaf_box, uint32_t m, cudaStream_t st, float4* nodes, float* ibox, uint32_t* parent_int,

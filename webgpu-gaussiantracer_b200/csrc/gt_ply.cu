@@ -295,6 +295,30 @@ __device__ __forceinline__ float ply_word(const uint8_t* row, const PlyFields& F
   return 0.0f;
 }
 
+// The activated values in double of vertex i: opacity, scale x y z, rotation
+// w x y z (the reference's gaussianData numbers, src/GS_ply.ts:225-235), by
+// the same operations as ply_word before its rounding to binary32.
+__global__ void k_ply_act64(const uint8_t* __restrict__ body, uint64_t n, const __grid_constant__ PlyFields F,
+                            double* __restrict__ act) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint8_t* row = body + i * F.row_bytes;
+  double* a = act + 8 * i;
+  const double x = ply_value(row, F.field[10]);
+  a[0] = __ddiv_rn(1.0, __dadd_rn(1.0, exp(-x)));
+#pragma unroll
+  for (int c = 0; c < 3; ++c) a[1 + c] = exp(ply_value(row, F.field[3 + c]));
+  const double q0 = ply_value(row, F.field[6]), q1 = ply_value(row, F.field[7]);
+  const double q2 = ply_value(row, F.field[8]), q3 = ply_value(row, F.field[9]);
+  const double s = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(q0, q0), __dmul_rn(q1, q1)), __dmul_rn(q2, q2)),
+                             __dmul_rn(q3, q3));
+  const double norm = __dsqrt_rn(s);
+  a[4] = __ddiv_rn(q0, norm);
+  a[5] = __ddiv_rn(q1, norm);
+  a[6] = __ddiv_rn(q2, norm);
+  a[7] = __ddiv_rn(q3, norm);
+}
+
 // One tile of rows per iteration: coalesced loads of the rows into shared
 // memory, one (row, word) item per thread step, coalesced 16-byte stores.
 __global__ void __launch_bounds__(256) k_ply_pack(const uint8_t* __restrict__ body, uint64_t n,
@@ -357,9 +381,12 @@ static Err launch_ply_pack(const PlyLayout& L, const uint8_t* body_dev, float* o
 }
 
 // Uploads the body of a host PLY buffer and packs it into a new device
-// buffer (*packed_dev, L.n * L.stride bytes).
-static Err ply_to_device(gt_context* ctx, const uint8_t* data, const PlyLayout& L, float** packed_dev) {
+// buffer (*packed_dev, L.n * L.stride bytes); with act_dev also the
+// activated values in double (8 per vertex) into a second new buffer.
+static Err ply_to_device(gt_context* ctx, const uint8_t* data, const PlyLayout& L, float** packed_dev,
+                         double** act_dev = nullptr) {
   *packed_dev = nullptr;
+  if (act_dev) *act_dev = nullptr;
   if (L.n == 0) return Err{};
   uint8_t* body = nullptr;
   float* packed = nullptr;
@@ -373,6 +400,30 @@ static Err ply_to_device(gt_context* ctx, const uint8_t* data, const PlyLayout& 
             std::string("PLY upload: ") + cudaGetErrorString(e)};
   } else {
     r = launch_ply_pack(L, body, packed, ctx->num_sms, ctx->stream, &ctx->launches);
+    if (r.code == GT_OK && act_dev) {
+      double* act = nullptr;
+      e = cudaMalloc(&act, L.n * 8 * sizeof(double));
+      if (e != cudaSuccess) {
+        r = Err{e == cudaErrorMemoryAllocation ? GT_ERR_OOM : GT_ERR_CUDA,
+                std::string("PLY activations: ") + cudaGetErrorString(e)};
+      } else {
+        PlyFields F;
+        memcpy(F.field, L.field, sizeof F.field);
+        F.row_bytes = L.row_bytes;
+        F.stride = L.stride;
+        F.n_sh = L.n_sh;
+        F.rows_per_tile = 1;
+        k_ply_act64<<<(unsigned)((L.n + 255) / 256), 256, 0, ctx->stream>>>(body, L.n, F, act);
+        ++ctx->launches;
+        e = cudaGetLastError();
+        if (e != cudaSuccess) {
+          cudaFree(act);
+          r = Err{GT_ERR_CUDA, std::string("PLY activations: ") + cudaGetErrorString(e)};
+        } else {
+          *act_dev = act;
+        }
+      }
+    }
     if (r.code == GT_OK) {
       e = cudaStreamSynchronize(ctx->stream);
       if (e != cudaSuccess) r = Err{GT_ERR_CUDA, std::string("PLY pack: ") + cudaGetErrorString(e)};
@@ -381,6 +432,10 @@ static Err ply_to_device(gt_context* ctx, const uint8_t* data, const PlyLayout& 
   cudaFree(body);
   if (r.code != GT_OK) {
     cudaFree(packed);
+    if (act_dev && *act_dev) {
+      cudaFree(*act_dev);
+      *act_dev = nullptr;
+    }
     return r;
   }
   *packed_dev = packed;
@@ -489,12 +544,15 @@ extern "C" gt_status gt_scene_create_from_ply(gt_context* ctx, const void* data,
   if (ce != cudaSuccess) return api_fail(ctx, GT_ERR_CUDA, cudaGetErrorString(ce));
   cudaEventRecord(ctx->int0, ctx->stream);
   float* packed = nullptr;
-  e = ply_to_device(ctx, static_cast<const uint8_t*>(data), L, &packed);
+  double* act = nullptr;
+  e = ply_to_device(ctx, static_cast<const uint8_t*>(data), L, &packed, &act);
   if (e.code != GT_OK) return api_fail(ctx, e.code, e.msg);
   cudaEventRecord(ctx->int1, ctx->stream);
-  gt_status s = gt_scene_create(ctx, packed, L.n, L.stride, alpha_min,
-                                (flags & GT_FLAG_FAST_BUILD) | GT_FLAG_INPUT_DEVICE, out);
+  // the proxies come from the activated values in double, as the reference's do
+  gt_status s = gt_scene_create_ex(ctx, packed, L.n, L.stride, alpha_min, act,
+                                   (flags & GT_FLAG_FAST_BUILD) | GT_FLAG_INPUT_DEVICE, out);
   cudaFree(packed);
+  cudaFree(act);
   if (s == GT_OK && info) cudaEventElapsedTime(&info->ingest_ms, ctx->int0, ctx->int1);
   return s;
 }

@@ -97,6 +97,7 @@ SIGNATURES = [
     ("gt_context_destroy", _i32, [_vp]),
     ("gt_last_error", _i32, [_vp, C.c_char_p, C.c_size_t]),
     ("gt_scene_create", _i32, [_vp, _vp, _u64, _u32, C.c_double, _u32, C.POINTER(_vp)]),
+    ("gt_scene_create_ex", _i32, [_vp, _vp, _u64, _u32, C.c_double, _vp, _u32, C.POINTER(_vp)]),
     ("gt_scene_destroy", _i32, [_vp]),
     ("gt_scene_get_info", _i32, [_vp, C.POINTER(SceneInfo)]),
     ("gt_ply_parse_header", _i32, [_vp, _u64, C.POINTER(PlyInfo)]),

@@ -185,6 +185,17 @@ class PackedGaussians:
         posb[:, :3] = pos
         self.positionsBuffer = posb
 
+    def activations(self) -> np.ndarray:
+        """(n, 8) float64: opacity, scale xyz, rotation wxyz of gaussianData,
+        the values the reference builds its proxies from (src/main.ts:74-87)."""
+        d = self.gaussianData
+        n = self.numGaussians
+        if n == 0:
+            return np.zeros((0, 8), dtype=np.float64)
+        return np.ascontiguousarray(np.concatenate(
+            [np.asarray(d["opacity"], dtype=np.float64).reshape(n, 1), np.asarray(d["scale"], dtype=np.float64),
+             np.asarray(d["rotQuat"], dtype=np.float64)], axis=1))
+
     @property
     def stride_bytes(self) -> int:
         return self.gaussiansBuffer.shape[1] * 4 if self.numGaussians else record_stride(self.sphericalHarmonicsDegree)

@@ -307,13 +307,18 @@ class Scene:
     """Proxies + BVH + shading records of one packed particle buffer, on the GPU."""
 
     def __init__(self, ctx: Context, packed: np.ndarray, alpha_min: float, device_ptr: int | None = None,
-                 n: int | None = None, stride: int | None = None, fast_build: bool = False):
-        """fast_build: Karras LBVH hierarchy (quicker build, slower traversal)."""
+                 n: int | None = None, stride: int | None = None, fast_build: bool = False, activated=None):
+        """fast_build: Karras LBVH hierarchy (quicker build, slower traversal).
+        activated: optional (n, 8) float64 opacity, scale xyz, rotation wxyz
+        (PackedGaussians.activations()): the proxies are then built from these
+        double values, as the reference builds them (gt_scene_create_ex)."""
         self.ctx = ctx
         self._lib = ctx._lib
         h = C.c_void_p()
         fb = L.GT_FLAG_FAST_BUILD if fast_build else 0
         if device_ptr is not None:
+            if activated is not None:
+                raise ValueError("activated values go with a host packed buffer")
             self.n = int(n)
             ctx.check(self._lib.gt_scene_create(ctx.handle, C.c_void_p(device_ptr), self.n, int(stride),
                                                 float(alpha_min), L.GT_FLAG_INPUT_DEVICE | fb, C.byref(h)))
@@ -321,8 +326,15 @@ class Scene:
             arr = np.ascontiguousarray(packed, dtype=np.float32)
             self.n = arr.shape[0]
             stride = arr.shape[1] * 4 if arr.ndim == 2 and self.n else 320
-            ctx.check(self._lib.gt_scene_create(ctx.handle, arr.ctypes.data_as(C.c_void_p) if self.n else None,
-                                                self.n, stride, float(alpha_min), fb, C.byref(h)))
+            act = None
+            if activated is not None:
+                act = np.ascontiguousarray(activated, dtype=np.float64)
+                if act.shape != (self.n, 8):
+                    raise ValueError("activated must have shape (n, 8)")
+            ctx.check(self._lib.gt_scene_create_ex(ctx.handle, arr.ctypes.data_as(C.c_void_p) if self.n else None,
+                                                   self.n, stride, float(alpha_min),
+                                                   act.ctypes.data_as(C.c_void_p) if act is not None and self.n
+                                                   else None, fb, C.byref(h)))
         self._h = h
         self.alpha_min = alpha_min
         ctx._scenes.add(self)
@@ -394,9 +406,11 @@ def ply_header(data) -> dict:
 def gaussian_scene_to_bvh(ctx: Context, gs_data: PackedGaussians, alpha_min: float,
                           gaussian_indices: list | None = None) -> Scene:
     """gaussianSceneToBvh (src/main.ts:30-111): one proxy per Gaussian with
-    opacity > alpha_min; fills ``gaussian_indices`` with the kept particle
-    indices in order, as the reference does for its shader binding table."""
+    opacity > alpha_min, built from the double-precision gaussianData values
+    as the reference builds it; fills ``gaussian_indices`` with the kept
+    particle indices in order, as the reference does for its shader binding
+    table."""
     if gaussian_indices is not None:
         op = gs_data.gaussianData["opacity"]
         gaussian_indices.extend(np.nonzero(op > alpha_min)[0].tolist())
-    return Scene(ctx, gs_data.gaussiansBuffer, alpha_min)
+    return Scene(ctx, gs_data.gaussiansBuffer, alpha_min, activated=gs_data.activations())

@@ -105,10 +105,17 @@ napi_value DestroyContext(napi_env env, napi_callback_info info) {
   return nullptr;
 }
 
-// createScene(ctx, gaussiansBuffer, numGaussians, strideBytes, alphaMin)
+// createScene(ctx, gaussiansBuffer, numGaussians, strideBytes, alphaMin[, activated])
+// activated: Float64Array of 8 numbers per Gaussian (opacity, scale xyz,
+// rotation wxyz from gsData.gaussianData): the proxies are then built from the
+// same double values as the reference's gaussianSceneToBvh.
 napi_value CreateScene(napi_env env, napi_callback_info info) {
-  napi_value argv[5];
-  if (!get_args(env, info, 5, argv)) return nullptr;
+  napi_value argv[6];
+  size_t argc = 6;
+  if (napi_get_cb_info(env, info, &argc, argv, nullptr, nullptr) != napi_ok || argc < 5) {
+    napi_throw_type_error(env, nullptr, "wrong number of arguments");
+    return nullptr;
+  }
   gt_context* ctx = get_external<gt_context>(env, argv[0]);
   void* data = nullptr;
   size_t len = 0;
@@ -117,8 +124,12 @@ napi_value CreateScene(napi_env env, napi_callback_info info) {
   double alpha_min = 0.0;
   napi_get_value_double(env, argv[4], &alpha_min);
   if ((uint64_t)n * stride > len) return throw_error(env, "createScene: buffer smaller than n * stride");
+  void* act = nullptr;
+  size_t alen = 0;
+  if (argc >= 6 && !get_bytes(env, argv[5], &act, &alen)) return throw_error(env, "createScene: bad activated");
+  if (act && alen < (uint64_t)n * 8 * sizeof(double)) return throw_error(env, "createScene: activated too small");
   gt_scene* scene = nullptr;
-  gt_status st = gt_scene_create(ctx, data, n, stride, alpha_min, 0, &scene);
+  gt_status st = gt_scene_create_ex(ctx, data, n, stride, alpha_min, static_cast<const double*>(act), 0, &scene);
   if (st != GT_OK) return throw_status(env, ctx, st);
   napi_value out;
   napi_create_external(env, scene, nullptr, nullptr, &out);
