@@ -180,6 +180,23 @@ gt_status gt_scene_create_ex(gt_context* ctx, const void* packed, uint64_t n, ui
 gt_status gt_scene_destroy(gt_scene* scene);
 gt_status gt_scene_get_info(const gt_scene* scene, gt_scene_info* info);
 
+/* Inspection of the built hierarchy (no counterpart in the reference; the
+ * tests check its invariants with it).  Host copies of the 8-wide nodes:
+ * n_nodes8 records of 8 children x 2 float4, child c of node i at floats
+ * 64 i + 8 c: (lo.x, lo.y, lo.z, hi.x), (hi.y, hi.z, ref, 0) with ref (as
+ * uint32 bits) = 0x80000000 | leaf j, a node index, or 0xFFFFFFFF for an
+ * empty slot; and the particle index of every leaf j.  The root is node 0,
+ * or the leaf reference `root` of a one-proxy scene.  Either buffer may be
+ * NULL. */
+typedef struct gt_bvh_info {
+  uint32_t n_nodes8;
+  uint32_t n_leaves;      /* proxies (particles with opacity > alpha_min) */
+  uint32_t root;
+  uint32_t depth;         /* deepest leaf of the binary hierarchy */
+} gt_bvh_info;
+gt_status gt_scene_export_bvh(const gt_scene* scene, void* nodes8, uint64_t nodes_bytes, uint32_t* leaf_pidx,
+                              uint64_t leaf_count, gt_bvh_info* info);
+
 /* ========================================================= PLY ingest
  * Native replacement of PackedGaussians (src/GS_ply.ts:39-253): the 3DGS
  * PLY header is decoded on the host with the reference loader's rules

@@ -344,6 +344,30 @@ extern "C" gt_status gt_scene_destroy(gt_scene* s) {
   return GT_OK;
 }
 
+extern "C" gt_status gt_scene_export_bvh(const gt_scene* s, void* nodes8, uint64_t nodes_bytes, uint32_t* leaf_pidx,
+                                        uint64_t leaf_count, gt_bvh_info* info) {
+  if (!s) return fail(nullptr, GT_ERR_INVALID_ARG, "scene is NULL");
+  gt_context* ctx = s->ctx;
+  if (!info) return fail(ctx, GT_ERR_INVALID_ARG, "info is NULL");
+  memset(info, 0, sizeof *info);
+  info->n_nodes8 = s->b.n_nodes8;
+  info->n_leaves = (uint32_t)s->b.n_kept;
+  info->root = s->b.root;
+  info->depth = s->b.depth;
+  const uint64_t nb = (uint64_t)s->b.n_nodes8 * 16 * sizeof(float4);
+  API_CUDA(ctx, cudaSetDevice(ctx->device));
+  API_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (nodes8) {
+    if (nodes_bytes < nb) return fail(ctx, GT_ERR_INVALID_ARG, "nodes8 buffer smaller than n_nodes8 * 256 bytes");
+    if (nb) API_CUDA(ctx, cudaMemcpy(nodes8, s->b.nodes8, nb, cudaMemcpyDeviceToHost));
+  }
+  if (leaf_pidx) {
+    if (leaf_count < s->b.n_kept) return fail(ctx, GT_ERR_INVALID_ARG, "leaf_pidx smaller than the leaf count");
+    if (s->b.n_kept) API_CUDA(ctx, cudaMemcpy(leaf_pidx, s->b.leaf_pidx, s->b.n_kept * 4, cudaMemcpyDeviceToHost));
+  }
+  return GT_OK;
+}
+
 extern "C" gt_status gt_scene_get_info(const gt_scene* s, gt_scene_info* info) {
   if (!s || !info) return GT_ERR_INVALID_ARG;
   memset(info, 0, sizeof *info);

@@ -78,6 +78,10 @@ class TuneResult(C.Structure):
                 ("kbuf", C.c_uint32), ("leaf_batch", C.c_uint32)]
 
 
+class BvhInfo(C.Structure):
+    _fields_ = [("n_nodes8", C.c_uint32), ("n_leaves", C.c_uint32), ("root", C.c_uint32), ("depth", C.c_uint32)]
+
+
 class PlyInfo(C.Structure):
     _fields_ = [("n_vertices", C.c_uint64), ("data_offset", C.c_uint64), ("sh_degree", C.c_uint32),
                 ("record_stride", C.c_uint32), ("row_bytes", C.c_uint32), ("n_properties", C.c_uint32),
@@ -100,6 +104,7 @@ SIGNATURES = [
     ("gt_scene_create_ex", _i32, [_vp, _vp, _u64, _u32, C.c_double, _vp, _u32, C.POINTER(_vp)]),
     ("gt_scene_destroy", _i32, [_vp]),
     ("gt_scene_get_info", _i32, [_vp, C.POINTER(SceneInfo)]),
+    ("gt_scene_export_bvh", _i32, [_vp, _vp, _u64, _vp, _u64, C.POINTER(BvhInfo)]),
     ("gt_ply_parse_header", _i32, [_vp, _u64, C.POINTER(PlyInfo)]),
     ("gt_ply_pack", _i32, [_vp, _vp, _u64, _vp, _u64, _u32, C.POINTER(PlyInfo)]),
     ("gt_scene_create_from_ply", _i32, [_vp, _vp, _u64, C.c_double, _u32, C.POINTER(_vp), C.POINTER(PlyInfo)]),

@@ -378,6 +378,17 @@ class Scene:
         d["bounds"] = list(i.bounds)
         return d
 
+    def export_bvh(self):
+        """(nodes8 as a float32 array (n_nodes8, 8, 8), leaf particle indices,
+        info dict) of the built hierarchy (gt_scene_export_bvh)."""
+        info = L.BvhInfo()
+        self.ctx.check(self._lib.gt_scene_export_bvh(self.handle, None, 0, None, 0, C.byref(info)))
+        nodes = np.zeros((info.n_nodes8, 8, 8), dtype=np.float32)
+        leaves = np.zeros(info.n_leaves, dtype=np.uint32)
+        self.ctx.check(self._lib.gt_scene_export_bvh(self.handle, nodes.ctypes.data_as(C.c_void_p), nodes.nbytes,
+                                                     leaves.ctypes.data_as(C.c_void_p), leaves.size, C.byref(info)))
+        return nodes, leaves, {name: getattr(info, name) for name, _ in info._fields_}
+
     def close(self):
         if getattr(self, "_h", None) and getattr(self.ctx, "_h", None):
             self._lib.gt_scene_destroy(self._h)
