@@ -326,3 +326,26 @@ def test_render_hits_any_pixel_count(ctx, n_pix):
     got = ctx.render_hits(g, v.uniforms, w, h, pix, max_entries=33)
     _, ref = o.render(v.uniforms, w, h, pixels=pix, max_entries=33)
     _assert_hits_equal(got, ref, 33)
+
+
+@pytest.mark.gpu
+def test_batch_debug_modes_after_render_batch_of_same_shape(ctx):
+    """Render-only launches use a kernel without the debug modes; a batch of
+    the same shape that holds a debug view must still get the kernel that
+    has them (the batch graphs are keyed on it)."""
+    pg = small_scene(n=3000, seed=71)
+    s = Scene(ctx, pg.gaussiansBuffer, 0.01)
+    views = [view(40, 32, pos=(0.2 * i, 0.0, 4.0), k=5) for i in range(2)]
+    plain = [(s, v.uniforms, v.width, v.height) for v in views]
+    out1, _ = ctx.render_batch(plain)
+    for v, o in zip(views, out1):
+        np.testing.assert_array_equal(o, ctx.render(s, v.uniforms, v.width, v.height))
+    for mode in (1, 2):
+        dv = view(40, 32, pos=(0.0, 0.0, 4.0), k=5, debug_mode=mode)
+        mixed = [(s, dv.uniforms, dv.width, dv.height), plain[1]]
+        out2, _ = ctx.render_batch(mixed)
+        np.testing.assert_array_equal(out2[0], ctx.render(s, dv.uniforms, dv.width, dv.height))
+        np.testing.assert_array_equal(out2[1], out1[1])
+        ref, _ = oracle.Scene(pg.gaussiansBuffer, 0.01, "f32").render(dv.uniforms, dv.width, dv.height)
+        np.testing.assert_array_equal(out2[0].reshape(-1, 4), ref)
+    s.close()

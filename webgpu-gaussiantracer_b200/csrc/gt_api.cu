@@ -616,8 +616,13 @@ extern "C" gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items
   // size and leaf batch here, and the graph's kernel matches its slot count
   apply_shape(ctx->h_views, count, shape);
   uint32_t kb_max = 1;
-  for (uint32_t q = 0; q < count; ++q) kb_max = std::max(kb_max, ctx->h_views[q].kbuf);
-  auto key = std::make_tuple(count, total_tiles, kmax, shape.blocks_per_sm, (kb_max + 31u) / 32u);
+  bool any_debug = false;  // the graph's kernel is the debug-mode instantiation
+  for (uint32_t q = 0; q < count; ++q) {
+    kb_max = std::max(kb_max, ctx->h_views[q].kbuf);
+    any_debug = any_debug || ctx->h_views[q].u.debug != 0;
+  }
+  auto key = std::make_tuple(count, total_tiles, kmax | (any_debug ? 0x10000u : 0u), shape.blocks_per_sm,
+                             (kb_max + 31u) / 32u);
   auto it = ctx->graphs.find(key);
   if (it == ctx->graphs.end()) {
     GraphEntry g;

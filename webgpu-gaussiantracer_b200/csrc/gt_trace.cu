@@ -47,7 +47,10 @@ __device__ __forceinline__ bool wray_more(const ViewDev& V, const WRay& R) {
 // tracePath (src/GS_shader.ts:192-273) for one pixel, by one warp.
 // RECORD: write the composited hit sequence (gt_render_hits).
 // CKPT: write the round checkpoint the adjoint replays (gt_backward).
-template <bool RECORD, bool CKPT, int NB>
+// DEBUG: also handle debugMode 1 and 2.  Launches whose views all render
+// (debugMode 0) use the instantiation without them: their extra traversal
+// copies cost the render loop registers and spills (4.7 % of its time).
+template <bool RECORD, bool CKPT, int NB, bool DEBUG>
 __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTable& F, WarpScratch& W, uint32_t px,
                                                  uint32_t py, RayStats& st, uint32_t& status, uint32_t lane,
                                                  const HitOut& ho, uint32_t slot, const Ckpt& ck) {
@@ -55,7 +58,7 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
   ray_gen(V.u, V.w, V.h, px, py, R.o, R.d);
   R.br = make_boxray(R.o, R.d, V.s.scene_mag);
   const float t_max = V.u.t_max;
-  if (V.u.debug != 0) {
+  if (DEBUG && V.u.debug != 0) {
     KBuf<1> kb;
     kbuf_init(kb, t_max);
     uint32_t cnt = 0;
@@ -256,7 +259,7 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
 // without spills by 12% on the 1M-Gaussian 1080p view: the kernel is bound by
 // dependent latencies, and more warps hide them better than the spill loads
 // cost (measured 4/5/6/8/10/12/16 blocks: 111/105/104/98/112/121/140 ms).
-template <bool RECORD, bool CKPT, int NB>
+template <bool RECORD, bool CKPT, int NB, bool DEBUG>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) k_trace8(const ViewDev* __restrict__ views, uint32_t n_views,
                                                                   uint32_t total_tiles, DevCounters* ctr,
                                                                   const __grid_constant__ FaceTable F,
@@ -299,7 +302,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) k_trace8(const ViewDev
       vu[6] = py;
       vu[7] = item;
     }
-    const float4 r = trace_ray_warp<RECORD, CKPT, NB>(views[vi], F, W, px, py, st, status, lane, ho, item, ck);
+    const float4 r = trace_ray_warp<RECORD, CKPT, NB, DEBUG>(views[vi], F, W, px, py, st, status, lane, ho, item,
+                                                            ck);
     {
       __syncwarp();
       volatile uint32_t* vu = W.ru;
@@ -348,15 +352,24 @@ Err launch_trace(ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCoun
   for (uint32_t i = 0; i < n_views; ++i) kmax = std::max(kmax, views[i].kbuf);
   const uint32_t nb = (kmax + 31u) / 32u;
   const Ckpt ck = ckpt ? *ckpt : Ckpt{};
+  bool debug = false;
+  for (uint32_t i = 0; i < n_views; ++i) debug = debug || views[i].u.debug != 0;
   const void* fn;
-  if (ckpt)
-    fn = nb <= 1 ? (const void*)k_trace8<false, true, 1>
-                 : nb == 2 ? (const void*)k_trace8<false, true, 2>
-                           : nb == 3 ? (const void*)k_trace8<false, true, 3> : (const void*)k_trace8<false, true, 4>;
+  if (ckpt)  // checkpointing renders have debugMode 0
+    fn = nb <= 1   ? (const void*)k_trace8<false, true, 1, false>
+         : nb == 2 ? (const void*)k_trace8<false, true, 2, false>
+         : nb == 3 ? (const void*)k_trace8<false, true, 3, false>
+                   : (const void*)k_trace8<false, true, 4, false>;
+  else if (debug)
+    fn = nb <= 1   ? (const void*)k_trace8<false, false, 1, true>
+         : nb == 2 ? (const void*)k_trace8<false, false, 2, true>
+         : nb == 3 ? (const void*)k_trace8<false, false, 3, true>
+                   : (const void*)k_trace8<false, false, 4, true>;
   else
-    fn = nb <= 1 ? (const void*)k_trace8<false, false, 1>
-                 : nb == 2 ? (const void*)k_trace8<false, false, 2>
-                           : nb == 3 ? (const void*)k_trace8<false, false, 3> : (const void*)k_trace8<false, false, 4>;
+    fn = nb <= 1   ? (const void*)k_trace8<false, false, 1, false>
+         : nb == 2 ? (const void*)k_trace8<false, false, 2, false>
+         : nb == 3 ? (const void*)k_trace8<false, false, 3, false>
+                   : (const void*)k_trace8<false, false, 4, false>;
   const ViewDev* dv = d_views;
   const uint32_t* no_pix = nullptr;
   uint32_t zero = 0;
@@ -376,7 +389,7 @@ Err launch_trace_hits(const ViewDev& view, ViewDev* d_views, const uint32_t* pix
   GT_CUDA_TRY(cudaMemcpyAsync(d_views, &view, sizeof(ViewDev), cudaMemcpyHostToDevice, stream));
   HitOut ho{out_pidx, out_t, out_alpha, out_count, out_rounds, out_rgba, max_entries};
   uint32_t grid = std::min<uint32_t>((n_pix + kWarpsPerBlock - 1) / kWarpsPerBlock, 148u * 8u);
-  k_trace8<true, false, 1><<<grid, kWarpsPerBlock * 32, 0, stream>>>(d_views, 1, 0, counters, faces, pixels, n_pix, ho,
+  k_trace8<true, false, 1, true><<<grid, kWarpsPerBlock * 32, 0, stream>>>(d_views, 1, 0, counters, faces, pixels, n_pix, ho,
                                                                   Ckpt{});
   ++*launches;
   GT_CUDA_TRY(cudaGetLastError());
