@@ -80,13 +80,28 @@ __device__ __forceinline__ void node_test(const float4& f0, const float4& f1, co
 //     face with num >= tlo*dn + M or num <= thi*dn - M (dn < 0) has its t
 //     outside (tlo, thi); M = 3e-5 nmax (|o|_1 + 2) + 1e-6 (|tlo|+|thi|)|dn|
 //     is ~50x that error.
-template <bool CULL, class OnHit>
+// The bounding-sphere filter of proxy_test on its own: false only when the
+// ray certainly misses proxy j.
+__device__ __forceinline__ bool proxy_sphere(const FaceTable& F, const float4* w2o, uint32_t j, V3 o, V3 d) {
+  Affine W = load_affine(w2o + 3 * (size_t)j);
+  V3 oo = xpoint(W, o), od = xdir(W, d);
+  float l1o = fabsf(oo.x) + fabsf(oo.y) + fabsf(oo.z);
+  float dd = __fmaf_rn(od.x, od.x, __fmaf_rn(od.y, od.y, od.z * od.z));
+  float ox = __fmaf_rn(oo.x, od.x, __fmaf_rn(oo.y, od.y, oo.z * od.z));
+  float tc = -__fdividef(ox, dd);
+  float cx = __fmaf_rn(tc, od.x, oo.x), cy = __fmaf_rn(tc, od.y, oo.y), cz = __fmaf_rn(tc, od.z, oo.z);
+  float r2 = __fmaf_rn(cx, cx, __fmaf_rn(cy, cy, cz * cz));
+  float rp = __fmaf_rn(1e-5f, l1o, F.r_circ + 1e-3f);
+  return (r2 <= rp * rp) || !(dd == dd && r2 == r2);
+}
+
+template <bool CULL, class OnHit, bool SPHERE = true>
 __device__ __forceinline__ void proxy_test(const FaceTable& F, const float4* w2o, uint32_t j, V3 o, V3 d, float tlo,
                                            float thi, OnHit&& on_hit) {
   Affine W = load_affine(w2o + 3 * (size_t)j);
   V3 oo = xpoint(W, o), od = xdir(W, d);
   float l1o = fabsf(oo.x) + fabsf(oo.y) + fabsf(oo.z);
-  {
+  if (SPHERE) {
     float dd = __fmaf_rn(od.x, od.x, __fmaf_rn(od.y, od.y, od.z * od.z));
     float ox = __fmaf_rn(oo.x, od.x, __fmaf_rn(oo.y, od.y, oo.z * od.z));
     float tc = -__fdividef(ox, dd);

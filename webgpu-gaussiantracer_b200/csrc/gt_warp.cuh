@@ -5,8 +5,10 @@
 //     box-tested by the 32 lanes; hit inner children are sorted by entry
 //     distance (warp bitonic sort) and pushed far-to-near onto a per-warp
 //     stack in shared memory; hit leaves go to a per-warp leaf queue;
-//   * leaves: 32 queued proxies are tested at a time, one per lane, with the
-//     exact object-space test of the reference (gt_trace_common.cuh);
+//   * leaves: 32 queued proxies at a time go through the bounding-sphere
+//     filter, one per lane; those that pass wait in a second queue, and
+//     kSurvivors of them at a time get the exact object-space face tests of
+//     the reference (gt_trace_common.cuh), one per lane;
 //   * k-buffer: lane i holds the i-th closest hit (t, particle) found so far;
 //     a hit is inserted with one ballot and one shuffle.
 #pragma once
@@ -22,6 +24,7 @@ namespace gt {
 constexpr int kWarpsPerBlock = 4;
 constexpr int kLeafQueue = 96;   // leaf queue entries per warp (<= 63 in use)
 constexpr int kMaxHitsPerProxy = 6;
+constexpr int kSurvivors = 24;   // face-test batch of the two-phase leaf test
 constexpr uint32_t kFull = 0xFFFFFFFFu;
 
 struct WarpScratch {
@@ -29,6 +32,8 @@ struct WarpScratch {
   float st[kWarpStack];
   uint32_t leafq[kLeafQueue];
   float leaft[kLeafQueue];
+  uint32_t svj[64];  // proxies that passed the sphere filter, waiting for the face tests
+  float svt[64];     // (< kSurvivors + 32 in use)
   uint32_t pop[4];  // nodes taken by the current pop (lanes 8s..8s+7 test pop[s])
   float hq[kMaxHitsPerProxy][32];  // hits of each lane's proxy, column per lane
   RayStats stats;                  // the warp's work counters (lane 0 writes)
@@ -191,6 +196,7 @@ __device__ __forceinline__ void traverse8(const SceneDev& S, const FaceTable& F,
   const uint32_t lt_mask = (1u << lane) - 1u;
   const int cull = MODE == kClosestAny ? 0 : kbuf - 1;  // the entry that bounds the search
   int sp = 0, nq = 0;
+  int ns = 0;  // proxies that passed the sphere filter, waiting for the face tests
   if (lane == 0) {
     W.snode[0] = 0;
     W.st[0] = -CUDART_INF_F;
@@ -292,6 +298,111 @@ __device__ __forceinline__ void traverse8(const SceneDev& S, const FaceTable& F,
       __syncwarp();
     }
     const bool drain = sp == 0;
+    // kCollect tests leaves in two phases: the bounding-sphere filter on each
+    // batch of 32 queued leaves, then the face tests on batches of kSurvivors
+    // proxies that passed it.  The face tests then run with (nearly) every
+    // lane busy instead of the ~60 % the filter leaves: 4 % faster on the 1M
+    // view although the far bound tightens a little later (3 % more tests).
+    if (MODE == kCollect) {
+      if (nq >= leaf_batch || (drain && nq > 0)) {
+        const int nb = nq < 32 ? nq : 32;
+        uint32_t j = 0;
+        float lt = 0.f;
+        bool have = (int)lane < nb;
+        if (have) {
+          j = W.leafq[lane];
+          lt = W.leaft[lane];
+          have = lt <= thi;
+        }
+        __syncwarp();
+        if (nq > nb) {
+          uint32_t qj = 0;
+          float qt = 0.f;
+          bool mv = (int)lane < nq - nb;
+          if (mv) {
+            qj = W.leafq[nb + lane];
+            qt = W.leaft[nb + lane];
+          }
+          __syncwarp();
+          if (mv) {
+            W.leafq[lane] = qj;
+            W.leaft[lane] = qt;
+          }
+          __syncwarp();
+        }
+        nq -= nb;
+        const uint32_t tested = __ballot_sync(kFull, have);
+        if (lane == 0) st.proxy_tests += (unsigned)__popc(tested);
+        const bool surv = have && proxy_sphere(F, S.w2o, j, o, d);
+        const uint32_t sm = __ballot_sync(kFull, surv);
+        if (surv) {
+          const int r = ns + __popc(sm & lt_mask);
+          W.svj[r] = j;
+          W.svt[r] = lt;
+        }
+        ns += __popc(sm);
+        __syncwarp();
+      }
+      const bool all_queued = sp == 0 && nq == 0;
+      if (ns >= kSurvivors || (all_queued && ns > 0)) {
+        const int nb = ns < 32 ? ns : 32;
+        uint32_t j = 0;
+        bool have = (int)lane < nb;
+        if (have) {
+          j = W.svj[lane];
+          have = W.svt[lane] <= thi;
+        }
+        __syncwarp();
+        if (ns > nb) {
+          uint32_t qj = 0;
+          float qt = 0.f;
+          bool mv = (int)lane < ns - nb;
+          if (mv) {
+            qj = W.svj[nb + lane];
+            qt = W.svt[nb + lane];
+          }
+          __syncwarp();
+          if (mv) {
+            W.svj[lane] = qj;
+            W.svt[lane] = qt;
+          }
+          __syncwarp();
+        }
+        ns -= nb;
+        int nh = 0;
+        if (have) {
+          const float tb = fminf(next_up(thi), t_max);
+          auto on_hit = [&](float t, int) {
+            if (nh < kMaxHitsPerProxy) W.hq[nh][lane] = t;
+            ++nh;
+          };
+          proxy_test<true, decltype(on_hit)&, false>(F, S.w2o, j, o, d, tlo, tb, on_hit);
+          if (nh > kMaxHitsPerProxy) {
+            status |= kStatusHitOverflow;
+            nh = kMaxHitsPerProxy;
+          }
+        }
+        const uint32_t found = __reduce_add_sync(kFull, (uint32_t)nh);
+        if (lane == 0) st.anyhits += found;
+        if (found) {
+          __syncwarp();
+          const uint32_t p = nh ? __ldg(S.leaf_pidx + j) : 0u;
+          while (true) {
+            const uint32_t pend = __ballot_sync(kFull, nh > 0);
+            if (!pend) break;
+            const int src = __ffs(pend) - 1;
+            const int slot = __shfl_sync(kFull, nh, src) - 1;
+            const float t = W.hq[slot][src];
+            const uint32_t pp = __shfl_sync(kFull, p, src);
+            if ((int)lane == src) --nh;
+            kbuf_insert(kb, t, pp, lane);
+          }
+          thi = kbuf_t_at(kb, cull);
+        }
+      }
+      if (sp == 0 && nq == 0 && ns == 0) break;
+      continue;
+    }
     if (nq >= leaf_batch || (drain && nq > 0)) {
       const int nb = nq < 32 ? nq : 32;
       uint32_t j = 0;
