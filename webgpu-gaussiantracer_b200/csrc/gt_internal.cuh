@@ -19,7 +19,6 @@
 namespace gt {
 
 // ------------------------------------------------------------------ limits
-constexpr int kStackSize = 128;            // traversal stack entries per ray
 constexpr uint32_t kMaxDepth = 120;        // deepest BVH the build accepts
 constexpr uint32_t kInvalid = 0xFFFFFFFFu; // empty k-buffer slot (uint(-1))
 constexpr uint32_t kLeafBit = 0x80000000u; // child reference: leaf flag

@@ -12,13 +12,14 @@
 //     box-tested by the 32 lanes; hit inner children are sorted by entry
 //     distance (warp bitonic sort) and pushed far-to-near onto a per-warp
 //     stack in shared memory; hit leaves go to a per-warp leaf queue;
-//   * leaves: 32 queued proxies are tested at a time, one per lane, with the
-//     exact object-space test of the reference (gt_trace_common.cuh);
-//   * k-buffer: lane i holds the i-th closest hit (t, particle) found so far;
-//     a hit is inserted with one ballot and one shuffle.  The buffer keeps the
-//     32 closest hits beyond t_curr, so a traversal can feed several rounds
-//     of k <= 16: a round's set (the k smallest hits with t > t_curr) is
-//     certain whenever it lies inside the buffer or the buffer is not full;
+//   * leaves: queued proxies go through the bounding-sphere filter 32 at a
+//     time, and those that pass through the exact object-space face tests of
+//     the reference (gt_trace_common.cuh) 24 at a time, one per lane;
+//   * k-buffer: entry 32 j + i (j < NB slots) lives in lane i; a hit is
+//     inserted with one ballot and shuffles.  A traversal keeps the kbuf
+//     (64 by default, up to 128) closest hits beyond t_curr and feeds several
+//     rounds: a round's set (the k smallest hits with t > t_curr) is certain
+//     whenever it lies inside the first kbuf entries or the buffer is not full;
 //   * compositing: lanes evaluate the response and SH colour of one entry
 //     each; the front-to-back accumulation then runs in entry order on
 //     broadcast values, so the float operations are those of the reference

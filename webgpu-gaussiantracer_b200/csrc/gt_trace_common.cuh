@@ -46,23 +46,6 @@ __device__ __forceinline__ BoxRay make_boxray(V3 o, V3 d, float scene_mag) {
   return b;
 }
 
-// Slab test of the two children of a node against [tlo, thi].
-__device__ __forceinline__ void node_test(const float4& f0, const float4& f1, const float4& f2, const BoxRay& r,
-                                          float tlo, float thi, float& n0, float& n1, bool& h0, bool& h1) {
-  float ax = __fmaf_rn(f0.x, r.ix, -r.ox), bx = __fmaf_rn(f0.y, r.ix, -r.ox);
-  float ay = __fmaf_rn(f0.z, r.iy, -r.oy), by = __fmaf_rn(f0.w, r.iy, -r.oy);
-  float az = __fmaf_rn(f2.x, r.iz, -r.oz), bz = __fmaf_rn(f2.y, r.iz, -r.oz);
-  n0 = fmaxf(fmaxf(fminf(ax, bx) - r.px, fminf(ay, by) - r.py), fmaxf(fminf(az, bz) - r.pz, tlo));
-  float x0 = fminf(fminf(fmaxf(ax, bx) + r.px, fmaxf(ay, by) + r.py), fminf(fmaxf(az, bz) + r.pz, thi));
-  h0 = n0 <= x0;
-  float cx = __fmaf_rn(f1.x, r.ix, -r.ox), dx = __fmaf_rn(f1.y, r.ix, -r.ox);
-  float cy = __fmaf_rn(f1.z, r.iy, -r.oy), dy = __fmaf_rn(f1.w, r.iy, -r.oy);
-  float cz = __fmaf_rn(f2.z, r.iz, -r.oz), dz = __fmaf_rn(f2.w, r.iz, -r.oz);
-  n1 = fmaxf(fmaxf(fminf(cx, dx) - r.px, fminf(cy, dy) - r.py), fmaxf(fminf(cz, dz) - r.pz, tlo));
-  float x1 = fminf(fminf(fmaxf(cx, dx) + r.px, fmaxf(cy, dy) + r.py), fminf(fmaxf(cz, dz) + r.pz, thi));
-  h1 = n1 <= x1;
-}
-
 // Ray/proxy test.  Calls on_hit(t, face) for every face hit by the reference
 // triangle test with t in (tlo, thi) that is front-facing (CULL) or any
 // (!CULL).  Three exact filters run before that test; each skips only work

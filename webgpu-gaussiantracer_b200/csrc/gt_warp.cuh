@@ -51,25 +51,6 @@ struct HitOut {
   uint32_t max_entries;
 };
 
-// Warp bitonic sort of (key, val), ascending by key over the 32 lanes.
-__device__ __forceinline__ void warp_sort(float& key, uint32_t& val, uint32_t lane) {
-#pragma unroll
-  for (int k = 2; k <= 32; k <<= 1) {
-#pragma unroll
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      float ok = __shfl_xor_sync(kFull, key, j);
-      uint32_t ov = __shfl_xor_sync(kFull, val, j);
-      bool up = (lane & k) == 0;
-      bool lower = (lane & j) == 0;
-      bool take = (lower == up) ? (ok < key) : (ok > key);
-      if (take) {
-        key = ok;
-        val = ov;
-      }
-    }
-  }
-}
-
 // Sorts lanes [0, w) ascending by key, w = the power of two >= m (m <= 32);
 // keys of lanes >= m are +inf.
 __device__ __forceinline__ void warp_sort_prefix(float& key, uint32_t& val, uint32_t lane, int m) {
