@@ -49,3 +49,17 @@ def test_limit_arguments_checked(ctx):
     assert ctx._lib.gt_set_limits(ctx.handle, 0, 257, 0) == L.GT_ERR_INVALID_ARG
     assert ctx._lib.gt_set_limits(ctx.handle, 0, 0, (1 << 22) + 1) == L.GT_ERR_INVALID_ARG
     assert ctx._lib.gt_set_limits(ctx.handle, 0, 0, 0) == L.GT_OK
+
+
+def test_out_of_memory_is_an_error_not_a_fault(ctx):
+    """A device allocation larger than the GPU returns GT_ERR_OOM (cudaMalloc
+    fails cleanly), and the context keeps working."""
+    p = L.C.c_void_p()
+    st = ctx._lib.gt_device_alloc(ctx.handle, 1 << 50, L.C.byref(p))
+    assert st == L.GT_ERR_OOM and not p.value
+    assert "memory" in L.last_error(ctx.handle).lower()
+    pg = small_scene(n=500, seed=52)
+    scene = Scene(ctx, pg.gaussiansBuffer, 0.01)
+    v = view(16, 16, k=4)
+    ctx.render(scene, v.uniforms, v.width, v.height)
+    scene.close()

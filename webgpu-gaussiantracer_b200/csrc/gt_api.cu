@@ -23,6 +23,9 @@ thread_local std::string g_last_error;  // errors without a context
 
 // ----------------------------------------------------------------- helpers
 static gt_status fail(gt_context* ctx, gt_status code, const std::string& msg) {
+  // a failed runtime call also stays behind as the thread's last error; read
+  // it here so that the next launch check does not report it a second time
+  (void)cudaGetLastError();
   if (ctx)
     ctx->err = msg;
   else
@@ -31,12 +34,16 @@ static gt_status fail(gt_context* ctx, gt_status code, const std::string& msg) {
 }
 static gt_status fail(gt_context* ctx, const Err& e) { return fail(ctx, e.code, e.msg); }
 
+// A failing runtime call also leaves its error as the thread's last error;
+// it is read back here so that a later launch check does not report it again.
 #define API_CUDA(ctx, expr)                                                                        \
   do {                                                                                             \
     cudaError_t e_ = (expr);                                                                       \
-    if (e_ != cudaSuccess)                                                                         \
+    if (e_ != cudaSuccess) {                                                                       \
+      (void)cudaGetLastError();                                                                    \
       return fail(ctx, e_ == cudaErrorMemoryAllocation ? GT_ERR_OOM : GT_ERR_CUDA,                 \
                   std::string(#expr) + ": " + cudaGetErrorString(e_));                             \
+    }                                                                                              \
   } while (0)
 
 static gt_status status_to_error(gt_context* ctx, uint32_t status) {

@@ -147,6 +147,7 @@ struct Err {
   do {                                                                            \
     cudaError_t e_ = (expr);                                                      \
     if (e_ != cudaSuccess) {                                                      \
+      (void)cudaGetLastError(); /* clear it: the caller reports it once */        \
       return ::gt::Err{e_ == cudaErrorMemoryAllocation ? GT_ERR_OOM : GT_ERR_CUDA, \
                        std::string(#expr) + ": " + cudaGetErrorString(e_)};        \
     }                                                                             \
