@@ -3,6 +3,8 @@
 The tracer and the oracle follow the same binary32 operation order, so
 images, hit sequences, hit t values and alphas must match bit for bit.  The
 oracle's double build gives the FP64 error statistics."""
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -10,7 +12,7 @@ from conftest import small_scene, view
 from oracle import oracle
 from gtrace import synth
 from gtrace import _lib as L
-from gtrace.tracer import Scene
+from gtrace.tracer import Scene, _uniforms
 from gtrace.uniforms import with_fields
 
 pytestmark = pytest.mark.gpu
@@ -164,6 +166,17 @@ def test_invalid_arguments(ctx):
     with pytest.raises(L.GTraceError) as e:
         Scene(ctx, pg.gaussiansBuffer, 1.5)
     assert e.value.status == L.GT_ERR_INVALID_ARG
+    # at most 2^31 pixels, and at most 2^31 work slots once the 8x4 tile grid
+    # is padded to 16x16-tile blocks (a 2^31 x 1 image has 2^31 pixels but
+    # 2^37 slots); both are rejected before anything is launched
+    u = _uniforms(v.uniforms)
+    dev = ctx.device_alloc(64)
+    try:
+        for w, h in [(1 << 31, 1), (1 << 28, 8), (65544, 32760)]:
+            assert ctx._lib.gt_render(ctx.handle, g.handle, C.byref(u), w, h, C.c_void_p(dev),
+                                      L.GT_FLAG_OUTPUT_DEVICE, None) == L.GT_ERR_INVALID_ARG
+    finally:
+        ctx.device_free(dev)
 
 
 def test_device_output_and_async(ctx):

@@ -129,8 +129,9 @@ static ViewDev make_view(const gt_scene* s, const gt_uniforms& u, uint32_t w, ui
   v.out = out;
   v.w = w;
   v.h = h;
-  v.tiles_x = (w + 7) / 8;
-  v.n_tiles = v.tiles_x * ((h + 3) / 4);
+  // the tile grid in whole blocks of 16 x 16 tiles (see tile_pixel)
+  v.tiles_x = ((w + 7) / 8 + 15) / 16 * 16;
+  v.n_tiles = v.tiles_x * (((h + 3) / 4 + 15) / 16 * 16);
   v.tile_begin = tile_begin;
   v.n_particles = s->n;
   v.kbuf = 32;
@@ -408,7 +409,8 @@ extern "C" gt_status gt_render(gt_context* ctx, const gt_scene* scene, const gt_
   gt_status st = check_uniforms(ctx, u);
   if (st != GT_OK) return st;
   if (!out_rgba) return fail(ctx, GT_ERR_INVALID_ARG, "out_rgba is NULL");
-  if (w == 0 || h == 0 || (uint64_t)w * h > (1ull << 31)) return fail(ctx, GT_ERR_INVALID_ARG, "bad image size");
+  if (w == 0 || h == 0 || (uint64_t)w * h > (1ull << 31) || view_slots(w, h) > kMaxSlots)
+    return fail(ctx, GT_ERR_INVALID_ARG, "bad image size");
   if ((flags & GT_FLAG_ASYNC) && !(flags & GT_FLAG_OUTPUT_DEVICE))
     return fail(ctx, GT_ERR_INVALID_ARG, "GT_FLAG_ASYNC needs a device output buffer");
   if ((flags & GT_FLAG_OUTPUT_DEVICE) && ((uintptr_t)out_rgba % 16) != 0)
@@ -467,7 +469,8 @@ extern "C" gt_status gt_render_hits(gt_context* ctx, const gt_scene* scene, cons
   if (!scene || scene->ctx != ctx) return fail(ctx, GT_ERR_INVALID_ARG, "scene is NULL or from another context");
   gt_status st = check_uniforms(ctx, u);
   if (st != GT_OK) return st;
-  if (w == 0 || h == 0 || (uint64_t)w * h > (1ull << 31)) return fail(ctx, GT_ERR_INVALID_ARG, "bad image size");
+  if (w == 0 || h == 0 || (uint64_t)w * h > (1ull << 31) || view_slots(w, h) > kMaxSlots)
+    return fail(ctx, GT_ERR_INVALID_ARG, "bad image size");
   if (n_pix == 0) return GT_OK;
   if (!pixels || !out_count || !out_rounds || (max_entries > 0 && (!out_pidx || !out_t || !out_alpha)))
     return fail(ctx, GT_ERR_INVALID_ARG, "NULL output buffer");
@@ -544,6 +547,7 @@ extern "C" gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items
     return fail(ctx, GT_ERR_INVALID_ARG, "GT_FLAG_ANTIALIAS renders are not checkpointed");
   API_CUDA(ctx, cudaSetDevice(ctx->device));
   size_t staging = 0;
+  uint64_t slots_all = 0;
   uint32_t kmax = 8, total_tiles = 0;
   for (uint32_t i = 0; i < count; ++i) {
     const gt_batch_item& it = items[i];
@@ -552,6 +556,8 @@ extern "C" gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items
     if (st != GT_OK) return st;
     if (!it.out_rgba || it.w == 0 || it.h == 0 || (uint64_t)it.w * it.h > (1ull << 31))
       return fail(ctx, GT_ERR_INVALID_ARG, "batch item image invalid");
+    slots_all += view_slots(it.w, it.h);
+    if (slots_all > kMaxSlots) return fail(ctx, GT_ERR_INVALID_ARG, "batch larger than 2^31 work slots");
     if ((flags & GT_FLAG_OUTPUT_DEVICE) && ((uintptr_t)it.out_rgba % 16) != 0)
       return fail(ctx, GT_ERR_INVALID_ARG, "device out_rgba must be 16-byte aligned");
     staging += (size_t)it.w * it.h;
@@ -685,7 +691,8 @@ extern "C" gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const g
   if (!scene || scene->ctx != ctx) return fail(ctx, GT_ERR_INVALID_ARG, "scene is NULL or from another context");
   gt_status st = check_uniforms(ctx, u);
   if (st != GT_OK) return st;
-  if (w == 0 || h == 0) return fail(ctx, GT_ERR_INVALID_ARG, "bad image size");
+  if (w == 0 || h == 0 || (uint64_t)w * h > (1ull << 31) || view_slots(w, h) > kMaxSlots)
+    return fail(ctx, GT_ERR_INVALID_ARG, "bad image size");
   API_CUDA(ctx, cudaSetDevice(ctx->device));
   size_t bytes = (size_t)w * h * sizeof(float4);
   st = ensure_staging(ctx, bytes);

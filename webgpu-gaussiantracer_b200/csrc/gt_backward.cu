@@ -209,9 +209,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewD
     uint32_t tile = item >> 5, sl = item & 31u;
     const uint32_t vi = n_views == 1 ? 0u : find_view(views, n_views, tile);
     const ViewDev& V = views[vi];
-    uint32_t lt = tile - V.tile_begin;
-    uint32_t px = (lt % V.tiles_x) * kTileW + (sl % kTileW);
-    uint32_t py = (lt / V.tiles_x) * kTileH + (sl / kTileW);
+    uint32_t px, py;
+    tile_pixel(V.tiles_x, tile - V.tile_begin, sl, px, py);
     if (px >= V.w || py >= V.h) continue;
     uint32_t rec = ck.head[item];
     if (rec == kInvalid) continue;
@@ -630,7 +629,8 @@ gt_status check_bwd_view(gt_context* ctx, const gt_scene* s, const gt_uniforms* 
   if (!dL) return api_fail(ctx, GT_ERR_INVALID_ARG, "dL_drgba is NULL");
   if ((flags & GT_FLAG_INPUT_DEVICE) && ((uintptr_t)dL % 16) != 0)  // read as float4
     return api_fail(ctx, GT_ERR_INVALID_ARG, "device dL_drgba must be 16-byte aligned");
-  if (w == 0 || h == 0 || (uint64_t)w * h > (1ull << 31)) return api_fail(ctx, GT_ERR_INVALID_ARG, "bad image size");
+  if (w == 0 || h == 0 || (uint64_t)w * h > (1ull << 31) || view_slots(w, h) > kMaxSlots)
+    return api_fail(ctx, GT_ERR_INVALID_ARG, "bad image size");
   return GT_OK;
 }
 
@@ -656,10 +656,13 @@ extern "C" gt_status gt_backward_batch(gt_context* ctx, const gt_batch_item* ite
   if (!items || !scenes || !dL_dparams || n_scenes == 0) return api_fail(ctx, GT_ERR_INVALID_ARG, "NULL argument");
   if (flags & GT_FLAG_ASYNC) return api_fail(ctx, GT_ERR_INVALID_ARG, "gt_backward_batch is synchronous");
   std::vector<BwdView> v(count);
+  uint64_t slots_all = 0;
   for (uint32_t i = 0; i < count; ++i) {
     gt_status st =
         check_bwd_view(ctx, items[i].scene, &items[i].u, items[i].w, items[i].h, items[i].dL_drgba, flags);
     if (st != GT_OK) return st;
+    slots_all += view_slots(items[i].w, items[i].h);
+    if (slots_all > kMaxSlots) return api_fail(ctx, GT_ERR_INVALID_ARG, "batch larger than 2^31 work slots");
     uint32_t s = 0;
     while (s < n_scenes && scenes[s] != items[i].scene) ++s;
     if (s == n_scenes) return api_fail(ctx, GT_ERR_INVALID_ARG, "a batch item's scene is not in `scenes`");

@@ -138,6 +138,16 @@ struct LaunchShape {
 };
 
 // ----------------------------------------------------------- host helpers
+// Work slots of a w x h view: 32 per 8 x 4 tile of its tile grid, padded to
+// whole blocks of 16 x 16 tiles (see tile_pixel).  A launch takes at most
+// kMaxSlots of them (its 32-bit work counter counts past the total).
+inline uint64_t view_slots(uint32_t w, uint32_t h) {
+  const uint64_t tx = (((uint64_t)w + 7) / 8 + 15) / 16 * 16;
+  const uint64_t ty = (((uint64_t)h + 3) / 4 + 15) / 16 * 16;
+  return tx * ty * 32;
+}
+constexpr uint64_t kMaxSlots = 1ull << 31;
+
 struct Err {
   gt_status code = GT_OK;
   std::string msg;

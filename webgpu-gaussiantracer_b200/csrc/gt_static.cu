@@ -69,6 +69,7 @@ extern "C" gt_status gt_render_batch_noalloc(gt_context* ctx, const gt_batch_ite
                     "gt_render_batch_noalloc needs device output buffers (GT_FLAG_OUTPUT_DEVICE): host outputs "
                     "would need a staging allocation");
   uint32_t total_tiles = 0;
+  uint64_t slots_all = 0;
   ViewDev views[kNoallocMaxViews];
   for (uint32_t i = 0; i < count; ++i) {
     const gt_batch_item& it = items[i];
@@ -77,6 +78,8 @@ extern "C" gt_status gt_render_batch_noalloc(gt_context* ctx, const gt_batch_ite
     if (st != GT_OK) return st;
     if (!it.out_rgba || it.w == 0 || it.h == 0 || (uint64_t)it.w * it.h > (1ull << 31))
       return api_fail(ctx, GT_ERR_INVALID_ARG, "batch item image invalid");
+    slots_all += view_slots(it.w, it.h);
+    if (slots_all > kMaxSlots) return api_fail(ctx, GT_ERR_INVALID_ARG, "batch larger than 2^31 work slots");
     if (((uintptr_t)it.out_rgba % 16) != 0)
       return api_fail(ctx, GT_ERR_INVALID_ARG, "device out_rgba must be 16-byte aligned");
     views[i] = api_make_view(it.scene, it.u, it.w, it.h, reinterpret_cast<float4*>(it.out_rgba), total_tiles);

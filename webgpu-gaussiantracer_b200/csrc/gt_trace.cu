@@ -290,9 +290,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) k_trace8(const ViewDev
       uint32_t tile = item >> 5, s = item & 31u;
       vi = n_views == 1 ? 0u : find_view(views, n_views, tile);
       const ViewDev& V = views[vi];
-      uint32_t lt = tile - V.tile_begin;
-      px = (lt % V.tiles_x) * kTileW + (s % kTileW);
-      py = (lt / V.tiles_x) * kTileH + (s / kTileW);
+      tile_pixel(V.tiles_x, tile - V.tile_begin, s, px, py);
       if (px >= V.w || py >= V.h) continue;
     }
     // the output position waits in shared memory as well
