@@ -373,14 +373,24 @@ gt_status gt_l2_loss(gt_context* ctx, const float* rgba, const float* target, ui
 /* ============================================================ tuning
  * No counterpart in the reference.  Times the tracer's launch shapes on the
  * given view and caches the fastest per (GPU, scene-size bucket, image-size
- * bucket, k).  gt_render and gt_render_batch use the cached choice. */
+ * bucket, k).  gt_render and gt_render_batch use the cached choice.
+ * Two kernels render the plain image (debugMode 0), with identical results:
+ *   block_threads 32:  a warp traces the 32 rays of an 8x4 tile together
+ *                      (the default); kbuf = k-buffer entries per ray
+ *                      (k..64, default 32); blocks_per_sm and leaf_batch
+ *                      are not used (the grid fills the SMs);
+ *   block_threads 128: a warp traces one ray; kbuf = k-buffer entries of a
+ *                      traversal (k..128, default 64), blocks_per_sm and
+ *                      leaf_batch as below.
+ * Debug modes, hit recording and the checkpointing forward of gt_backward
+ * always use the second kernel. */
 typedef struct gt_tune_result {
-  uint32_t block_threads; /* threads per block                                  */
+  uint32_t block_threads; /* 32: a warp per 8x4 tile; 128: a warp per ray      */
   uint32_t blocks_per_sm; /* resident blocks per SM of the persistent grid      */
   uint32_t tile_w, tile_h;/* pixel tile a warp takes per work-stealing step     */
   float best_ms;          /* fastest trace time measured                        */
   float default_ms;       /* trace time of the default launch shape             */
-  uint32_t kbuf;          /* k-buffer size of a traversal (k..128; raised to k) */
+  uint32_t kbuf;          /* k-buffer entries (see above; raised to k)          */
   uint32_t leaf_batch;    /* queued leaves that start a batch of proxy tests    */
 } gt_tune_result;
 
@@ -388,8 +398,9 @@ gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const gt_uniforms*
                       uint32_t w, uint32_t h, gt_tune_result* result);
 /* Installs a launch shape for the bucket of (scene, u->k, w x h) without
  * timing anything (for example one found by gt_autotune in an earlier run).
- * block_threads must be 128 and the tile 8 x 4; blocks_per_sm 1..32,
- * kbuf 1..128 and leaf_batch 1..32.  best_ms/default_ms are ignored. */
+ * block_threads must be 32 or 128 and the tile 8 x 4; blocks_per_sm 1..32,
+ * kbuf 1..128 (used up to 64 with block_threads 32) and leaf_batch 1..32.
+ * best_ms/default_ms are ignored. */
 gt_status gt_set_tune(gt_context* ctx, const gt_scene* scene, const gt_uniforms* u, uint32_t w,
                       uint32_t h, const gt_tune_result* shape);
 /* Drops every cached tuning result of the context. */

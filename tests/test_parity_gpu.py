@@ -233,7 +233,8 @@ def test_autotune_keeps_results(ctx):
     v = view(64, 64, k=6)
     before = ctx.render(g, v.uniforms, 64, 64)
     r = ctx.autotune(g, v.uniforms, 64, 64)
-    assert r["blocks_per_sm"] >= 1 and r["best_ms"] > 0
+    assert r["blocks_per_sm"] >= 1 and r["best_ms"] > 0 and r["block_threads"] in (32, 128)
+    assert r["kbuf"] >= 6 and (r["block_threads"] == 128 or r["kbuf"] <= 64)
     after = ctx.render(g, v.uniforms, 64, 64)
     np.testing.assert_array_equal(before, after)
 
@@ -253,6 +254,26 @@ def test_tuned_shapes_are_bit_exact(ctx, k):
         np.testing.assert_array_equal(ctx.render(g, v.uniforms, w, h), ref, err_msg=f"kbuf={kbuf} lb={lb}")
     with pytest.raises(RuntimeError):
         ctx.set_tune(g, v.uniforms, w, h, kbuf=129)
+    ctx._lib.gt_autotune_reset(ctx._h)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("k", [1, 7, 16, 32])
+def test_both_kernels_and_packet_kbufs_are_bit_exact(ctx, k):
+    """The tile-packet kernel (block_threads 32) at every k-buffer size and
+    the warp-per-ray kernel (128) give the oracle's image, bit for bit."""
+    pg = small_scene(n=3000, seed=33)
+    g, o = _both(ctx, pg.gaussiansBuffer, 0.01)
+    w, h = 45, 37
+    v = view(w, h, k=k)
+    ref, _ = o.render(v.uniforms, w, h)
+    for bt, kbuf in [(32, k), (32, 24), (32, 32), (32, 40), (32, 48), (32, 64), (32, 100), (128, 64)]:
+        ctx.set_tune(g, v.uniforms, w, h, kbuf=kbuf, block_threads=bt)
+        img = ctx.render(g, v.uniforms, w, h)
+        np.testing.assert_array_equal(img.reshape(-1, 4).view(np.uint32), ref.view(np.uint32),
+                                      err_msg=f"block_threads={bt} kbuf={kbuf}")
+    with pytest.raises(RuntimeError):
+        ctx.set_tune(g, v.uniforms, w, h, block_threads=64)
     ctx._lib.gt_autotune_reset(ctx._h)
 
 

@@ -172,8 +172,13 @@ static LaunchShape shape_for(gt_context* ctx, const gt_scene* s, uint32_t w, uin
   LaunchShape sh;
   auto it = ctx->tune.find(tune_key(s, w, h, k));
   if (it != ctx->tune.end()) {
+    // block_threads 32: tile packets with this k-buffer; 128: a warp per ray
+    sh.packet = it->second.block_threads == 32 ? 1u : 0u;
+    if (sh.packet)
+      sh.packet_kbuf = it->second.kbuf;
+    else
+      sh.kbuf = it->second.kbuf;
     sh.blocks_per_sm = it->second.blocks_per_sm;
-    sh.kbuf = it->second.kbuf;
     sh.leaf_batch = it->second.leaf_batch;
   }
   return sh;
@@ -627,15 +632,16 @@ extern "C" gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items
   LaunchShape shape = shape_for(ctx, items[0].scene, items[0].w, items[0].h, items[0].u.k);
   // the view table is rebuilt on every call: it takes the shape's k-buffer
   // size and leaf batch here, and the graph's kernel matches its slot count
-  apply_shape(ctx->h_views, count, shape);
+  const bool packet = packet_launch(ctx->h_views, count, shape, false);
+  apply_shape(ctx->h_views, count, shape, packet);
   uint32_t kb_max = 1;
   bool any_debug = false;  // the graph's kernel is the debug-mode instantiation
   for (uint32_t q = 0; q < count; ++q) {
     kb_max = std::max(kb_max, ctx->h_views[q].kbuf);
     any_debug = any_debug || ctx->h_views[q].u.debug != 0;
   }
-  auto key = std::make_tuple(count, total_tiles, kmax | (any_debug ? 0x10000u : 0u), shape.blocks_per_sm,
-                             (kb_max + 31u) / 32u);
+  auto key = std::make_tuple(count, total_tiles, kmax | (any_debug ? 0x10000u : 0u) | (packet ? 0x20000u : 0u),
+                             shape.blocks_per_sm, packet ? kb_max : (kb_max + 31u) / 32u);
   auto it = ctx->graphs.find(key);
   if (it == ctx->graphs.end()) {
     GraphEntry g;
@@ -718,50 +724,73 @@ extern "C" gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const g
     *out_ms = ms_min;
     return GT_OK;
   };
-  // 1. resident blocks per SM at the default traversal settings
+  // 1. tile packets (the default kernel): k-buffer entries per ray
+  const uint32_t k = u->k;
   LaunchShape best_sh;
   float best = 1e30f, def = 0.0f;
-  const uint32_t cands[] = {1, 2, 3, 4, 6, 8, 12, 16};
-  for (uint32_t b : cands) {
+  const uint32_t pkbufs[] = {k, 24u, 32u, 48u, 64u};
+  for (int i = 0; i < 5; ++i) {
+    const uint32_t kb = pkbufs[i];
+    if (kb < k || (i > 0 && kb == k)) continue;  // below k, or already timed as k
     LaunchShape sh;
-    sh.blocks_per_sm = b;
+    sh.packet = 1;
+    sh.packet_kbuf = std::min(kMaxPacketKbuf, kb);
     float ms = 0.0f;
     st = time_shape(sh, 3, &ms);
     if (st != GT_OK) return st;
-    if (b == LaunchShape().blocks_per_sm) def = ms;
+    if (sh.packet_kbuf == std::max(k, LaunchShape().packet_kbuf)) def = ms;
     if (ms < best) {
       best = ms;
       best_sh = sh;
     }
   }
-  // 2. k-buffer size and leaf batch at that occupancy
-  const uint32_t k = u->k;
+  // 2. a warp per ray: resident blocks per SM, then k-buffer size and leaf batch
+  LaunchShape warp_sh;
+  warp_sh.packet = 0;
+  float warp_best = 1e30f;
+  const uint32_t cands[] = {1, 2, 3, 4, 6, 8, 12, 16};
+  for (uint32_t b : cands) {
+    LaunchShape sh = warp_sh;
+    sh.blocks_per_sm = b;
+    float ms = 0.0f;
+    st = time_shape(sh, 3, &ms);
+    if (st != GT_OK) return st;
+    if (ms < warp_best) {
+      warp_best = ms;
+      warp_sh = sh;
+    }
+  }
   const uint32_t kbufs[] = {k, 32u, 64u, 96u, 128u};
   const uint32_t batches[] = {8u, 16u, 24u, 32u};
+  const LaunchShape occ_sh = warp_sh;
   for (uint32_t kb : kbufs) {
     for (uint32_t lb : batches) {
-      LaunchShape sh = best_sh;
+      LaunchShape sh = occ_sh;
       sh.kbuf = std::min(kMaxKbuf, kb);
       sh.leaf_batch = lb;
-      if (sh.kbuf == best_sh.kbuf && sh.leaf_batch == best_sh.leaf_batch) continue;
+      if (sh.kbuf == occ_sh.kbuf && sh.leaf_batch == occ_sh.leaf_batch) continue;
       float ms = 0.0f;
       st = time_shape(sh, 2, &ms);
       if (st != GT_OK) return st;
-      if (ms < best) {
-        best = ms;
-        best_sh = sh;
+      if (ms < warp_best) {
+        warp_best = ms;
+        warp_sh = sh;
       }
     }
   }
+  if (warp_best < best) {
+    best = warp_best;
+    best_sh = warp_sh;
+  }
   gt_tune_result r;
   memset(&r, 0, sizeof r);
-  r.block_threads = 128;
+  r.block_threads = best_sh.packet ? 32u : 128u;
   r.blocks_per_sm = best_sh.blocks_per_sm;
   r.tile_w = 8;
   r.tile_h = 4;
   r.best_ms = best;
   r.default_ms = def;
-  r.kbuf = std::max(best_sh.kbuf, k);
+  r.kbuf = std::max(best_sh.packet ? best_sh.packet_kbuf : best_sh.kbuf, k);
   r.leaf_batch = best_sh.leaf_batch;
   ctx->tune[tune_key(scene, w, h, k)] = r;
   if (result) *result = r;
@@ -775,8 +804,8 @@ extern "C" gt_status gt_set_tune(gt_context* ctx, const gt_scene* scene, const g
   gt_status st = check_uniforms(ctx, u);
   if (st != GT_OK) return st;
   if (!shape) return fail(ctx, GT_ERR_INVALID_ARG, "shape is NULL");
-  if (shape->block_threads != 128 || shape->tile_w != 8 || shape->tile_h != 4)
-    return fail(ctx, GT_ERR_INVALID_ARG, "block_threads must be 128 and the tile 8 x 4");
+  if ((shape->block_threads != 32 && shape->block_threads != 128) || shape->tile_w != 8 || shape->tile_h != 4)
+    return fail(ctx, GT_ERR_INVALID_ARG, "block_threads must be 32 or 128 and the tile 8 x 4");
   if (shape->blocks_per_sm < 1 || shape->blocks_per_sm > 32 || shape->kbuf < 1 || shape->kbuf > kMaxKbuf ||
       shape->leaf_batch < 1 || shape->leaf_batch > 32)
     return fail(ctx, GT_ERR_INVALID_ARG, "blocks_per_sm and leaf_batch must lie in 1..32, kbuf in 1..128");

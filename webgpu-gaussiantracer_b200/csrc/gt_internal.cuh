@@ -135,7 +135,13 @@ struct LaunchShape {
   uint32_t tile_w = 8, tile_h = 4;  // pixel tile of the work order (tile_w*tile_h == 32)
   uint32_t kbuf = 64;               // k-buffer entries (raised to k when k is larger; <= kMaxKbuf)
   uint32_t leaf_batch = 32;         // leaf queue size that triggers proxy tests
+  // Plain renders (debugMode 0, no checkpoint) run one warp per 8x4 tile of
+  // rays (gt_packet.cu) unless packet is 0; their k-buffer has packet_kbuf
+  // entries per ray (raised to k; <= kMaxPacketKbuf).
+  uint32_t packet = 1;
+  uint32_t packet_kbuf = 32;
 };
+constexpr uint32_t kMaxPacketKbuf = 64;
 
 // ----------------------------------------------------------- host helpers
 // Work slots of a w x h view: 32 per 8 x 4 tile of its tile grid, padded to
@@ -216,10 +222,16 @@ constexpr uint32_t kCkptHeader = 4;
 
 // Trace launches (gt_trace.cu).  launch_trace writes the shape's k-buffer
 // size and leaf batch into the host view table before uploading it.
-void apply_shape(ViewDev* views, uint32_t n_views, const LaunchShape& shape);
+// Whether launch_trace renders these views with the tile-packet kernel.
+bool packet_launch(const ViewDev* views, uint32_t n_views, const LaunchShape& shape, bool ckpt);
+// Sets each view's k-buffer size and leaf batch for a launch of either kernel.
+void apply_shape(ViewDev* views, uint32_t n_views, const LaunchShape& shape, bool packet = false);
 Err launch_trace(ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
                  const FaceTable& faces, const LaunchShape& shape, int num_sms, cudaStream_t stream,
                  uint64_t* launches, ViewDev* d_views_scratch, const Ckpt* ckpt = nullptr);
+Err launch_trace_packet(const ViewDev* views, const ViewDev* d_views, uint32_t n_views, uint32_t total_tiles,
+                        DevCounters* counters, const FaceTable& faces, int num_sms, cudaStream_t stream,
+                        uint64_t* launches);
 Err launch_trace_hits(const ViewDev& view, ViewDev* d_views, const uint32_t* pixels, uint32_t n_pix,
                       uint32_t max_entries, uint32_t* out_pidx, float* out_t, float* out_alpha, uint32_t* out_count,
                       uint32_t* out_rounds, float4* out_rgba, DevCounters* counters, const FaceTable& faces,

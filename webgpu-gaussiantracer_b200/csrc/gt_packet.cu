@@ -1,0 +1,463 @@
+// gt_packet.cu — forward tracer, one warp per 8x4 pixel tile (a packet of 32
+// primary rays, one per lane), over the 8-wide BVH.
+//
+// Same output as k_trace8 (gt_trace.cu) bit for bit: the same per-round hit
+// sets, the same compositing arithmetic in the same order.  What differs is
+// how the work is shared out:
+//   * traversal: the warp walks the hierarchy once for all its rays.  A node
+//     is popped when its entry distance (the smallest over the rays that hit
+//     its box) is within the largest far bound of the packet; each lane tests
+//     its own ray against the node's children; an inner child hit by any ray
+//     is pushed (near-first by that entry distance).  Primary rays of one
+//     tile are so coherent that the packet visits only ~1.13x the nodes of
+//     one of its rays, so a node visit serves ~28 rays.  The node's 256 bytes
+//     come in one coalesced load into shared memory, issued for the top of
+//     the stack as soon as it is known so that it overlaps the leaf work;
+//   * leaves: a leaf hit by ray r becomes a (proxy, ray) pair; pairs go 32 at
+//     a time through the bounding-sphere filter and those that pass 24 at a
+//     time through the exact face tests, one pair per lane.  Pairs are made
+//     from a visit's hit leaves only while fewer than 32 wait, which keeps
+//     the queue (and the shared memory of a warp) small: warps per SM are
+//     bounded by shared memory, and more of them hide more latency;
+//   * k-buffer: each ray keeps the kbuf smallest (t, particle) hits in a
+//     max-heap of its own (a column of a shared-memory array of 64-bit keys
+//     that order like (t, particle)); its root is the ray's far bound.  Hits
+//     of one face-test batch are inserted by one lane per target ray at a
+//     time (__match_any_sync groups the lanes);
+//   * rounds and compositing: after the traversal each lane sorts its heap
+//     (heapsort) and runs the rounds of its own ray serially, in entry
+//     order.  Rays whose buffer ran out traverse again (with the packet's
+//     other such rays) from their t_curr.
+#include <math_constants.h>
+
+#include "gt_device.cuh"
+#include "gt_internal.cuh"
+#include "gt_trace_common.cuh"
+#include "gt_warp.cuh"
+
+namespace gt {
+
+constexpr int kPairCap = 64;  // (proxy, ray) pairs: < 32 queued + the rays of one leaf
+constexpr int kSurvCap = 64;  // pairs that passed the sphere filter (< kSurvivors + 32)
+
+template <int KB>
+struct PacketScratch {
+  unsigned long long hk[KB][32];  // heap of ray r in column r: hit keys, max at row 0
+  uint32_t snode[kWarpStack];
+  float skey[kWarpStack];
+  uint32_t lj[8];  // leaf children of the visited node that some ray hit,
+  uint32_t lm[8];  // with the mask of those rays
+  uint32_t pj[kPairCap];
+  uint8_t pr[kPairCap];
+  uint32_t svj[kSurvCap];
+  uint8_t svr[kSurvCap];
+  float hq[kMaxHitsPerProxy][32];  // hits of each lane's pair, column per lane
+  float dx[32], dy[32], dz[32];    // ray directions
+  float tlo[32], thi[32];          // ray intervals; thi = far bound
+  uint32_t hn[32];                 // heap sizes
+  float4 nbuf[16];                 // the node being visited
+  RayStats stats;
+};
+
+// float -> uint map that preserves order (for warp min/max reductions)
+__device__ __forceinline__ uint32_t ord_f(float x) {
+  const uint32_t u = __float_as_uint(x);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float unord_f(uint32_t u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
+}
+
+// Key of hit (t, p): ordered like (t, p) in the k-buffer (t first, then the
+// particle index).  -0 is folded into +0 so that equal t compare equal.
+__device__ __forceinline__ unsigned long long hit_key(float t, uint32_t p) {
+  return ((unsigned long long)ord_f(t + 0.0f) << 32) | p;
+}
+__device__ __forceinline__ float key_t(unsigned long long k) { return unord_f((uint32_t)(k >> 32)); }
+__device__ __forceinline__ uint32_t key_p(unsigned long long k) { return (uint32_t)k; }
+
+// Sift key x down from row i of heap column r holding n entries.
+template <int KB>
+__device__ __forceinline__ void heap_sift(PacketScratch<KB>& W, uint32_t r, uint32_t i, uint32_t n,
+                                          unsigned long long x) {
+  while (true) {
+    uint32_t c = 2 * i + 1;
+    if (c >= n) break;
+    unsigned long long ck = W.hk[c][r];
+    if (c + 1 < n) {
+      const unsigned long long c2 = W.hk[c + 1][r];
+      if (ck < c2) {
+        c = c + 1;
+        ck = c2;
+      }
+    }
+    if (!(x < ck)) break;
+    W.hk[i][r] = ck;
+    i = c;
+  }
+  W.hk[i][r] = x;
+}
+
+// Offers hit key x to the k-buffer of ray r (capacity cap): kept when the
+// buffer is not full or x is below its largest entry.
+template <int KB>
+__device__ __forceinline__ void heap_offer(PacketScratch<KB>& W, uint32_t r, uint32_t cap, unsigned long long x) {
+  const uint32_t n = W.hn[r];
+  if (n < cap) {
+    uint32_t i = n;
+    while (i > 0) {
+      const uint32_t par = (i - 1) >> 1;
+      const unsigned long long pk = W.hk[par][r];
+      if (!(pk < x)) break;
+      W.hk[i][r] = pk;
+      i = par;
+    }
+    W.hk[i][r] = x;
+    W.hn[r] = n + 1;
+    if (n + 1 == cap) W.thi[r] = key_t(W.hk[0][r]);
+  } else {
+    if (!(x < W.hk[0][r])) return;
+    heap_sift(W, r, 0, n, x);
+    W.thi[r] = key_t(W.hk[0][r]);
+  }
+}
+
+// Sorts heap column r (n entries) ascending.
+template <int KB>
+__device__ __forceinline__ void heap_sort(PacketScratch<KB>& W, uint32_t r, uint32_t n) {
+  for (uint32_t end = n; end > 1; --end) {
+    const unsigned long long x = W.hk[end - 1][r];
+    W.hk[end - 1][r] = W.hk[0][r];
+    heap_sift(W, r, 0, end - 1, x);
+  }
+}
+
+__device__ __forceinline__ float warp_max_f(float x) { return unord_f(__reduce_max_sync(kFull, ord_f(x))); }
+
+// One traversal of the packet: every live lane's ray collects the cap
+// smallest front-face hits with t in (its t_curr, t_max) into its heap.
+// Lanes that are not live take no part (far bound -inf).
+template <int KB>
+__device__ __forceinline__ void packet_traverse(const SceneDev& S, const FaceTable& F, PacketScratch<KB>& W, V3 o,
+                                                const BoxRay& br, bool live, float tlo, float t_max, uint32_t cap,
+                                                uint32_t& status, uint32_t lane) {
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  float thi = live ? t_max : -CUDART_INF_F;
+  W.tlo[lane] = tlo;
+  W.thi[lane] = thi;
+  W.hn[lane] = 0;
+  if (S.n_kept == 0) return;
+  float thi_max = warp_max_f(thi);
+  RayStats& st = W.stats;
+  int sp = 1, nq = 0, ns = 0;
+  if (lane == 0) {
+    W.snode[0] = 0;
+    W.skey[0] = -CUDART_INF_F;
+  }
+  __syncwarp();
+  uint32_t iters = 0;
+  const uint32_t max_iters = min(4u * S.n_kept + 64u, F.lim_steps);
+  // lanes 0..15 prefetch the 16 float4 of the node the next pop most likely
+  // takes (the top of the stack), so that its load overlaps the leaf work
+  uint32_t pf_node = 0;
+  float4 pf = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (lane < 16) pf = __ldg(S.nodes8 + lane);
+  while (true) {
+    if (++iters > max_iters) {
+      status |= kStatusVisitCap;
+      return;
+    }
+    // pop the top node whose entry distance is within some ray's far bound
+    uint32_t node = kInvalid;
+    while (sp > 0) {
+      --sp;
+      const uint32_t n = W.snode[sp];
+      if (W.skey[sp] <= thi_max) {
+        node = n;
+        break;
+      }
+    }
+    int nl = 0;  // leaf children of this visit waiting to become pairs
+    if (node != kInvalid) {
+      if (lane < 16) {
+        if (node != pf_node) pf = __ldg(S.nodes8 + 16 * (size_t)node + lane);
+        W.nbuf[lane] = pf;
+      }
+      __syncwarp();
+      int ni = 0;
+      float mykey = CUDART_INF_F;
+      uint32_t myref = 0;
+#pragma unroll
+      for (int c = 0; c < 8; ++c) {
+        const float4 a = W.nbuf[2 * c], b = W.nbuf[2 * c + 1];
+        const uint32_t ref = __float_as_uint(b.z);
+        const float x0 = __fmaf_rn(a.x, br.ix, -br.ox), x1 = __fmaf_rn(a.w, br.ix, -br.ox);
+        const float y0 = __fmaf_rn(a.y, br.iy, -br.oy), y1 = __fmaf_rn(b.x, br.iy, -br.oy);
+        const float z0 = __fmaf_rn(a.z, br.iz, -br.oz), z1 = __fmaf_rn(b.y, br.iz, -br.oz);
+        const float tn =
+            fmaxf(fmaxf(fminf(x0, x1) - br.px, fminf(y0, y1) - br.py), fmaxf(fminf(z0, z1) - br.pz, tlo));
+        const float tf =
+            fminf(fminf(fmaxf(x0, x1) + br.px, fmaxf(y0, y1) + br.py), fminf(fmaxf(z0, z1) + br.pz, thi));
+        const bool hit = ref != kInvalid && tn <= tf;  // empty slots (packed at the end) never hit
+        const uint32_t m = __ballot_sync(kFull, hit);
+        if (m == 0) continue;
+        if (ref & kLeafBit) {
+          if (lane == 0) {
+            W.lj[nl] = ref & ~kLeafBit;
+            W.lm[nl] = m;
+          }
+          ++nl;
+        } else {
+          const uint32_t key = __reduce_min_sync(kFull, hit ? ord_f(tn) : 0xFFFFFFFFu);
+          if ((int)lane == ni) {
+            mykey = unord_f(key);
+            myref = ref;
+          }
+          ++ni;
+        }
+      }
+      if (lane == 0) st.node_visits += 1;
+      if (ni > 0) {
+        if (sp + ni > (int)F.lim_stack) {
+          status |= kStatusStackOverflow;
+          return;
+        }
+        if (ni > 1) warp_sort_prefix(mykey, myref, lane, ni);
+        if ((int)lane < ni) {
+          W.snode[sp + ni - 1 - (int)lane] = myref;
+          W.skey[sp + ni - 1 - (int)lane] = mykey;
+        }
+        sp += ni;
+      }
+      __syncwarp();
+      if (sp > 0) {
+        pf_node = W.snode[sp - 1];
+        if (lane < 16) pf = __ldg(S.nodes8 + 16 * (size_t)pf_node + lane);
+      }
+    }
+    // leaf work: face tests once kSurvivors pairs passed the sphere filter;
+    // the visit's hit leaves become (proxy, ray) pairs while fewer than 32
+    // pairs wait; the sphere filter once 32 pairs wait; everything when no
+    // node is left
+    int li = 0;
+    while (true) {
+      const bool drain = sp == 0 && li == nl;
+      if (ns >= kSurvivors || (drain && nq == 0 && ns > 0)) {
+        const int nb = ns < 32 ? ns : 32;
+        const bool have = (int)lane < nb;
+        uint32_t j = 0, r = 0;
+        if (have) {
+          j = W.svj[ns - nb + (int)lane];
+          r = W.svr[ns - nb + (int)lane];
+        }
+        ns -= nb;
+        int nh = 0;
+        if (have) {
+          const V3 d = mk(W.dx[r], W.dy[r], W.dz[r]);
+          const float tb = fminf(next_up(W.thi[r]), t_max);
+          auto on_hit = [&](float t, int) {
+            if (nh < kMaxHitsPerProxy) W.hq[nh][lane] = t;
+            ++nh;
+          };
+          proxy_test<true, decltype(on_hit)&, false>(F, S.w2o, j, o, d, W.tlo[r], tb, on_hit);
+          if (nh > kMaxHitsPerProxy) {
+            status |= kStatusHitOverflow;
+            nh = kMaxHitsPerProxy;
+          }
+        }
+        const uint32_t found = __reduce_add_sync(kFull, (uint32_t)nh);
+        if (lane == 0) st.anyhits += found;
+        if (found) {
+          __syncwarp();
+          const uint32_t p = nh ? __ldg(S.leaf_pidx + j) : 0u;
+          // one lane per target ray inserts at a time
+          while (true) {
+            const bool pend = nh > 0;
+            if (!__any_sync(kFull, pend)) break;
+            const uint32_t peers = __match_any_sync(kFull, pend ? r : 64u + lane);
+            if (pend && (int)lane == __ffs(peers) - 1) {
+              heap_offer(W, r, cap, hit_key(W.hq[nh - 1][lane], p));
+              --nh;
+            }
+            __syncwarp();
+          }
+          thi = W.thi[lane];
+          thi_max = warp_max_f(thi);
+        }
+        continue;
+      }
+      if (nq < 32 && li < nl) {
+        const uint32_t m = W.lm[li];
+        if ((m >> lane) & 1u) {
+          const int q = nq + __popc(m & lt_mask);
+          W.pj[q] = W.lj[li];
+          W.pr[q] = (uint8_t)lane;
+        }
+        nq += __popc(m);
+        ++li;
+        __syncwarp();
+        continue;
+      }
+      if (nq >= 32 || (drain && nq > 0)) {
+        const int nb = nq < 32 ? nq : 32;
+        uint32_t j = 0, r = 0;
+        const bool have = (int)lane < nb;
+        if (have) {
+          j = W.pj[nq - nb + (int)lane];
+          r = W.pr[nq - nb + (int)lane];
+        }
+        nq -= nb;
+        if (lane == 0) st.proxy_tests += (unsigned)nb;
+        const bool surv = have && proxy_sphere(F, S.w2o, j, o, mk(W.dx[r], W.dy[r], W.dz[r]));
+        const uint32_t sm = __ballot_sync(kFull, surv);
+        if (surv) {
+          const int q = ns + __popc(sm & lt_mask);
+          W.svj[q] = j;
+          W.svr[q] = (uint8_t)r;
+        }
+        ns += __popc(sm);
+        __syncwarp();
+        continue;
+      }
+      break;
+    }
+    if (sp == 0 && nq == 0 && ns == 0) break;
+  }
+}
+
+__device__ __forceinline__ bool ray_more(const RayUniforms& u, float T, float t_curr, uint32_t step) {
+  return u.T_min < T && t_curr < u.t_max && u.early_stop != step;
+}
+
+// Persistent kernel: each warp takes one 8x4 tile at a time from a global
+// counter (tiles of all views back to back) and traces its 32 rays.
+template <int KB>
+__global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__ views, uint32_t n_views,
+                                                     uint32_t total_tiles, DevCounters* ctr,
+                                                     const __grid_constant__ FaceTable F) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  PacketScratch<KB>& W = *reinterpret_cast<PacketScratch<KB>*>(smem_raw);
+  const uint32_t lane = threadIdx.x & 31;
+  if (lane == 0) W.stats = RayStats{0, 0, 0, 0, 0, 0};
+  __syncwarp();
+  uint32_t status = 0, rays = 0;
+  uint32_t n_rounds = 0, n_entries = 0, n_contrib = 0;
+  while (true) {
+    uint32_t tile = 0;
+    if (lane == 0) tile = atomicAdd(&ctr->work, 1u);
+    tile = __shfl_sync(kFull, tile, 0);
+    if (tile >= total_tiles) break;
+    const uint32_t vi = n_views == 1 ? 0u : find_view(views, n_views, tile);
+    const ViewDev& V = views[vi];
+    uint32_t px, py;
+    tile_pixel(V.tiles_x, tile - V.tile_begin, lane, px, py);
+    const bool valid = px < V.w && py < V.h;
+    if (__ballot_sync(kFull, valid) == 0) continue;
+    V3 o, d;
+    ray_gen(V.u, V.w, V.h, valid ? px : 0u, valid ? py : 0u, o, d);
+    const BoxRay br = make_boxray(o, d, V.s.scene_mag);
+    W.dx[lane] = d.x;
+    W.dy[lane] = d.y;
+    W.dz[lane] = d.z;
+    const float t_max = V.u.t_max;
+    const uint32_t k = V.u.k;
+    const uint32_t cap = V.kbuf < (uint32_t)KB ? V.kbuf : (uint32_t)KB;
+    float L0 = 0.f, L1 = 0.f, L2 = 0.f, T = 1.f, t_curr = V.u.t_min;
+    uint32_t step = 0;
+    bool live = valid && ray_more(V.u, T, t_curr, step);
+    while (__any_sync(kFull, live)) {
+      packet_traverse<KB>(V.s, F, W, o, br, live, t_curr, t_max, cap, status, lane);
+      __syncwarp();
+      if (__reduce_or_sync(kFull, status) & (kStatusStackOverflow | kStatusVisitCap | kStatusHitOverflow)) break;
+      if (live) {
+        const uint32_t cnt = W.hn[lane];
+        const bool complete = cnt < cap;  // every hit beyond t_curr is in the buffer
+        heap_sort(W, lane, cnt);
+        uint32_t head = 0;
+        while (ray_more(V.u, T, t_curr, step)) {
+          while (head < cnt && !(key_t(W.hk[head][lane]) > t_curr)) ++head;
+          const uint32_t avail = cnt - head;
+          if (!complete && avail < k) break;  // the next round reaches past the buffer
+          const uint32_t n = avail < k ? avail : k;
+          const float new_t = n == k ? key_t(W.hk[head + k - 1][lane]) + 1e-4f : t_max;
+          ++step;
+          ++n_rounds;
+          n_entries += n;
+          // front-to-back accumulation in entry order (src/GS_shader.ts:250-269)
+          for (uint32_t e = 0; e < n; ++e) {
+            const uint32_t ep = key_p(W.hk[head + e][lane]);
+            const Shade sd = load_shade(V.s.shade, ep);
+            const float alpha = response(sd, o, d) * sd.opacity;
+            if (V.u.alpha_min < alpha) {
+              const V3 dir = vnorm(vsub(sd.mu, o));
+              float c[3];
+              sh_radiance(V.s.sh, ep, dir, V.u.deg, c);
+              const float x0 = c[0] > 0.f ? c[0] : 0.f;
+              const float x1 = c[1] > 0.f ? c[1] : 0.f;
+              const float x2 = c[2] > 0.f ? c[2] : 0.f;
+              const float ta = T * alpha;
+              L0 = L0 + ta * x0;
+              L1 = L1 + ta * x1;
+              L2 = L2 + ta * x2;
+              T = T * (1.0f - alpha);
+              ++n_contrib;
+            }
+          }
+          head += n;
+          t_curr = new_t;
+          if (step >= F.lim_rounds && ray_more(V.u, T, t_curr, step)) {
+            status |= kStatusRoundCap;
+            t_curr = t_max;
+          }
+        }
+        live = ray_more(V.u, T, t_curr, step);
+      }
+      __syncwarp();
+    }
+    if (valid) {
+      const float4 r = make_float4(L0, L1, L2, 1.0f);
+      float4* dst = V.out + (size_t)py * V.w + px;
+      *dst = V.u.aa ? aa_blend(*dst, r, V.u.frames) : r;
+      ++rays;
+    }
+  }
+  const uint32_t s_rays = __reduce_add_sync(kFull, rays);
+  const uint32_t s_rounds = __reduce_add_sync(kFull, n_rounds);
+  const uint32_t s_entries = __reduce_add_sync(kFull, n_entries);
+  const uint32_t s_contrib = __reduce_add_sync(kFull, n_contrib);
+  if (lane == 0) {
+    W.stats.rounds += s_rounds;
+    W.stats.entries += s_entries;
+    W.stats.contributing += s_contrib;
+  }
+  __syncwarp();
+  flush_stats(ctr, W.stats, lane == 0 ? s_rays : 0u, status);
+}
+
+template <int KB>
+static Err launch_packet_kb(const ViewDev* d_views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
+                            const FaceTable& faces, int num_sms, cudaStream_t stream, uint64_t* launches) {
+  const size_t smem = sizeof(PacketScratch<KB>);
+  GT_CUDA_TRY(cudaFuncSetAttribute(k_trace_packet<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  GT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_packet<KB>, 32, smem));
+  uint32_t grid = (uint32_t)num_sms * (uint32_t)std::max(1, per_sm);
+  if (grid > total_tiles) grid = std::max(1u, total_tiles);
+  k_trace_packet<KB><<<grid, 32, smem, stream>>>(d_views, n_views, total_tiles, counters, faces);
+  ++*launches;
+  GT_CUDA_TRY(cudaGetLastError());
+  return Err{};
+}
+
+Err launch_trace_packet(const ViewDev* views, const ViewDev* d_views, uint32_t n_views, uint32_t total_tiles,
+                        DevCounters* counters, const FaceTable& faces, int num_sms, cudaStream_t stream,
+                        uint64_t* launches) {
+  uint32_t kmax = 1;
+  for (uint32_t i = 0; i < n_views; ++i) kmax = std::max(kmax, views[i].kbuf);
+  if (kmax <= 24) return launch_packet_kb<24>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches);
+  if (kmax <= 32) return launch_packet_kb<32>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches);
+  if (kmax <= 48) return launch_packet_kb<48>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches);
+  return launch_packet_kb<64>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches);
+}
+
+}  // namespace gt

@@ -327,9 +327,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) k_trace8(const ViewDev
 
 uint32_t kmax_for(uint32_t k) { return k <= 8 ? 8u : (k <= 16 ? 16u : 32u); }
 
-void apply_shape(ViewDev* views, uint32_t n_views, const LaunchShape& shape) {
+bool packet_launch(const ViewDev* views, uint32_t n_views, const LaunchShape& shape, bool ckpt) {
+  if (!shape.packet || ckpt) return false;
+  for (uint32_t i = 0; i < n_views; ++i)
+    if (views[i].u.debug != 0) return false;
+  return true;
+}
+
+void apply_shape(ViewDev* views, uint32_t n_views, const LaunchShape& shape, bool packet) {
   for (uint32_t i = 0; i < n_views; ++i) {
-    uint32_t kb = std::min(kMaxKbuf, std::max(shape.kbuf, views[i].u.k));
+    uint32_t kb = packet ? std::min(kMaxPacketKbuf, std::max(shape.packet_kbuf, views[i].u.k))
+                         : std::min(kMaxKbuf, std::max(shape.kbuf, views[i].u.k));
     views[i].kbuf = std::max(1u, kb);
     views[i].leaf_batch = std::min(32u, std::max(1u, shape.leaf_batch));
   }
@@ -338,8 +346,11 @@ void apply_shape(ViewDev* views, uint32_t n_views, const LaunchShape& shape) {
 Err launch_trace(ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
                  const FaceTable& faces, const LaunchShape& shape, int num_sms, cudaStream_t stream,
                  uint64_t* launches, ViewDev* d_views, const Ckpt* ckpt) {
-  apply_shape(views, n_views, shape);
+  const bool packet = packet_launch(views, n_views, shape, ckpt != nullptr);
+  apply_shape(views, n_views, shape, packet);
   GT_CUDA_TRY(cudaMemcpyAsync(d_views, views, sizeof(ViewDev) * n_views, cudaMemcpyHostToDevice, stream));
+  if (packet)
+    return launch_trace_packet(views, d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches);
   uint32_t block = kWarpsPerBlock * 32;
   uint32_t grid = (uint32_t)num_sms * std::max(1u, shape.blocks_per_sm);
   uint64_t warps_needed = (uint64_t)total_tiles * 32u;
