@@ -375,15 +375,18 @@ gt_status gt_l2_loss(gt_context* ctx, const float* rgba, const float* target, ui
  * given view and caches the fastest per (GPU, scene-size bucket, image-size
  * bucket, k).  gt_render and gt_render_batch use the cached choice.
  * Two kernels render the plain image (debugMode 0), with identical results:
- *   block_threads 32:  a warp traces the 32 rays of an 8x4 tile together
- *                      (the default); kbuf = k-buffer entries per ray
- *                      (k..64, default 32); blocks_per_sm and leaf_batch
- *                      are not used (the grid fills the SMs);
+ *   block_threads 32:  a warp traces the 32 rays of an 8x4 tile together;
+ *                      kbuf = k-buffer entries per ray (k..64, default 32);
+ *                      blocks_per_sm and leaf_batch are not used (the grid
+ *                      fills the SMs);
  *   block_threads 128: a warp traces one ray; kbuf = k-buffer entries of a
  *                      traversal (k..128, default 64), blocks_per_sm and
  *                      leaf_batch as below.
- * Debug modes, hit recording and the checkpointing forward of gt_backward
- * always use the second kernel. */
+ * Without a cached shape a launch takes the first kernel when it has at
+ * least 160 8x4 tiles per SM (about 0.75 Mpixels on a 148-SM B200) and the
+ * second otherwise: tiles are coarse work items, and with few of them per
+ * warp the slowest ones decide the time.  Debug modes, hit recording and the
+ * checkpointing forward of gt_backward always use the second kernel. */
 typedef struct gt_tune_result {
   uint32_t block_threads; /* 32: a warp per 8x4 tile; 128: a warp per ray      */
   uint32_t blocks_per_sm; /* resident blocks per SM of the persistent grid      */

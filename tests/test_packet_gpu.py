@@ -1,0 +1,111 @@
+"""The tile-packet kernel (one warp per 8x4 tile of rays, gt_packet.cu)
+against the oracle on the cases the other parity tests cover with the
+default choice.  At test image sizes the default is the warp-per-ray kernel,
+so every case here installs block_threads = 32 for its view first
+(gt_set_tune); the results must be the oracle's, bit for bit."""
+import numpy as np
+import pytest
+
+from conftest import small_scene, view
+from oracle import oracle
+from gtrace.tracer import Scene
+from gtrace.uniforms import with_fields
+
+pytestmark = pytest.mark.gpu
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, dtype=np.float32).reshape(-1, 4).view(np.uint32)
+
+
+def _packet_render(ctx, scene, u, w, h, kbuf=32, **kw):
+    ctx.set_tune(scene, u, w, h, kbuf=kbuf, block_threads=32)
+    try:
+        return ctx.render(scene, u, w, h, **kw)
+    finally:
+        ctx._lib.gt_autotune_reset(ctx._h)
+
+
+def test_uniform_variants_and_sizes(ctx):
+    pg = small_scene(n=2500, seed=51)
+    g = Scene(ctx, pg.gaussiansBuffer, 0.05)
+    o = oracle.Scene(pg.gaussiansBuffer, 0.05, "f32")
+    base = view(40, 28, k=5).uniforms
+    for u in [base, with_fields(base, early_stop=1), with_fields(base, early_stop=3), with_fields(base, T_min=0.5),
+              with_fields(base, sh_degree_max=0), with_fields(base, sh_degree_max=2),
+              with_fields(base, alpha_min=0.3), with_fields(base, t_min=3.9), with_fields(base, t_max=4.2)]:
+        img = _packet_render(ctx, g, u, 40, 28)
+        ref, _ = o.render(u, 40, 28)
+        assert np.array_equal(_bits(img), ref.view(np.uint32))
+    for w, h in [(1, 1), (9, 5), (130, 7), (33, 65)]:
+        v = view(w, h, k=7)
+        img = _packet_render(ctx, g, v.uniforms, w, h)
+        ref, _ = o.render(v.uniforms, w, h)
+        assert np.array_equal(_bits(img), ref.view(np.uint32)), (w, h)
+
+
+def test_camera_inside_and_small_scenes(ctx):
+    pg = small_scene(n=2000, seed=52)
+    g = Scene(ctx, pg.gaussiansBuffer, 0.01)
+    o = oracle.Scene(pg.gaussiansBuffer, 0.01, "f32")
+    v = view(40, 40, pos=(0.05, -0.02, 0.1), target=(1.0, 0.3, -2.0), k=6)
+    img = _packet_render(ctx, g, v.uniforms, 40, 40)
+    ref, _ = o.render(v.uniforms, 40, 40)
+    assert np.array_equal(_bits(img), ref.view(np.uint32))
+    empty = Scene(ctx, np.zeros((0, 80), np.float32), 0.01)
+    img = _packet_render(ctx, empty, view(16, 16).uniforms, 16, 16)
+    assert (img[..., :3] == 0).all() and (img[..., 3] == 1).all()
+    rec = np.zeros((1, 80), np.float32)
+    rec[0, 4:7] = 0.3
+    rec[0, 8] = 1.0
+    rec[0, 12] = 0.9
+    rec[0, 16:19] = (0.5, 0.1, -0.3)
+    one = Scene(ctx, rec, 0.01)
+    v = view(32, 32, k=2)
+    img = _packet_render(ctx, one, v.uniforms, 32, 32)
+    ref, _ = oracle.Scene(rec, 0.01, "f32").render(v.uniforms, 32, 32)
+    assert np.array_equal(_bits(img), ref.view(np.uint32)) and img[..., :3].max() > 0
+
+
+def test_dense_scene_many_rounds(ctx):
+    """Many rounds per ray and k-buffers that run out several times."""
+    pg = small_scene(n=12000, seed=53)
+    g = Scene(ctx, pg.gaussiansBuffer, 0.01)
+    o = oracle.Scene(pg.gaussiansBuffer, 0.01, "f32")
+    for k, kbuf in [(1, 24), (3, 32), (16, 32), (32, 64)]:
+        v = view(48, 40, k=k, T_min=0.0001)
+        img = _packet_render(ctx, g, v.uniforms, 48, 40, kbuf=kbuf)
+        ref, _ = o.render(v.uniforms, 48, 40)
+        assert np.array_equal(_bits(img), ref.view(np.uint32)), (k, kbuf)
+
+
+def test_antialias_frames(ctx):
+    pg = small_scene(n=3000, seed=54)
+    w, h = 45, 29
+    g = Scene(ctx, pg.gaussiansBuffer, 0.01)
+    o = oracle.Scene(pg.gaussiansBuffer, 0.01, "f32")
+    acc_gpu = np.zeros((h, w, 4), np.float32)
+    acc_ref = np.zeros((w * h, 4), np.float32)
+    for f in range(3):
+        v = view(w, h, k=5, accumulated_frames=f)
+        _packet_render(ctx, g, v.uniforms, w, h, out=acc_gpu, antialias=True)
+        o.render_accum(v.uniforms, w, h, acc_ref)
+        assert np.array_equal(_bits(acc_gpu), acc_ref.view(np.uint32)), f
+
+
+def test_batch_of_views_and_scenes(ctx):
+    pa = small_scene(n=1500, seed=55)
+    pb = small_scene(n=2500, seed=56)
+    ga, gb = Scene(ctx, pa.gaussiansBuffer, 0.01), Scene(ctx, pb.gaussiansBuffer, 0.02)
+    oa, ob = oracle.Scene(pa.gaussiansBuffer, 0.01, "f32"), oracle.Scene(pb.gaussiansBuffer, 0.02, "f32")
+    views = [(ga, view(37, 21, k=4).uniforms, 37, 21), (gb, view(24, 40, k=9).uniforms, 24, 40),
+             (ga, view(16, 16, pos=(1.0, 2.0, 3.5), k=16).uniforms, 16, 16)]
+    ctx.set_tune(views[0][0], views[0][1], 37, 21, kbuf=32, block_threads=32)  # the batch takes item 0's shape
+    try:
+        outs, st = ctx.render_batch(views)
+    finally:
+        ctx._lib.gt_autotune_reset(ctx._h)
+    for (sc, u, w, h), out in zip(views, outs):
+        ref, _ = (oa if sc is ga else ob).render(u, w, h)
+        assert np.array_equal(_bits(out), ref.view(np.uint32))
+    assert st["rays"] == 37 * 21 + 24 * 40 + 16 * 16

@@ -632,7 +632,7 @@ extern "C" gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items
   LaunchShape shape = shape_for(ctx, items[0].scene, items[0].w, items[0].h, items[0].u.k);
   // the view table is rebuilt on every call: it takes the shape's k-buffer
   // size and leaf batch here, and the graph's kernel matches its slot count
-  const bool packet = packet_launch(ctx->h_views, count, shape, false);
+  const bool packet = packet_launch(ctx->h_views, count, total_tiles, ctx->num_sms, shape, false);
   apply_shape(ctx->h_views, count, shape, packet);
   uint32_t kb_max = 1;
   bool any_debug = false;  // the graph's kernel is the debug-mode instantiation
@@ -724,10 +724,12 @@ extern "C" gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const g
     *out_ms = ms_min;
     return GT_OK;
   };
-  // 1. tile packets (the default kernel): k-buffer entries per ray
   const uint32_t k = u->k;
   LaunchShape best_sh;
   float best = 1e30f, def = 0.0f;
+  st = time_shape(LaunchShape(), 3, &def);
+  if (st != GT_OK) return st;
+  // 1. tile packets: k-buffer entries per ray
   const uint32_t pkbufs[] = {k, 24u, 32u, 48u, 64u};
   for (int i = 0; i < 5; ++i) {
     const uint32_t kb = pkbufs[i];
@@ -738,7 +740,6 @@ extern "C" gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const g
     float ms = 0.0f;
     st = time_shape(sh, 3, &ms);
     if (st != GT_OK) return st;
-    if (sh.packet_kbuf == std::max(k, LaunchShape().packet_kbuf)) def = ms;
     if (ms < best) {
       best = ms;
       best_sh = sh;

@@ -136,12 +136,20 @@ struct LaunchShape {
   uint32_t kbuf = 64;               // k-buffer entries (raised to k when k is larger; <= kMaxKbuf)
   uint32_t leaf_batch = 32;         // leaf queue size that triggers proxy tests
   // Plain renders (debugMode 0, no checkpoint) run one warp per 8x4 tile of
-  // rays (gt_packet.cu) unless packet is 0; their k-buffer has packet_kbuf
-  // entries per ray (raised to k; <= kMaxPacketKbuf).
-  uint32_t packet = 1;
+  // rays (gt_packet.cu) when packet is 1, one warp per ray when it is 0, and
+  // by default (2) the tile packets when the launch has at least
+  // kPacketTilesPerSm tiles per SM.  The packet kernel's k-buffer has
+  // packet_kbuf entries per ray (raised to k; <= kMaxPacketKbuf).
+  uint32_t packet = 2;
   uint32_t packet_kbuf = 32;
 };
 constexpr uint32_t kMaxPacketKbuf = 64;
+// A tile packet is a coarse work item: a few tiles whose rays have many
+// hits take several times the mean, so with fewer than ~10 tiles per
+// resident warp (16 warps an SM) their tail outweighs the packets' gain
+// (1M-Gaussian view: 960x540, 6.8 tiles a warp, 21.4 ms as packets against
+// 18.6 ms a ray per warp; 1280x720, 12 tiles a warp, 29.1 against 32.7 ms).
+constexpr uint32_t kPacketTilesPerSm = 160;
 
 // ----------------------------------------------------------- host helpers
 // Work slots of a w x h view: 32 per 8 x 4 tile of its tile grid, padded to
@@ -223,7 +231,8 @@ constexpr uint32_t kCkptHeader = 4;
 // Trace launches (gt_trace.cu).  launch_trace writes the shape's k-buffer
 // size and leaf batch into the host view table before uploading it.
 // Whether launch_trace renders these views with the tile-packet kernel.
-bool packet_launch(const ViewDev* views, uint32_t n_views, const LaunchShape& shape, bool ckpt);
+bool packet_launch(const ViewDev* views, uint32_t n_views, uint32_t total_tiles, int num_sms,
+                   const LaunchShape& shape, bool ckpt);
 // Sets each view's k-buffer size and leaf batch for a launch of either kernel.
 void apply_shape(ViewDev* views, uint32_t n_views, const LaunchShape& shape, bool packet = false);
 Err launch_trace(ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,

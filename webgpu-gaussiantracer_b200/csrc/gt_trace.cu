@@ -327,11 +327,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) k_trace8(const ViewDev
 
 uint32_t kmax_for(uint32_t k) { return k <= 8 ? 8u : (k <= 16 ? 16u : 32u); }
 
-bool packet_launch(const ViewDev* views, uint32_t n_views, const LaunchShape& shape, bool ckpt) {
+bool packet_launch(const ViewDev* views, uint32_t n_views, uint32_t total_tiles, int num_sms,
+                   const LaunchShape& shape, bool ckpt) {
   if (!shape.packet || ckpt) return false;
   for (uint32_t i = 0; i < n_views; ++i)
     if (views[i].u.debug != 0) return false;
-  return true;
+  if (shape.packet == 1) return true;
+  return (uint64_t)total_tiles >= (uint64_t)kPacketTilesPerSm * (uint64_t)std::max(1, num_sms);
 }
 
 void apply_shape(ViewDev* views, uint32_t n_views, const LaunchShape& shape, bool packet) {
@@ -346,7 +348,7 @@ void apply_shape(ViewDev* views, uint32_t n_views, const LaunchShape& shape, boo
 Err launch_trace(ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
                  const FaceTable& faces, const LaunchShape& shape, int num_sms, cudaStream_t stream,
                  uint64_t* launches, ViewDev* d_views, const Ckpt* ckpt) {
-  const bool packet = packet_launch(views, n_views, shape, ckpt != nullptr);
+  const bool packet = packet_launch(views, n_views, total_tiles, num_sms, shape, ckpt != nullptr);
   apply_shape(views, n_views, shape, packet);
   GT_CUDA_TRY(cudaMemcpyAsync(d_views, views, sizeof(ViewDev) * n_views, cudaMemcpyHostToDevice, stream));
   if (packet)
