@@ -383,9 +383,11 @@ gt_status gt_l2_loss(gt_context* ctx, const float* rgba, const float* target, ui
  *                      traversal (k..128, default 64), blocks_per_sm and
  *                      leaf_batch as below.
  * Without a cached shape a launch takes the first kernel when it has at
- * least 160 8x4 tiles per SM (about 0.75 Mpixels on a 148-SM B200) and the
+ * least 80 8x4 tiles per SM (about 0.38 Mpixels on a 148-SM B200) and the
  * second otherwise: tiles are coarse work items, and with few of them per
- * warp the slowest ones decide the time.  Debug modes, hit recording and the
+ * warp the slowest ones decide the time.  With the first kernel, the rays
+ * of a tile that still need hits after three traversals are finished by
+ * the second one (a second launch).  Debug modes, hit recording and the
  * checkpointing forward of gt_backward always use the second kernel. */
 typedef struct gt_tune_result {
   uint32_t block_threads; /* 32: a warp per 8x4 tile; 128: a warp per ray      */

@@ -71,6 +71,26 @@ static void drop_graphs(gt_context* ctx) {
   ctx->graphs.clear();
 }
 
+// Handoff buffer for a launch of `rays` rays: room for a quarter of them (a
+// packet whose rays do not fit keeps tracing them itself).
+static gt_status ensure_handoff(gt_context* ctx, uint64_t rays, Handoff* out) {
+  const uint64_t want64 = std::max<uint64_t>(4096, rays / 4);
+  const uint32_t want = (uint32_t)std::min<uint64_t>(want64, 1u << 28);
+  if (want > ctx->handoff_cap) {
+    // captured graphs hold the old buffer address
+    cudaStreamSynchronize(ctx->stream);
+    drop_graphs(ctx);
+    cudaFree(ctx->d_handoff);
+    ctx->d_handoff = nullptr;
+    ctx->handoff_cap = 0;
+    API_CUDA(ctx, cudaMalloc(&ctx->d_handoff, sizeof(HandoffRay) * (size_t)want));
+    ctx->handoff_cap = want;
+  }
+  out->rays = ctx->d_handoff;
+  out->cap = ctx->handoff_cap;
+  return GT_OK;
+}
+
 static gt_status ensure_views(gt_context* ctx, uint32_t n) {
   if (n > ctx->d_views_cap || n > ctx->h_views_cap) {
     // captured graphs hold the old table addresses
@@ -259,6 +279,7 @@ extern "C" gt_status gt_context_destroy(gt_context* ctx) {
   cudaFree(ctx->d_ctr);
   cudaFreeHost(ctx->h_ctr);
   cudaFree(ctx->d_views);
+  cudaFree(ctx->d_handoff);
   cudaFreeHost(ctx->h_views);
   cudaFree(ctx->staging);
   for (cudaEvent_t ev : {ctx->call0, ctx->call1, ctx->timer0, ctx->timer1, ctx->int0, ctx->int1})
@@ -456,8 +477,11 @@ extern "C" gt_status gt_render(gt_context* ctx, const gt_scene* scene, const gt_
   uint64_t slot = ring_slot(ctx);
   API_CUDA(ctx, cudaEventRecord(ctx->ring[2 * slot], ctx->stream));
   LaunchShape shape = shape_for(ctx, scene, w, h, u->k);
+  Handoff hand;
+  st = ensure_handoff(ctx, (uint64_t)w * h, &hand);
+  if (st != GT_OK) return st;
   Err e = launch_trace(&v, 1, v.n_tiles, ctx->d_ctr, ctx->faces, shape, ctx->num_sms, ctx->stream, &ctx->launches,
-                       ctx->d_views);
+                       ctx->d_views, nullptr, &hand);
   if (e.code != GT_OK) return fail(ctx, e);
   API_CUDA(ctx, cudaEventRecord(ctx->ring[2 * slot + 1], ctx->stream));
   if (!(flags & GT_FLAG_OUTPUT_DEVICE))
@@ -607,13 +631,15 @@ extern "C" gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items
   std::stable_sort(order.begin(), order.end(),
                    [&](uint32_t a, uint32_t b) { return items[a].scene < items[b].scene; });
   std::vector<size_t> offs(count);
-  {
-    size_t o = 0;
-    for (uint32_t i = 0; i < count; ++i) {
-      offs[i] = o;
-      o += (size_t)items[i].w * items[i].h;
-    }
+  size_t all_pixels = 0;
+  for (uint32_t i = 0; i < count; ++i) {
+    offs[i] = all_pixels;
+    all_pixels += (size_t)items[i].w * items[i].h;
   }
+  // before a graph is looked up: growing the handoff buffer drops the graphs
+  Handoff hand;
+  st = ensure_handoff(ctx, all_pixels, &hand);
+  if (st != GT_OK) return st;
   for (uint32_t q = 0; q < count; ++q) {
     const uint32_t i = order[q];
     const gt_batch_item& it = items[i];
@@ -633,15 +659,19 @@ extern "C" gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items
   // the view table is rebuilt on every call: it takes the shape's k-buffer
   // size and leaf batch here, and the graph's kernel matches its slot count
   const bool packet = packet_launch(ctx->h_views, count, total_tiles, ctx->num_sms, shape, false);
-  apply_shape(ctx->h_views, count, shape, packet);
-  uint32_t kb_max = 1;
+  apply_shape(ctx->h_views, count, shape);
+  uint32_t kb_max = 1, pkb_max = 1;
   bool any_debug = false;  // the graph's kernel is the debug-mode instantiation
   for (uint32_t q = 0; q < count; ++q) {
     kb_max = std::max(kb_max, ctx->h_views[q].kbuf);
+    pkb_max = std::max(pkb_max, ctx->h_views[q].pkbuf);
     any_debug = any_debug || ctx->h_views[q].u.debug != 0;
   }
+  // the kernels of the graph: warp-per-ray slots per lane, and with tile
+  // packets their heap size and handoff
   auto key = std::make_tuple(count, total_tiles, kmax | (any_debug ? 0x10000u : 0u) | (packet ? 0x20000u : 0u),
-                             shape.blocks_per_sm, packet ? kb_max : (kb_max + 31u) / 32u);
+                             shape.blocks_per_sm,
+                             ((kb_max + 31u) / 32u) | (packet ? (pkb_max << 8) | (shape.handoff_after << 16) : 0u));
   auto it = ctx->graphs.find(key);
   if (it == ctx->graphs.end()) {
     GraphEntry g;
@@ -651,7 +681,7 @@ extern "C" gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items
     // launch_trace re-uploads the view table; inside the graph it copies from
     // the pinned staging table, which is refreshed before every replay.
     Err e = launch_trace(ctx->h_views, count, total_tiles, ctx->d_ctr, ctx->faces, shape, ctx->num_sms, cs,
-                         &ctx->launches, ctx->d_views);
+                         &ctx->launches, ctx->d_views, nullptr, &hand);
     cudaError_t ce = cudaStreamEndCapture(cs, &g.graph);
     if (e.code != GT_OK) return fail(ctx, e);
     if (ce != cudaSuccess) return fail(ctx, GT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
@@ -706,6 +736,9 @@ extern "C" gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const g
   st = ensure_views(ctx, 1);
   if (st != GT_OK) return st;
   ViewDev v = make_view(scene, *u, w, h, ctx->staging, 0);
+  Handoff hand;
+  st = ensure_handoff(ctx, (uint64_t)w * h, &hand);
+  if (st != GT_OK) return st;
   // fastest of `reps` launches of one shape
   auto time_shape = [&](const LaunchShape& sh, int reps, float* out_ms) -> gt_status {
     float ms_min = 1e30f;
@@ -713,7 +746,7 @@ extern "C" gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const g
       API_CUDA(ctx, cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), ctx->stream));
       API_CUDA(ctx, cudaEventRecord(ctx->int0, ctx->stream));
       Err e = launch_trace(&v, 1, v.n_tiles, ctx->d_ctr, ctx->faces, sh, ctx->num_sms, ctx->stream, &ctx->launches,
-                           ctx->d_views);
+                           ctx->d_views, nullptr, &hand);
       if (e.code != GT_OK) return fail(ctx, e);
       API_CUDA(ctx, cudaEventRecord(ctx->int1, ctx->stream));
       API_CUDA(ctx, cudaEventSynchronize(ctx->int1));

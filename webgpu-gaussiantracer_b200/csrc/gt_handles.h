@@ -58,6 +58,8 @@ struct gt_context {
   uint32_t h_views_cap = 0;
   float4* staging = nullptr;
   size_t staging_bytes = 0;
+  gt::HandoffRay* d_handoff = nullptr;  // rays tile packets hand to the warp-per-ray kernel
+  uint32_t handoff_cap = 0;
   cudaEvent_t call0 = nullptr, call1 = nullptr, timer0 = nullptr, timer1 = nullptr;
   cudaEvent_t int0 = nullptr, int1 = nullptr;  // library-internal timing (never the user's timer)
   cudaEvent_t ring[2 * gt::kEventRing];

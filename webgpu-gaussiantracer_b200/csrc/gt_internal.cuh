@@ -63,8 +63,8 @@ struct DevCounters {
   unsigned long long ckpt_rounds;
   unsigned int status;
   unsigned int work;  // work-stealing tile counter
-  unsigned int work2;
-  unsigned int pad;
+  unsigned int work2;    // the same for the second kernel of a launch
+  unsigned int handoff;  // rays the tile-packet kernel handed to the warp-per-ray kernel
 };
 
 // Scene as the kernels see it.  Records of kept proxies are in BVH leaf
@@ -120,6 +120,7 @@ struct ViewDev {
   uint32_t tile_begin;  // first global tile index of this view
   uint32_t n_tiles;
   uint32_t kbuf;        // k-buffer entries (k..128): a traversal keeps the kbuf closest hits
+  uint32_t pkbuf;       // the tile-packet kernel's k-buffer entries per ray (k..64)
   uint32_t leaf_batch;  // queued leaves that trigger a batch of proxy tests (8..32)
   const float4* dL;     // backward: dL/drgba (w*h)
   float* grad;          // backward: 59 x n parameter-major gradient
@@ -142,14 +143,18 @@ struct LaunchShape {
   // packet_kbuf entries per ray (raised to k; <= kMaxPacketKbuf).
   uint32_t packet = 2;
   uint32_t packet_kbuf = 32;
+  // A packet that has traced handoff_after times hands its rays that still
+  // need hits to the warp-per-ray kernel (0: never), when the launch has a
+  // handoff buffer.
+  uint32_t handoff_after = 3;
 };
 constexpr uint32_t kMaxPacketKbuf = 64;
 // A tile packet is a coarse work item: a few tiles whose rays have many
-// hits take several times the mean, so with fewer than ~10 tiles per
-// resident warp (16 warps an SM) their tail outweighs the packets' gain
-// (1M-Gaussian view: 960x540, 6.8 tiles a warp, 21.4 ms as packets against
-// 18.6 ms a ray per warp; 1280x720, 12 tiles a warp, 29.1 against 32.7 ms).
-constexpr uint32_t kPacketTilesPerSm = 160;
+// hits take several times the mean, so with few tiles per resident warp (16
+// warps an SM) their tail outweighs the packets' gain even with the handoff
+// (1M-Gaussian view, ms as packets / a ray per warp: 480x270, 1.7 tiles a
+// warp, 8.3 / 5.0; 960x540, 6.8 tiles a warp, 17.2 / 18.6).
+constexpr uint32_t kPacketTilesPerSm = 80;
 
 // ----------------------------------------------------------- host helpers
 // Work slots of a w x h view: 32 per 8 x 4 tile of its tile grid, padded to
@@ -228,19 +233,33 @@ struct Ckpt {
 };
 constexpr uint32_t kCkptHeader = 4;
 
+// A ray that a tile packet hands over part way: its work slot (32 * tile +
+// position in the tile) and its compositing state between two rounds.
+struct HandoffRay {
+  uint32_t item, step;
+  float t_curr, T, L0, L1, L2;
+  uint32_t pad;
+};
+// The handoff buffer of a launch (rays == nullptr: no handoff).
+struct Handoff {
+  HandoffRay* rays = nullptr;
+  uint32_t cap = 0;
+};
+
 // Trace launches (gt_trace.cu).  launch_trace writes the shape's k-buffer
 // size and leaf batch into the host view table before uploading it.
 // Whether launch_trace renders these views with the tile-packet kernel.
 bool packet_launch(const ViewDev* views, uint32_t n_views, uint32_t total_tiles, int num_sms,
                    const LaunchShape& shape, bool ckpt);
 // Sets each view's k-buffer size and leaf batch for a launch of either kernel.
-void apply_shape(ViewDev* views, uint32_t n_views, const LaunchShape& shape, bool packet = false);
+void apply_shape(ViewDev* views, uint32_t n_views, const LaunchShape& shape);
 Err launch_trace(ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
                  const FaceTable& faces, const LaunchShape& shape, int num_sms, cudaStream_t stream,
-                 uint64_t* launches, ViewDev* d_views_scratch, const Ckpt* ckpt = nullptr);
+                 uint64_t* launches, ViewDev* d_views_scratch, const Ckpt* ckpt = nullptr,
+                 const Handoff* handoff = nullptr);
 Err launch_trace_packet(const ViewDev* views, const ViewDev* d_views, uint32_t n_views, uint32_t total_tiles,
                         DevCounters* counters, const FaceTable& faces, int num_sms, cudaStream_t stream,
-                        uint64_t* launches);
+                        uint64_t* launches, const Handoff& handoff, uint32_t handoff_after);
 Err launch_trace_hits(const ViewDev& view, ViewDev* d_views, const uint32_t* pixels, uint32_t n_pix,
                       uint32_t max_entries, uint32_t* out_pidx, float* out_t, float* out_alpha, uint32_t* out_count,
                       uint32_t* out_rounds, float4* out_rgba, DevCounters* counters, const FaceTable& faces,

@@ -27,7 +27,13 @@
 //   * rounds and compositing: after the traversal each lane sorts its heap
 //     (heapsort) and runs the rounds of its own ray serially, in entry
 //     order.  Rays whose buffer ran out traverse again (with the packet's
-//     other such rays) from their t_curr.
+//     other such rays) from their t_curr;
+//   * handoff: a tile takes as long as its rays with the most hits, and a
+//     packet traversal for a few rays costs about as much as one for all 32.
+//     After handoff_after traversals a packet writes its rays that still
+//     need hits (their compositing state between two rounds) to a buffer,
+//     and the warp-per-ray kernel, launched next, finishes them; the
+//     arithmetic of every round is the same in both kernels.
 #include <math_constants.h>
 
 #include "gt_device.cuh"
@@ -334,7 +340,8 @@ __device__ __forceinline__ bool ray_more(const RayUniforms& u, float T, float t_
 template <int KB>
 __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__ views, uint32_t n_views,
                                                      uint32_t total_tiles, DevCounters* ctr,
-                                                     const __grid_constant__ FaceTable F) {
+                                                     const __grid_constant__ FaceTable F, const Handoff hand,
+                                                     uint32_t hand_after) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   PacketScratch<KB>& W = *reinterpret_cast<PacketScratch<KB>*>(smem_raw);
   const uint32_t lane = threadIdx.x & 31;
@@ -361,11 +368,28 @@ __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__
     W.dz[lane] = d.z;
     const float t_max = V.u.t_max;
     const uint32_t k = V.u.k;
-    const uint32_t cap = V.kbuf < (uint32_t)KB ? V.kbuf : (uint32_t)KB;
+    const uint32_t cap = V.pkbuf < (uint32_t)KB ? V.pkbuf : (uint32_t)KB;
     float L0 = 0.f, L1 = 0.f, L2 = 0.f, T = 1.f, t_curr = V.u.t_min;
     uint32_t step = 0;
     bool live = valid && ray_more(V.u, T, t_curr, step);
+    bool handed = false;
+    uint32_t n_trav = 0;
     while (__any_sync(kFull, live)) {
+      if (hand.rays && n_trav == hand_after) {
+        // hand the rays that still need hits to the warp-per-ray kernel
+        const uint32_t hm = __ballot_sync(kFull, live);
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&ctr->handoff, (uint32_t)__popc(hm));
+        base = __shfl_sync(kFull, base, 0);
+        const uint32_t idx = base + (uint32_t)__popc(hm & ((1u << lane) - 1u));
+        if (live && idx < hand.cap) {
+          hand.rays[idx] = HandoffRay{32u * tile + lane, step, t_curr, T, L0, L1, L2, 0u};
+          live = false;
+          handed = true;
+        }
+        if (!__any_sync(kFull, live)) break;  // (the buffer may be full: the rest go on here)
+      }
+      ++n_trav;
       packet_traverse<KB>(V.s, F, W, o, br, live, t_curr, t_max, cap, status, lane);
       __syncwarp();
       if (__reduce_or_sync(kFull, status) & (kStatusStackOverflow | kStatusVisitCap | kStatusHitOverflow)) break;
@@ -414,7 +438,7 @@ __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__
       }
       __syncwarp();
     }
-    if (valid) {
+    if (valid && !handed) {
       const float4 r = make_float4(L0, L1, L2, 1.0f);
       float4* dst = V.out + (size_t)py * V.w + px;
       *dst = V.u.aa ? aa_blend(*dst, r, V.u.frames) : r;
@@ -436,14 +460,15 @@ __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__
 
 template <int KB>
 static Err launch_packet_kb(const ViewDev* d_views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
-                            const FaceTable& faces, int num_sms, cudaStream_t stream, uint64_t* launches) {
+                            const FaceTable& faces, int num_sms, cudaStream_t stream, uint64_t* launches,
+                            const Handoff& hand, uint32_t hand_after) {
   const size_t smem = sizeof(PacketScratch<KB>);
   GT_CUDA_TRY(cudaFuncSetAttribute(k_trace_packet<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   GT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_packet<KB>, 32, smem));
   uint32_t grid = (uint32_t)num_sms * (uint32_t)std::max(1, per_sm);
   if (grid > total_tiles) grid = std::max(1u, total_tiles);
-  k_trace_packet<KB><<<grid, 32, smem, stream>>>(d_views, n_views, total_tiles, counters, faces);
+  k_trace_packet<KB><<<grid, 32, smem, stream>>>(d_views, n_views, total_tiles, counters, faces, hand, hand_after);
   ++*launches;
   GT_CUDA_TRY(cudaGetLastError());
   return Err{};
@@ -451,13 +476,20 @@ static Err launch_packet_kb(const ViewDev* d_views, uint32_t n_views, uint32_t t
 
 Err launch_trace_packet(const ViewDev* views, const ViewDev* d_views, uint32_t n_views, uint32_t total_tiles,
                         DevCounters* counters, const FaceTable& faces, int num_sms, cudaStream_t stream,
-                        uint64_t* launches) {
+                        uint64_t* launches, const Handoff& hand, uint32_t hand_after) {
   uint32_t kmax = 1;
-  for (uint32_t i = 0; i < n_views; ++i) kmax = std::max(kmax, views[i].kbuf);
-  if (kmax <= 24) return launch_packet_kb<24>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches);
-  if (kmax <= 32) return launch_packet_kb<32>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches);
-  if (kmax <= 48) return launch_packet_kb<48>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches);
-  return launch_packet_kb<64>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches);
+  for (uint32_t i = 0; i < n_views; ++i) kmax = std::max(kmax, views[i].pkbuf);
+  if (kmax <= 24)
+    return launch_packet_kb<24>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches, hand,
+                                hand_after);
+  if (kmax <= 32)
+    return launch_packet_kb<32>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches, hand,
+                                hand_after);
+  if (kmax <= 48)
+    return launch_packet_kb<48>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches, hand,
+                                hand_after);
+  return launch_packet_kb<64>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches, hand,
+                              hand_after);
 }
 
 }  // namespace gt

@@ -51,10 +51,12 @@ __device__ __forceinline__ bool wray_more(const ViewDev& V, const WRay& R) {
 // DEBUG: also handle debugMode 1 and 2.  Launches whose views all render
 // (debugMode 0) use the instantiation without them: their extra traversal
 // copies cost the render loop registers and spills (4.7 % of its time).
+// init: the state of a ray handed over by a tile packet (nullptr: a new ray).
 template <bool RECORD, bool CKPT, int NB, bool DEBUG>
 __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTable& F, WarpScratch& W, uint32_t px,
                                                  uint32_t py, RayStats& st, uint32_t& status, uint32_t lane,
-                                                 const HitOut& ho, uint32_t slot, const Ckpt& ck) {
+                                                 const HitOut& ho, uint32_t slot, const Ckpt& ck,
+                                                 const HandoffRay* init) {
   WRay R;
   ray_gen(V.u, V.w, V.h, px, py, R.o, R.d);
   R.br = make_boxray(R.o, R.d, V.s.scene_mag);
@@ -106,6 +108,14 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
   R.t_curr = V.u.t_min;
   R.step = 0;
   R.n_entries = 0;
+  if (!RECORD && !CKPT && init) {
+    R.L0 = init->L0;
+    R.L1 = init->L1;
+    R.L2 = init->L2;
+    R.T = init->T;
+    R.t_curr = init->t_curr;
+    R.step = init->step;
+  }
   const uint32_t k = V.u.k;
   uint32_t ck_head = kInvalid;
   while (wray_more(V, R)) {
@@ -255,7 +265,10 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
 
 // Persistent kernel: each warp takes one pixel slot at a time from a global
 // counter (slot = 32 * tile + position in the 8x4 tile, views back to back),
-// so neighbouring pixels run on neighbouring warps at the same time.
+// so neighbouring pixels run on neighbouring warps at the same time.  With
+// `resume`, the slots are instead the rays a tile-packet launch handed over
+// (DevCounters::handoff of them, at most resume_cap), continued from their
+// state.
 // 8 resident blocks (32 warps per SM, 64 registers a thread) beat 4 blocks
 // without spills by 12% on the 1M-Gaussian 1080p view: the kernel is bound by
 // dependent latencies, and more warps hide them better than the spill loads
@@ -265,7 +278,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) k_trace8(const ViewDev
                                                                   uint32_t total_tiles, DevCounters* ctr,
                                                                   const __grid_constant__ FaceTable F,
                                                                   const uint32_t* pixels, uint32_t n_pix,
-                                                                  const HitOut ho, const Ckpt ck) {
+                                                                  const HitOut ho, const Ckpt ck,
+                                                                  const HandoffRay* resume, uint32_t resume_cap) {
   __shared__ WarpScratch scratch[kWarpsPerBlock];
   const uint32_t lane = threadIdx.x & 31;
   WarpScratch& W = scratch[threadIdx.x >> 5];
@@ -273,12 +287,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) k_trace8(const ViewDev
   if (lane == 0) st = RayStats{0, 0, 0, 0, 0, 0};
   __syncwarp();
   uint32_t status = 0, rays = 0;
-  const uint32_t total = RECORD ? n_pix : total_tiles * 32u;
+  const uint32_t total = RECORD ? n_pix : (resume ? min(ctr->handoff, resume_cap) : total_tiles * 32u);
   while (true) {
     uint32_t item = 0;
-    if (lane == 0) item = atomicAdd(&ctr->work, 1u);
+    if (lane == 0) item = atomicAdd(resume ? &ctr->work2 : &ctr->work, 1u);
     item = __shfl_sync(kFull, item, 0);
     if (item >= total) break;
+    const HandoffRay* init = nullptr;
+    if (!RECORD && !CKPT && resume) {
+      init = resume + item;
+      item = init->item;
+    }
     uint32_t vi = 0, px, py;
     if (RECORD) {
       uint32_t pix = pixels[item];
@@ -302,7 +321,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) k_trace8(const ViewDev
       vu[7] = item;
     }
     const float4 r = trace_ray_warp<RECORD, CKPT, NB, DEBUG>(views[vi], F, W, px, py, st, status, lane, ho, item,
-                                                            ck);
+                                                            ck, init);
     {
       __syncwarp();
       volatile uint32_t* vu = W.ru;
@@ -336,23 +355,26 @@ bool packet_launch(const ViewDev* views, uint32_t n_views, uint32_t total_tiles,
   return (uint64_t)total_tiles >= (uint64_t)kPacketTilesPerSm * (uint64_t)std::max(1, num_sms);
 }
 
-void apply_shape(ViewDev* views, uint32_t n_views, const LaunchShape& shape, bool packet) {
+void apply_shape(ViewDev* views, uint32_t n_views, const LaunchShape& shape) {
   for (uint32_t i = 0; i < n_views; ++i) {
-    uint32_t kb = packet ? std::min(kMaxPacketKbuf, std::max(shape.packet_kbuf, views[i].u.k))
-                         : std::min(kMaxKbuf, std::max(shape.kbuf, views[i].u.k));
-    views[i].kbuf = std::max(1u, kb);
+    views[i].kbuf = std::max(1u, std::min(kMaxKbuf, std::max(shape.kbuf, views[i].u.k)));
+    views[i].pkbuf = std::max(1u, std::min(kMaxPacketKbuf, std::max(shape.packet_kbuf, views[i].u.k)));
     views[i].leaf_batch = std::min(32u, std::max(1u, shape.leaf_batch));
   }
 }
 
 Err launch_trace(ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
                  const FaceTable& faces, const LaunchShape& shape, int num_sms, cudaStream_t stream,
-                 uint64_t* launches, ViewDev* d_views, const Ckpt* ckpt) {
+                 uint64_t* launches, ViewDev* d_views, const Ckpt* ckpt, const Handoff* handoff) {
   const bool packet = packet_launch(views, n_views, total_tiles, num_sms, shape, ckpt != nullptr);
-  apply_shape(views, n_views, shape, packet);
+  apply_shape(views, n_views, shape);
   GT_CUDA_TRY(cudaMemcpyAsync(d_views, views, sizeof(ViewDev) * n_views, cudaMemcpyHostToDevice, stream));
-  if (packet)
-    return launch_trace_packet(views, d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches);
+  const bool hand = packet && handoff && handoff->rays && handoff->cap && shape.handoff_after;
+  if (packet) {
+    Err e = launch_trace_packet(views, d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches,
+                                hand ? *handoff : Handoff{}, shape.handoff_after);
+    if (e.code != GT_OK || !hand) return e;
+  }
   uint32_t block = kWarpsPerBlock * 32;
   uint32_t grid = (uint32_t)num_sms * std::max(1u, shape.blocks_per_sm);
   uint64_t warps_needed = (uint64_t)total_tiles * 32u;
@@ -385,8 +407,12 @@ Err launch_trace(ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCoun
   const ViewDev* dv = d_views;
   const uint32_t* no_pix = nullptr;
   uint32_t zero = 0;
+  // after a tile-packet launch: the rays it handed over, one warp per ray
+  const HandoffRay* resume = hand ? handoff->rays : nullptr;
+  const uint32_t resume_cap = hand ? handoff->cap : 0u;
+  if (hand) grid = (uint32_t)num_sms * std::max(1u, shape.blocks_per_sm);
   void* args[] = {(void*)&dv, (void*)&n_views, (void*)&total_tiles, (void*)&counters, (void*)&faces,
-                  (void*)&no_pix, (void*)&zero, (void*)&ho, (void*)&ck};
+                  (void*)&no_pix, (void*)&zero, (void*)&ho, (void*)&ck, (void*)&resume, (void*)&resume_cap};
   GT_CUDA_TRY(cudaLaunchKernel(fn, dim3(grid), dim3(block), args, 0, stream));
   ++*launches;
   GT_CUDA_TRY(cudaGetLastError());
@@ -402,7 +428,7 @@ Err launch_trace_hits(const ViewDev& view, ViewDev* d_views, const uint32_t* pix
   HitOut ho{out_pidx, out_t, out_alpha, out_count, out_rounds, out_rgba, max_entries};
   uint32_t grid = std::min<uint32_t>((n_pix + kWarpsPerBlock - 1) / kWarpsPerBlock, 148u * 8u);
   k_trace8<true, false, 1, true><<<grid, kWarpsPerBlock * 32, 0, stream>>>(d_views, 1, 0, counters, faces, pixels, n_pix, ho,
-                                                                  Ckpt{});
+                                                                  Ckpt{}, nullptr, 0u);
   ++*launches;
   GT_CUDA_TRY(cudaGetLastError());
   return Err{};
