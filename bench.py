@@ -453,7 +453,9 @@ def main():
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "alg_bytes_per_launch": alg_bytes, "kernel_ms": k_ms},
+                         "alg_bytes_per_launch": alg_bytes, "kernel_ms": k_ms,
+                         "timed": "a render's trace launches (large views: the tile-packet kernel and the "
+                                  "warp-per-ray launch that finishes the rays it hands over)"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": 112 + 256,
                     "d2h_bytes_per_step": rays * 16},
