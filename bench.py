@@ -305,6 +305,8 @@ def extra_batched_fwd_bwd(ctx, pg, amin, reps: int = 1):
         its[i].w, its[i].h = w_, h_
         its[i].out_rgba = p_
 
+    info = {}
+
     def step():
         flags = L.GT_FLAG_OUTPUT_DEVICE | L.GT_FLAG_CHECKPOINT
         ctx.check(lib.gt_render_batch(ctx.handle, its, len(views), flags, None))
@@ -314,6 +316,11 @@ def extra_batched_fwd_bwd(ctx, pg, amin, reps: int = 1):
         ctx.check(lib.gt_backward_batch(ctx.handle, bitems, len(views), sc, op, 1,
                                         L.GT_FLAG_INPUT_DEVICE | L.GT_FLAG_OUTPUT_DEVICE | L.GT_FLAG_CHECKPOINT,
                                         C.byref(opts), None))
+        info.update(used_mode=opts.used_mode, bwd_ms=opts.bwd_ms)
+
+    def fwd_ckpt():
+        flags = L.GT_FLAG_OUTPUT_DEVICE | L.GT_FLAG_CHECKPOINT
+        ctx.check(lib.gt_render_batch(ctx.handle, its, len(views), flags, None))
     def plain():
         for s_, u_, w_, h_, p_ in items:
             ctx.render_device(s_, u_, w_, h_, p_, asynchronous=True)
@@ -321,12 +328,15 @@ def extra_batched_fwd_bwd(ctx, pg, amin, reps: int = 1):
     plain()
     tfb = _time_device(ctx, step, reps)
     tp = _time_device(ctx, plain, reps)
+    tfc = _time_device(ctx, fwd_ckpt, reps)
     for p in imgs + tgts + dls + [gout]:
         ctx.device_free(p)
     scene.close()
     target.close()
     return {"workload": "1M Gaussians (64 clusters), 32 views 640x480-1920x1080, k=16, L2 loss vs perturbed scene",
-            "rays": rays, "batched_fwd_bwd_ms": tfb, "plain_fwd_ms": tp, "ratio": tfb / tp}
+            "rays": rays, "batched_fwd_bwd_ms": tfb, "plain_fwd_ms": tp, "ratio": tfb / tp,
+            "checkpoint_fwd_ms": tfc, "adjoint_ms": info.get("bwd_ms"),
+            "mode": "checkpoint" if info.get("used_mode") == 1 else "replay"}
 
 
 def main():

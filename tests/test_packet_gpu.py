@@ -109,3 +109,27 @@ def test_batch_of_views_and_scenes(ctx):
         ref, _ = (oa if sc is ga else ob).render(u, w, h)
         assert np.array_equal(_bits(out), ref.view(np.uint32))
     assert st["rays"] == 37 * 21 + 24 * 40 + 16 * 16
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_checkpointing_forward_and_gradients(ctx, mode):
+    """gt_backward's checkpointing forward as tile packets (with rays handed
+    to the warp-per-ray kernel after three traversals): the image is the
+    oracle's and the gradients match the FP64 oracle's adjoint."""
+    from test_backward_gpu import _check, _ref_grad
+    pg = small_scene(n=4000, seed=57)
+    rec = pg.gaussiansBuffer
+    w, h = 48, 40
+    v = view(w, h, k=6, T_min=0.001)
+    s = Scene(ctx, rec, 0.01)
+    ctx.set_tune(s, v.uniforms, w, h, kbuf=32, block_threads=32)
+    try:
+        img = ctx.render(s, v.uniforms, w, h, checkpoint=True)
+        ref, _ = oracle.Scene(rec, 0.01, "f32").render(v.uniforms, w, h)
+        assert np.array_equal(_bits(img), ref.view(np.uint32))
+        g = np.random.default_rng(11).normal(size=(h, w, 4)).astype(np.float32)
+        got, info = ctx.backward(s, v.uniforms, w, h, g, mode=mode)
+    finally:
+        ctx._lib.gt_autotune_reset(ctx._h)
+    assert info["used_mode"] == mode
+    _check(got, _ref_grad(rec, 0.01, v.uniforms, w, h, g))

@@ -412,6 +412,9 @@ gt_status api_forward_ckpt(gt_context* ctx, const gt_scene* const* scenes, const
   sst = grow(ctx, (void**)&ck.head, &ck.head_bytes, slots * 4);
   if (sst != GT_OK) return sst;
   LaunchShape shape = api_shape_for(ctx, scenes[0], ws[0], hs[0], us[0].k);
+  Handoff hand;
+  sst = api_ensure_handoff(ctx, rays, &hand);
+  if (sst != GT_OK) return sst;
   for (int attempt = 0; attempt < 3; ++attempt) {
     if (want > 0xFFFFFFF0ull) return api_fail(ctx, GT_ERR_OOM, "checkpoint needs more than 2^32 round records");
     uint32_t m = mode == 1 ? 1u : (mode == 2 ? 2u : (want * (kCkptHeader + kmax) * 4 <= budget ? 1u : 2u));
@@ -429,7 +432,7 @@ gt_status api_forward_ckpt(gt_context* ctx, const gt_scene* const* scenes, const
     CK_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), st));
     CK_TRY(cudaEventRecord(ctx->int0, st));
     Err e = launch_trace(vd.data(), count, total_tiles, ctx->d_ctr, ctx->faces, shape, ctx->num_sms, st,
-                         &ctx->launches, ctx->d_views, &c);
+                         &ctx->launches, ctx->d_views, &c, &hand);
     if (e.code != GT_OK) return api_fail(ctx, e.code, e.msg);
     CK_TRY(cudaEventRecord(ctx->int1, st));
     uint32_t used = 0;

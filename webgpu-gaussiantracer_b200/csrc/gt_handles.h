@@ -91,6 +91,7 @@ ViewDev api_make_view(const gt_scene* s, const gt_uniforms& u, uint32_t w, uint3
 LaunchShape api_shape_for(gt_context* ctx, const gt_scene* s, uint32_t w, uint32_t h, uint32_t k);
 void api_fill_stats(const DevCounters& c, gt_render_stats* st);
 gt_status api_ensure_views(gt_context* ctx, uint32_t n);
+gt_status api_ensure_handoff(gt_context* ctx, uint64_t rays, Handoff* out);
 // Checkpointing forward (gt_backward.cu): renders the views into `outs`
 // (device, one per view) and keeps the round checkpoint in ctx->ckpt.
 gt_status api_forward_ckpt(gt_context* ctx, const gt_scene* const* scenes, const gt_uniforms* us, const uint32_t* ws,

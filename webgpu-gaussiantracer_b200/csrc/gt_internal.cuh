@@ -238,7 +238,7 @@ constexpr uint32_t kCkptHeader = 4;
 struct HandoffRay {
   uint32_t item, step;
   float t_curr, T, L0, L1, L2;
-  uint32_t pad;
+  uint32_t ck_head;  // checkpointing launches: the ray's last round record
 };
 // The handoff buffer of a launch (rays == nullptr: no handoff).
 struct Handoff {
@@ -259,7 +259,8 @@ Err launch_trace(ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCoun
                  const Handoff* handoff = nullptr);
 Err launch_trace_packet(const ViewDev* views, const ViewDev* d_views, uint32_t n_views, uint32_t total_tiles,
                         DevCounters* counters, const FaceTable& faces, int num_sms, cudaStream_t stream,
-                        uint64_t* launches, const Handoff& handoff, uint32_t handoff_after);
+                        uint64_t* launches, const Handoff& handoff, uint32_t handoff_after,
+                        const Ckpt* ckpt = nullptr);
 Err launch_trace_hits(const ViewDev& view, ViewDev* d_views, const uint32_t* pixels, uint32_t n_pix,
                       uint32_t max_entries, uint32_t* out_pidx, float* out_t, float* out_alpha, uint32_t* out_count,
                       uint32_t* out_rounds, float4* out_rgba, DevCounters* counters, const FaceTable& faces,

@@ -33,7 +33,9 @@
 //     After handoff_after traversals a packet writes its rays that still
 //     need hits (their compositing state between two rounds) to a buffer,
 //     and the warp-per-ray kernel, launched next, finishes them; the
-//     arithmetic of every round is the same in both kernels.
+//     arithmetic of every round is the same in both kernels;
+//   * checkpoint (for gt_backward): each round's record (t_curr, T, the
+//     ray's previous record, the entries) as k_trace8 writes it.
 #include <math_constants.h>
 
 #include "gt_device.cuh"
@@ -337,11 +339,13 @@ __device__ __forceinline__ bool ray_more(const RayUniforms& u, float T, float t_
 
 // Persistent kernel: each warp takes one 8x4 tile at a time from a global
 // counter (tiles of all views back to back) and traces its 32 rays.
-template <int KB>
+// CKPT: write the round checkpoint the adjoint replays (gt_backward), with
+// the layout and slot numbering of k_trace8's.
+template <int KB, bool CKPT>
 __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__ views, uint32_t n_views,
                                                      uint32_t total_tiles, DevCounters* ctr,
                                                      const __grid_constant__ FaceTable F, const Handoff hand,
-                                                     uint32_t hand_after) {
+                                                     uint32_t hand_after, const Ckpt ck) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   PacketScratch<KB>& W = *reinterpret_cast<PacketScratch<KB>*>(smem_raw);
   const uint32_t lane = threadIdx.x & 31;
@@ -374,6 +378,7 @@ __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__
     bool live = valid && ray_more(V.u, T, t_curr, step);
     bool handed = false;
     uint32_t n_trav = 0;
+    uint32_t ck_head = kInvalid;
     while (__any_sync(kFull, live)) {
       if (hand.rays && n_trav == hand_after) {
         // hand the rays that still need hits to the warp-per-ray kernel
@@ -383,7 +388,7 @@ __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__
         base = __shfl_sync(kFull, base, 0);
         const uint32_t idx = base + (uint32_t)__popc(hm & ((1u << lane) - 1u));
         if (live && idx < hand.cap) {
-          hand.rays[idx] = HandoffRay{32u * tile + lane, step, t_curr, T, L0, L1, L2, 0u};
+          hand.rays[idx] = HandoffRay{32u * tile + lane, step, t_curr, T, L0, L1, L2, ck_head};
           live = false;
           handed = true;
         }
@@ -393,17 +398,52 @@ __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__
       packet_traverse<KB>(V.s, F, W, o, br, live, t_curr, t_max, cap, status, lane);
       __syncwarp();
       if (__reduce_or_sync(kFull, status) & (kStatusStackOverflow | kStatusVisitCap | kStatusHitOverflow)) break;
+      // the rounds each live ray's buffer serves, warp-synchronously (one
+      // record allocation a round for the whole warp when checkpointing)
+      uint32_t cnt = 0, head = 0;
+      bool complete = false, rounds_on = live;
       if (live) {
-        const uint32_t cnt = W.hn[lane];
-        const bool complete = cnt < cap;  // every hit beyond t_curr is in the buffer
+        cnt = W.hn[lane];
+        complete = cnt < cap;  // every hit beyond t_curr is in the buffer
         heap_sort(W, lane, cnt);
-        uint32_t head = 0;
-        while (ray_more(V.u, T, t_curr, step)) {
-          while (head < cnt && !(key_t(W.hk[head][lane]) > t_curr)) ++head;
-          const uint32_t avail = cnt - head;
-          if (!complete && avail < k) break;  // the next round reaches past the buffer
-          const uint32_t n = avail < k ? avail : k;
-          const float new_t = n == k ? key_t(W.hk[head + k - 1][lane]) + 1e-4f : t_max;
+      }
+      while (true) {
+        bool act = false;
+        uint32_t n = 0;
+        float new_t = t_max;
+        if (rounds_on) {
+          if (!ray_more(V.u, T, t_curr, step)) {
+            rounds_on = false;
+          } else {
+            while (head < cnt && !(key_t(W.hk[head][lane]) > t_curr)) ++head;
+            const uint32_t avail = cnt - head;
+            if (!complete && avail < k) {
+              rounds_on = false;  // the next round reaches past the buffer
+            } else {
+              n = avail < k ? avail : k;
+              new_t = n == k ? key_t(W.hk[head + k - 1][lane]) + 1e-4f : t_max;
+              act = true;
+            }
+          }
+        }
+        const uint32_t am = __ballot_sync(kFull, act);
+        if (am == 0) break;
+        if (CKPT) {
+          uint32_t base = 0;
+          if (lane == 0) base = atomicAdd(ck.pool_next, (uint32_t)__popc(am));
+          base = __shfl_sync(kFull, base, 0);
+          const uint32_t rec = base + (uint32_t)__popc(am & ((1u << lane) - 1u));
+          if (act && rec < ck.pool_cap) {  // past the pool the host sizes it up and runs again
+            uint32_t* r = ck.pool + (size_t)rec * (kCkptHeader + ck.kc);
+            r[0] = __float_as_uint(t_curr);
+            r[1] = __float_as_uint(T);
+            r[2] = ck_head;
+            r[3] = n;
+            for (uint32_t e = 0; e < ck.kc; ++e) r[kCkptHeader + e] = e < n ? key_p(W.hk[head + e][lane]) : kInvalid;
+            ck_head = rec;
+          }
+        }
+        if (act) {
           ++step;
           ++n_rounds;
           n_entries += n;
@@ -434,10 +474,13 @@ __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__
             t_curr = t_max;
           }
         }
+      }
+      if (live) {
         live = ray_more(V.u, T, t_curr, step);
       }
       __syncwarp();
     }
+    if (CKPT && valid && !handed) ck.head[32u * tile + lane] = ck_head;
     if (valid && !handed) {
       const float4 r = make_float4(L0, L1, L2, 1.0f);
       float4* dst = V.out + (size_t)py * V.w + px;
@@ -458,38 +501,51 @@ __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__
   flush_stats(ctr, W.stats, lane == 0 ? s_rays : 0u, status);
 }
 
-template <int KB>
+template <int KB, bool CKPT>
 static Err launch_packet_kb(const ViewDev* d_views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
                             const FaceTable& faces, int num_sms, cudaStream_t stream, uint64_t* launches,
-                            const Handoff& hand, uint32_t hand_after) {
+                            const Handoff& hand, uint32_t hand_after, const Ckpt& ck) {
   const size_t smem = sizeof(PacketScratch<KB>);
-  GT_CUDA_TRY(cudaFuncSetAttribute(k_trace_packet<KB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  GT_CUDA_TRY(
+      cudaFuncSetAttribute(k_trace_packet<KB, CKPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
-  GT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_packet<KB>, 32, smem));
+  GT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_trace_packet<KB, CKPT>, 32, smem));
   uint32_t grid = (uint32_t)num_sms * (uint32_t)std::max(1, per_sm);
   if (grid > total_tiles) grid = std::max(1u, total_tiles);
-  k_trace_packet<KB><<<grid, 32, smem, stream>>>(d_views, n_views, total_tiles, counters, faces, hand, hand_after);
+  k_trace_packet<KB, CKPT><<<grid, 32, smem, stream>>>(d_views, n_views, total_tiles, counters, faces, hand,
+                                                       hand_after, ck);
   ++*launches;
   GT_CUDA_TRY(cudaGetLastError());
   return Err{};
 }
 
+template <int KB>
+static Err launch_packet_k(const ViewDev* d_views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
+                           const FaceTable& faces, int num_sms, cudaStream_t stream, uint64_t* launches,
+                           const Handoff& hand, uint32_t hand_after, const Ckpt* ckpt) {
+  if (ckpt)
+    return launch_packet_kb<KB, true>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches,
+                                      hand, hand_after, *ckpt);
+  return launch_packet_kb<KB, false>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches,
+                                     hand, hand_after, Ckpt{});
+}
+
 Err launch_trace_packet(const ViewDev* views, const ViewDev* d_views, uint32_t n_views, uint32_t total_tiles,
                         DevCounters* counters, const FaceTable& faces, int num_sms, cudaStream_t stream,
-                        uint64_t* launches, const Handoff& hand, uint32_t hand_after) {
+                        uint64_t* launches, const Handoff& hand, uint32_t hand_after, const Ckpt* ckpt) {
   uint32_t kmax = 1;
   for (uint32_t i = 0; i < n_views; ++i) kmax = std::max(kmax, views[i].pkbuf);
   if (kmax <= 24)
-    return launch_packet_kb<24>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches, hand,
-                                hand_after);
+    return launch_packet_k<24>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches, hand,
+                               hand_after, ckpt);
   if (kmax <= 32)
-    return launch_packet_kb<32>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches, hand,
-                                hand_after);
+    return launch_packet_k<32>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches, hand,
+                               hand_after, ckpt);
   if (kmax <= 48)
-    return launch_packet_kb<48>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches, hand,
-                                hand_after);
-  return launch_packet_kb<64>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches, hand,
-                              hand_after);
+    return launch_packet_k<48>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches, hand,
+                               hand_after, ckpt);
+  return launch_packet_k<64>(d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches, hand,
+                             hand_after, ckpt);
 }
 
 }  // namespace gt

@@ -108,16 +108,17 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
   R.t_curr = V.u.t_min;
   R.step = 0;
   R.n_entries = 0;
-  if (!RECORD && !CKPT && init) {
+  uint32_t ck_head = kInvalid;
+  if (!RECORD && init) {
     R.L0 = init->L0;
     R.L1 = init->L1;
     R.L2 = init->L2;
     R.T = init->T;
     R.t_curr = init->t_curr;
     R.step = init->step;
+    ck_head = init->ck_head;
   }
   const uint32_t k = V.u.k;
-  uint32_t ck_head = kInvalid;
   while (wray_more(V, R)) {
     // one traversal: the kbuf closest front-face hits with t > t_curr
     KBuf<NB> kb;
@@ -294,7 +295,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 8) k_trace8(const ViewDev
     item = __shfl_sync(kFull, item, 0);
     if (item >= total) break;
     const HandoffRay* init = nullptr;
-    if (!RECORD && !CKPT && resume) {
+    if (!RECORD && resume) {
       init = resume + item;
       item = init->item;
     }
@@ -348,7 +349,8 @@ uint32_t kmax_for(uint32_t k) { return k <= 8 ? 8u : (k <= 16 ? 16u : 32u); }
 
 bool packet_launch(const ViewDev* views, uint32_t n_views, uint32_t total_tiles, int num_sms,
                    const LaunchShape& shape, bool ckpt) {
-  if (!shape.packet || ckpt) return false;
+  (void)ckpt;  // the tile packets write the checkpoint as well
+  if (!shape.packet) return false;
   for (uint32_t i = 0; i < n_views; ++i)
     if (views[i].u.debug != 0) return false;
   if (shape.packet == 1) return true;
@@ -372,7 +374,7 @@ Err launch_trace(ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCoun
   const bool hand = packet && handoff && handoff->rays && handoff->cap && shape.handoff_after;
   if (packet) {
     Err e = launch_trace_packet(views, d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches,
-                                hand ? *handoff : Handoff{}, shape.handoff_after);
+                                hand ? *handoff : Handoff{}, shape.handoff_after, ckpt);
     if (e.code != GT_OK || !hand) return e;
   }
   uint32_t block = kWarpsPerBlock * 32;
