@@ -387,8 +387,9 @@ gt_status gt_l2_loss(gt_context* ctx, const float* rgba, const float* target, ui
  * second otherwise: tiles are coarse work items, and with few of them per
  * warp the slowest ones decide the time.  With the first kernel, the rays
  * of a tile that still need hits after three traversals are finished by
- * the second one (a second launch).  Debug modes, hit recording and the
- * checkpointing forward of gt_backward always use the second kernel. */
+ * the second one (a second launch).  The same choice holds for the
+ * checkpointing forward of gt_backward; debug modes and hit recording
+ * always use the second kernel. */
 typedef struct gt_tune_result {
   uint32_t block_threads; /* 32: a warp per 8x4 tile; 128: a warp per ray      */
   uint32_t blocks_per_sm; /* resident blocks per SM of the persistent grid      */
