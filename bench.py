@@ -147,6 +147,11 @@ def make_workload(name: str):
         pg, amin, v = synth.clusters_1m_config()
         v = synth.view(480, 270, (0.0, 0.0, 12.0), k=16)
         desc = "1M Gaussians (64 clusters), 480x270 (profiling size), k=16, alpha_min=0.01, T_min=0.01, SH3"
+    elif name == "clusters-1m-960x540":
+        pg, amin, v = synth.clusters_1m_config()
+        v = synth.view(960, 540, (0.0, 0.0, 12.0), k=16)
+        desc = ("1M Gaussians (64 clusters), 960x540 (profiling size of the tile-packet kernel), k=16, "
+                "alpha_min=0.01, T_min=0.01, SH3")
     elif name == "small-256":
         pg, amin, v = synth.small_config()
         desc = "16,384 Gaussians (uniform), 256x256, k=6, alpha_min=0.01, T_min=0.01, SH3, camera at distance 4"
