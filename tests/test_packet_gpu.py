@@ -133,3 +133,16 @@ def test_checkpointing_forward_and_gradients(ctx, mode):
         ctx._lib.gt_autotune_reset(ctx._h)
     assert info["used_mode"] == mode
     _check(got, _ref_grad(rec, 0.01, v.uniforms, w, h, g))
+
+
+@pytest.mark.parametrize("pos", [(0.0, 0.0, 40.0), (0.3, 0.2, 0.9), (2.5, -1.5, 2.0)])
+def test_entry_face_test_across_distances(ctx, pos):
+    """Near and far cameras (object-space origins from ~1 to ~10^4 proxy
+    radii): the tile packets give the oracle's image, bit for bit."""
+    pg = small_scene(n=6000, seed=58)
+    g = Scene(ctx, pg.gaussiansBuffer, 0.01)
+    o = oracle.Scene(pg.gaussiansBuffer, 0.01, "f32")
+    v = view(56, 44, pos=pos, k=8, T_min=0.001)
+    img = _packet_render(ctx, g, v.uniforms, 56, 44)
+    ref, _ = o.render(v.uniforms, 56, 44)
+    assert np.array_equal(_bits(img), ref.view(np.uint32))
