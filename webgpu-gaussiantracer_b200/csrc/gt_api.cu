@@ -71,11 +71,12 @@ static void drop_graphs(gt_context* ctx) {
   ctx->graphs.clear();
 }
 
-// Handoff buffer for a launch of `rays` rays: room for a quarter of them (a
-// packet whose rays do not fit keeps tracing them itself).
+// Handoff buffer for a launch of `rays` rays: room for a quarter of them, at
+// most 4M rays (128 MB); a packet whose rays do not fit keeps tracing them
+// itself, so the cap changes only how the tail of a large batch is shared.
 static gt_status ensure_handoff(gt_context* ctx, uint64_t rays, Handoff* out) {
   const uint64_t want64 = std::max<uint64_t>(4096, rays / 4);
-  const uint32_t want = (uint32_t)std::min<uint64_t>(want64, 1u << 28);
+  const uint32_t want = (uint32_t)std::min<uint64_t>(want64, 1u << 22);
   if (want > ctx->handoff_cap) {
     // captured graphs hold the old buffer address
     cudaStreamSynchronize(ctx->stream);
