@@ -2,12 +2,15 @@
 against the oracle on the cases the other parity tests cover with the
 default choice.  At test image sizes the default is the warp-per-ray kernel,
 so every case here installs block_threads = 32 for its view first
-(gt_set_tune); the results must be the oracle's, bit for bit."""
+(gt_set_tune); the results must be the oracle's, bit for bit.  The last
+test renders the full-size batched configuration, where the default is the
+tile packets."""
 import numpy as np
 import pytest
 
 from conftest import small_scene, view
 from oracle import oracle
+from gtrace import synth
 from gtrace.tracer import Scene
 from gtrace.uniforms import with_fields
 
@@ -146,3 +149,28 @@ def test_entry_face_test_across_distances(ctx, pos):
     img = _packet_render(ctx, g, v.uniforms, 56, 44)
     ref, _ = o.render(v.uniforms, 56, 44)
     assert np.array_equal(_bits(img), ref.view(np.uint32))
+
+
+def test_batched_config_full_size_equals_single_renders(ctx):
+    """The batched configuration at full size (8 scenes of 100k-1M Gaussians,
+    64 views up to 1920x1080, 44.7M rays in one launch: tile packets, and a
+    handoff buffer that fills up): every view equals its own single render
+    bit for bit."""
+    raw_scenes, views = synth.batched_scenes_config()
+    scenes = [Scene(ctx, synth.pack(raw).gaussiansBuffer, amin) for raw, amin in raw_scenes]
+    items = []
+    try:
+        for s, w, h, pos in views:
+            v = synth.view(w, h, pos, k=16, alpha_min=raw_scenes[s][1])
+            items.append((scenes[s], v.uniforms, w, h, ctx.device_alloc(w * h * 16)))
+        _, st = ctx.render_batch(items, device_outputs=True)
+        assert st["rays"] == sum(w * h for _, _, w, h, _ in items)
+        for sc, u, w, h, ptr in items:
+            got = np.zeros((h, w, 4), np.float32)
+            ctx.memcpy(got.ctypes.data, ptr, w * h * 16, 1)
+            assert np.array_equal(_bits(got), _bits(ctx.render(sc, u, w, h)))
+    finally:
+        for it in items:
+            ctx.device_free(it[4])
+        for s in scenes:
+            s.close()
