@@ -2,8 +2,9 @@
 file data/pc_short.ply (100 SH-3 Gaussians) through gtrace.ply.PackedGaussians,
 cross-checked against the oracle's C restatement of the same loader.
 
-Run in a checkout where the reference is mounted:
-    python tests/golden/make_golden.py /root/reference/data/pc_short.ply
+Run with the path of that file (in the reference's checkout) as the argument
+or in the GTRACE_REFERENCE_PLY environment variable:
+    python tests/golden/make_golden.py <reference checkout>/data/pc_short.ply
 """
 import json
 import os
@@ -36,4 +37,7 @@ def main(path):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/data/pc_short.ply")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GTRACE_REFERENCE_PLY", "")
+    if not src:
+        raise SystemExit("usage: make_golden.py <reference checkout>/data/pc_short.ply")
+    main(src)

@@ -14,7 +14,8 @@ from gtrace.uniforms import look_at, pack_uniforms, unpack_uniforms
 from gtrace import synth
 
 HEADER = os.path.join(ROOT, "include", "gtrace.h")
-REF_PLY = "/root/reference/data/pc_short.ply"
+# the reference's sample file (data/pc_short.ply of its checkout), when available
+REF_PLY = os.environ.get("GTRACE_REFERENCE_PLY", "")
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
@@ -36,8 +37,10 @@ def test_library_exports_every_declared_symbol():
 
 def test_version_and_struct_layouts():
     lib = L.load()
-    assert lib.gt_version() == 1
+    assert lib.gt_version() == 2
     assert C.sizeof(L.Uniforms) == 112
+    assert C.sizeof(L.TuneResult) == 40 and L.TuneResult.handoff_after.offset == 32
+    assert C.sizeof(L.SceneInfo) == 64 and L.SceneInfo.upload_ms.offset == 60
     assert L.Uniforms.k.offset == 88 and L.Uniforms.debug_mode.offset == 104
     assert L.Uniforms.camera_aspect.offset == 64 and L.Uniforms.T_min.offset == 80
 
@@ -121,7 +124,7 @@ def test_lower_sh_degree_stride():
     assert pg.sphericalHarmonicsDegree == 1 and pg.gaussiansBuffer.shape == (3, (64 + 16 * 4) // 4)
 
 
-@pytest.mark.skipif(not os.path.exists(REF_PLY), reason="reference sample data not mounted")
+@pytest.mark.skipif(not (REF_PLY and os.path.exists(REF_PLY)), reason="GTRACE_REFERENCE_PLY not set")
 def test_reference_sample_ply_golden():
     """The reference's own sample file (data/pc_short.ply, 100 SH-3 Gaussians)
     ingests to the committed golden summary (tests/golden/make_golden.py)."""

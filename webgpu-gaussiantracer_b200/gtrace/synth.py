@@ -153,3 +153,18 @@ def batched_scenes_config(n_scenes: int = 8, n_views: int = 64, scale: float = 1
         pos = random_sphere_camera(rng, 8.0, 14.0)
         views.append((s, w, h, pos))
     return scenes, views
+
+
+def batched_fwd_bwd_views(n_views: int = 32):
+    """Views of the batched forward + backward configuration over the 1M
+    clusters scene: W ~ U{640..1920}, H ~ U{480..1080}, camera radius
+    U[10, 14], k 16.  The target scene is ``perturb(raw_clusters(1M,
+    SEED_BASE + 1), SEED_BASE + 44)``."""
+    rng = _rng(SEED_BASE + 4)
+    views = []
+    for _ in range(n_views):
+        w = int(rng.integers(640, 1921))
+        h = int(rng.integers(480, 1081))
+        pos = random_sphere_camera(rng, 10.0, 14.0)
+        views.append(view(w, h, pos, k=16))
+    return views
