@@ -68,6 +68,10 @@ extern "C" gt_status gt_render_batch_noalloc(gt_context* ctx, const gt_batch_ite
     return api_fail(ctx, GT_ERR_INVALID_ARG,
                     "gt_render_batch_noalloc needs device output buffers (GT_FLAG_OUTPUT_DEVICE): host outputs "
                     "would need a staging allocation");
+  if (flags & GT_FLAG_CHECKPOINT)
+    return api_fail(ctx, GT_ERR_INVALID_ARG,
+                    "gt_render_batch_noalloc does not checkpoint: the round records need an allocation");
+  const bool aa = (flags & GT_FLAG_ANTIALIAS) != 0;
   uint32_t total_tiles = 0;
   uint64_t slots_all = 0;
   ViewDev views[kNoallocMaxViews];
@@ -83,6 +87,7 @@ extern "C" gt_status gt_render_batch_noalloc(gt_context* ctx, const gt_batch_ite
     if (((uintptr_t)it.out_rgba % 16) != 0)
       return api_fail(ctx, GT_ERR_INVALID_ARG, "device out_rgba must be 16-byte aligned");
     views[i] = api_make_view(it.scene, it.u, it.w, it.h, reinterpret_cast<float4*>(it.out_rgba), total_tiles);
+    views[i].u.aa = aa ? 1u : 0u;  // jittered sample blended into out_rgba, as gt_render_batch does
     total_tiles += views[i].n_tiles;
   }
   cudaError_t e = cudaSetDevice(ctx->device);
@@ -93,19 +98,26 @@ extern "C" gt_status gt_render_batch_noalloc(gt_context* ctx, const gt_batch_ite
   DevCounters* d_ctr = reinterpret_cast<DevCounters*>(scratch);
   ViewDev* d_views = reinterpret_cast<ViewDev*>(scratch + kCounterSlot);
   // the array keeps the previous call's contents: the counters must start at zero
-  e = cudaMemsetAsync(d_ctr, 0, sizeof(DevCounters), ctx->stream);
+  e = cudaEventRecord(ctx->call0, ctx->stream);  // the context's own timing events
+  if (e == cudaSuccess) e = cudaMemsetAsync(d_ctr, 0, sizeof(DevCounters), ctx->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->int0, ctx->stream);
   if (e != cudaSuccess) return api_fail(ctx, GT_ERR_CUDA, cudaGetErrorString(e));
   LaunchShape shape = api_shape_for(ctx, items[0].scene, items[0].w, items[0].h, items[0].u.k);
   Err err = launch_trace(views, count, total_tiles, d_ctr, ctx->faces, shape, ctx->num_sms, ctx->stream,
                          &ctx->launches, d_views);
   if (err.code != GT_OK) return api_fail(ctx, err.code, err.msg);
+  e = cudaEventRecord(ctx->int1, ctx->stream);
+  if (e != cudaSuccess) return api_fail(ctx, GT_ERR_CUDA, cudaGetErrorString(e));
   if (flags & GT_FLAG_ASYNC) return GT_OK;
   e = cudaMemcpyAsync(ctx->h_ctr, d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->call1, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return api_fail(ctx, GT_ERR_CUDA, cudaGetErrorString(e));
   if (stats) {
     memset(stats, 0, sizeof *stats);
     api_fill_stats(*ctx->h_ctr, stats);
+    cudaEventElapsedTime(&stats->kernel_ms, ctx->int0, ctx->int1);
+    cudaEventElapsedTime(&stats->total_ms, ctx->call0, ctx->call1);
   }
   return api_status_to_error(ctx, ctx->h_ctr->status);
 }
