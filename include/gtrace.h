@@ -341,7 +341,10 @@ gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items, uint32_t 
  * a process whose GPU memory is owned and capped by another allocator.
  * No counterpart in the reference.
  *   - outputs must be device buffers: GT_FLAG_OUTPUT_DEVICE is required
- *     (host outputs would need a staging allocation);
+ *     (host outputs would need a staging allocation); GT_FLAG_ANTIALIAS
+ *     blends into them as in gt_render_batch; GT_FLAG_CHECKPOINT is
+ *     rejected (the round records would need an allocation);
+ *   - stats (optional) carries the counters and the kernel and call times;
  *   - at most 256 views per call; larger counts are rejected with
  *     GT_ERR_INVALID_ARG;
  *   - the launch's scratch (tile counter, statistics, device view table,
