@@ -294,7 +294,10 @@ typedef struct gt_bwd_opts {
   uint32_t max_rounds;    /* in: expected rounds per ray, sizes the first checkpoint pool
                              (0 = the previous call's count, else 4); the pool grows to
                              the rounds actually traced.  out: round records used     */
-  uint64_t mem_budget;    /* bytes the checkpoint may use; 0 = 1/2 of free device memory */
+  uint64_t mem_budget;    /* bytes the checkpoint may use (0 = 1/2 of free device memory),
+                             and the adjoint's per-view colour sums (16 bytes a particle
+                             a view; 0 = 1/4 of free memory): views whose sums do not fit
+                             together run in successive adjoint launches               */
   uint32_t used_mode;     /* out: 1 = checkpoint, 2 = replay                              */
   uint32_t _pad;
   float fwd_ms;           /* out: device time of the forward (checkpointing) pass         */

@@ -186,3 +186,25 @@ def test_differentiable_config_subset(ctx):
                                 alpha_min=unpack_uniforms(v.uniforms)["alpha_min"])
     _check(got, ref)
     assert np.abs(got).sum() > 0
+
+
+@pytest.mark.parametrize("budget", [0, 1])
+def test_batch_of_two_scenes_matches_fp64_oracle(ctx, budget):
+    """Interleaved views of two scenes in one gt_backward_batch: each scene's
+    gradient is the sum of the FP64 adjoints of its views.  budget = 1 byte
+    puts every view in an adjoint launch of its own (the per-view colour sums
+    then never fit together), which must give the same sums."""
+    pa, pb = small_scene(n=1200, seed=45), small_scene(n=900, seed=46)
+    sa, sb = Scene(ctx, pa.gaussiansBuffer, 0.01), Scene(ctx, pb.gaussiansBuffer, 0.01)
+    rng = np.random.default_rng(7)
+    specs = [(sa, pa, view(32, 24, k=6)), (sb, pb, view(28, 20, pos=(1.0, 0.5, 3.6), k=4)),
+             (sa, pa, view(20, 36, pos=(-1.5, 0.5, 3.5), k=8))]
+    views, refs = [], {sa: 0.0, sb: 0.0}
+    for sc, pg, v in specs:
+        g = rng.normal(size=(v.height, v.width, 4)).astype(np.float32)
+        views.append((sc, v.uniforms, v.width, v.height, g))
+        refs[sc] = refs[sc] + _ref_grad(pg.gaussiansBuffer, 0.01, v.uniforms, v.width, v.height, g)
+    got, info = ctx.backward_batch(views, mode=1, mem_budget=budget)
+    assert info["used_mode"] == 1
+    for sc in (sa, sb):
+        _check(got[sc], refs[sc])

@@ -43,8 +43,6 @@
 
 namespace gt {
 
-constexpr int kGradStride = 60;  // floats per particle in the accumulation buffer
-
 // Real SH basis of degree <= deg at direction d and its gradient
 // (the polynomials of shToRadiance, src/GS_shader.ts:138-177).
 __device__ __forceinline__ void sh_basis(V3 d, uint32_t deg, float B[16], float dB[16][3]) {
@@ -89,53 +87,36 @@ __device__ __forceinline__ void sh_basis(V3 d, uint32_t deg, float B[16], float 
   }
 }
 
-// Gradient contribution of one composited entry (alpha > alpha_min).
-//   T: transmittance before the entry; a: its alpha; resp: exp(E);
-//   q: p - mu at the point of maximum density; craw: SH colour before the
-//   clamp; ga: dL/dalpha; g: dL/dpixel (rgb).
-__device__ __forceinline__ void entry_gradient(const SceneDev& S, uint32_t p, const Shade& sd, V3 o, V3 dr, float T,
-                                               float a, float resp, V3 q, const float craw[3], float ga,
-                                               const float g[3], uint32_t deg, float* G) {
-  double aqd[3];
-  float out[kGradStride];
+// Per-entry terms of the adjoint.  The 59 parameter gradients of a particle
+// are linear in a few sums over its composited entries (alpha > alpha_min),
+// so the adjoint adds those sums per particle and k_expand turns them into
+// gradients once per particle:
+//   response terms, independent of the view (v[0..15]):
+//     [0..2]  gE A q                position, through the response
+//     [3]     ga resp               opacity
+//     [4..6]  gE u_k^2              scales
+//     [7..15] gE q_r u_c            rotation (c fastest within r)
+//   with q = p - mu at the point of maximum density, u = R^T q in the
+//   particle's frame, gE = ga opacity resp = dL/dE;
+//   colour weights, per view (v[16..18]):
+//     gc = T alpha g                per channel where the SH colour is > 0
+//   from which the SH coefficient gradients B_k(dir) gc and the position term
+//   of the SH direction dir = normalize(mu - origin) follow; dir is the same
+//   for every ray of a view (all primary rays start at the camera).
+//   T: transmittance before the entry; a: its alpha; resp: exp(E); craw: SH
+//   colour before the clamp; ga: dL/dalpha; g: dL/dpixel (rgb).
+__device__ __forceinline__ void entry_terms(const SceneDev& S, uint32_t p, const Shade& sd, V3 o, V3 dr, float T,
+                                            float a, float resp, const float craw[3], float ga, const float g[3],
+                                            float v[20]) {
 #pragma unroll
-  for (int i = 0; i < kGradStride; ++i) out[i] = 0.f;
-  // colour: SH coefficients and the direction normalize(mu - o)
-  float gc[3];
-#pragma unroll
-  for (int ch = 0; ch < 3; ++ch) gc[ch] = craw[ch] > 0.f ? T * a * g[ch] : 0.f;
-  V3 v = vsub(sd.mu, o);
-  float len = sqrtf(vdot(v, v));
-  V3 dir = mk(v.x / len, v.y / len, v.z / len);
-  float B[16], dB[16][3];
-  sh_basis(dir, deg, B, dB);
-  const float4* shp = S.sh + 12 * (size_t)p;
-  float shv[48];
-#pragma unroll
-  for (int i = 0; i < 12; ++i) {
-    float4 c = __ldg(shp + i);
-    shv[4 * i] = c.x;
-    shv[4 * i + 1] = c.y;
-    shv[4 * i + 2] = c.z;
-    shv[4 * i + 3] = c.w;
-  }
-  float dd0 = 0.f, dd1 = 0.f, dd2 = 0.f;
-#pragma unroll
-  for (int k = 0; k < 16; ++k) {
-    float sg = shv[3 * k] * gc[0] + shv[3 * k + 1] * gc[1] + shv[3 * k + 2] * gc[2];
-    dd0 += dB[k][0] * sg;
-    dd1 += dB[k][1] * sg;
-    dd2 += dB[k][2] * sg;
-#pragma unroll
-    for (int ch = 0; ch < 3; ++ch) out[11 + 3 * k + ch] = B[k] * gc[ch];
-  }
-  float dd = dd0 * dir.x + dd1 * dir.y + dd2 * dir.z;
-  float dmu0 = (dd0 - dir.x * dd) / len, dmu1 = (dd1 - dir.y * dd) / len, dmu2 = (dd2 - dir.z * dd) / len;
-  // alpha = opacity * exp(E).  q = p - mu is the small difference of two
-  // points about |origin - mu| away, so it is formed in double here; A q is
-  // nearly orthogonal to the ray and keeps its small components only so.
-  out[10] = ga * resp;
+  for (int ch = 0; ch < 3; ++ch) v[16 + ch] = craw[ch] > 0.f ? T * a * g[ch] : 0.f;
+  v[19] = 0.f;
   const float gE = ga * sd.opacity * resp;
+  v[3] = ga * resp;
+  // q = p - mu is the small difference of two points about |origin - mu|
+  // apart, so it is formed in double; A q is nearly orthogonal to the ray and
+  // keeps its small components only so
+  double aqd[3], qd[3];
   {
     const double a00 = sd.a00, a01 = sd.a01, a02 = sd.a02, a11 = sd.a11, a12 = sd.a12, a22 = sd.a22;
     const double dx = dr.x, dy = dr.y, dz = dr.z;
@@ -144,162 +125,321 @@ __device__ __forceinline__ void entry_gradient(const SceneDev& S, uint32_t p, co
     const double t0 = a00 * dx + a01 * dy + a02 * dz, t1 = a01 * dx + a11 * dy + a12 * dz,
                  t2 = a02 * dx + a12 * dy + a22 * dz;
     const double tau = (mx * t0 + my * t1 + mz * t2) / (dx * t0 + dy * t1 + dz * t2);
-    const double qx = tau * dx - mx, qy = tau * dy - my, qz = tau * dz - mz;
-    q = mk((float)qx, (float)qy, (float)qz);
-    aqd[0] = a00 * qx + a01 * qy + a02 * qz;
-    aqd[1] = a01 * qx + a11 * qy + a12 * qz;
-    aqd[2] = a02 * qx + a12 * qy + a22 * qz;
+    qd[0] = tau * dx - mx;
+    qd[1] = tau * dy - my;
+    qd[2] = tau * dz - mz;
+    aqd[0] = a00 * qd[0] + a01 * qd[1] + a02 * qd[2];
+    aqd[1] = a01 * qd[0] + a11 * qd[1] + a12 * qd[2];
+    aqd[2] = a02 * qd[0] + a12 * qd[1] + a22 * qd[2];
   }
-  const float aq0 = (float)aqd[0], aq1 = (float)aqd[1], aq2 = (float)aqd[2];
-  out[0] = dmu0 + 2.f * gE * aq0;
-  out[1] = dmu1 + 2.f * gE * aq1;
-  out[2] = dmu2 + 2.f * gE * aq2;
-  const float4 sa = __ldg(S.params + 2 * (size_t)p), qa = __ldg(S.params + 2 * (size_t)p + 1);
-  const float s[3] = {sa.x, sa.y, sa.z};
+  const float q[3] = {(float)qd[0], (float)qd[1], (float)qd[2]};
+  const float4 qa = __ldg(S.params + 2 * (size_t)p + 1);
   const float qw = qa.x, qx = qa.y, qy = qa.z, qz = qa.w;
   // rotation of the quaternion (rows); computeResponse's matrix is its transpose
   const float R[3][3] = {{1.f - 2.f * (qy * qy + qz * qz), 2.f * (qx * qy - qw * qz), 2.f * (qx * qz + qw * qy)},
                          {2.f * (qx * qy + qw * qz), 1.f - 2.f * (qx * qx + qz * qz), 2.f * (qy * qz - qw * qx)},
                          {2.f * (qx * qz - qw * qy), 2.f * (qy * qz + qw * qx), 1.f - 2.f * (qx * qx + qy * qy)}};
-  const float qv[3] = {q.x, q.y, q.z};
   float u[3];
 #pragma unroll
-  for (int k = 0; k < 3; ++k) u[k] = R[0][k] * qv[0] + R[1][k] * qv[1] + R[2][k] * qv[2];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) out[3 + k] = gE * 2.f * u[k] * u[k] / (s[k] * s[k] * s[k]);
-  float GR[3][3];
-#pragma unroll
-  for (int r = 0; r < 3; ++r)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) GR[r][c] = -2.f * gE * qv[r] * u[c] / (s[c] * s[c]);
-  out[6] = 2.f * (-qz * GR[0][1] + qy * GR[0][2] + qz * GR[1][0] - qx * GR[1][2] - qy * GR[2][0] + qx * GR[2][1]);
-  out[7] = 2.f * (qy * GR[0][1] + qz * GR[0][2] + qy * GR[1][0] - 2.f * qx * GR[1][1] - qw * GR[1][2] +
-                  qz * GR[2][0] + qw * GR[2][1] - 2.f * qx * GR[2][2]);
-  out[8] = 2.f * (-2.f * qy * GR[0][0] + qx * GR[0][1] + qw * GR[0][2] + qx * GR[1][0] + qz * GR[1][2] -
-                  qw * GR[2][0] + qz * GR[2][1] - 2.f * qy * GR[2][2]);
-  out[9] = 2.f * (-2.f * qz * GR[0][0] - qw * GR[0][1] + qx * GR[0][2] + qw * GR[1][0] - 2.f * qz * GR[1][1] +
-                  qy * GR[1][2] + qx * GR[2][0] + qy * GR[2][1]);
-  float4* dst = reinterpret_cast<float4*>(G + (size_t)p * kGradStride);
-#pragma unroll
-  for (int c = 0; c < kGradStride / 4; ++c) {
-    float4 v4 = make_float4(out[4 * c], out[4 * c + 1], out[4 * c + 2], out[4 * c + 3]);
-    if (v4.x != 0.f || v4.y != 0.f || v4.z != 0.f || v4.w != 0.f) atomicAdd(dst + c, v4);
-  }
+  for (int k = 0; k < 3; ++k) u[k] = R[0][k] * q[0] + R[1][k] * q[1] + R[2][k] * q[2];
+  const float gu0 = gE * u[0], gu1 = gE * u[1], gu2 = gE * u[2];
+  v[0] = gE * (float)aqd[0];
+  v[1] = gE * (float)aqd[1];
+  v[2] = gE * (float)aqd[2];
+  v[4] = gu0 * u[0];
+  v[5] = gu1 * u[1];
+  v[6] = gu2 * u[2];
+  v[7] = gu0 * q[0];
+  v[8] = gu1 * q[0];
+  v[9] = gu2 * q[0];
+  v[10] = gu0 * q[1];
+  v[11] = gu1 * q[1];
+  v[12] = gu2 * q[1];
+  v[13] = gu0 * q[2];
+  v[14] = gu1 * q[2];
+  v[15] = gu2 * q[2];
 }
 
-// The adjoint, one warp per ray slot (same slot numbering as the forward).
+// Per-warp table of per-particle sums.  The rays of one 8x4 tile composite
+// mostly the same particles, so the warp adds its tile's entry terms here
+// (shared-memory atomics; the entries of one round are distinct particles
+// but for shared-edge duplicates) and each particle's sums reach global
+// memory once per tile: 5 vector atomics per particle and tile instead of
+// per entry.
+constexpr int kAggSlots = 64;
+struct AggTable {
+  uint32_t key[kAggSlots];   // particle index, kInvalid when empty
+  float4 val[kAggSlots][5];  // the 16 response sums, then the 3 colour sums and 0
+};
+
+__device__ __forceinline__ void agg_clear(AggTable& A, uint32_t lane) {
+  for (uint32_t i = lane; i < (uint32_t)kAggSlots; i += 32) {
+    A.key[i] = kInvalid;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) A.val[i][c] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  __syncwarp();
+}
+
+// Adds the terms v of particle p; returns whether p took an empty slot.  The
+// caller keeps at most kAggSlots particles in the table, so the probe finds
+// p or an empty slot within kAggSlots steps; past them (never) the terms go
+// straight to global memory.
+__device__ __forceinline__ bool agg_add(AggTable& A, uint32_t p, const float v[20], float4* G, float4* GS) {
+  uint32_t h = (p * 2654435761u) >> 26;
+  for (int step = 0; step < kAggSlots; ++step) {
+    const uint32_t prev = atomicCAS(&A.key[h], kInvalid, p);
+    if (prev == kInvalid || prev == p) {
+      float* d = reinterpret_cast<float*>(&A.val[h][0]);
+#pragma unroll
+      for (int i = 0; i < 19; ++i)
+        if (v[i] != 0.f) atomicAdd(d + i, v[i]);
+      return prev == kInvalid;
+    }
+    h = (h + 1) & (kAggSlots - 1);
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c)
+    atomicAdd(G + 4 * (size_t)p + c, make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]));
+  atomicAdd(GS + p, make_float4(v[16], v[17], v[18], 0.f));
+  return false;
+}
+
+// Adds the table to the scene's response sums G and the view's colour sums
+// GS and empties it.
+__device__ __forceinline__ void agg_flush(AggTable& A, float4* G, float4* GS, uint32_t lane) {
+  __syncwarp();
+  for (uint32_t i = lane; i < (uint32_t)kAggSlots; i += 32) {
+    const uint32_t p = A.key[i];
+    if (p == kInvalid) continue;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+      const float4 x = A.val[i][c];
+      if (x.x != 0.f || x.y != 0.f || x.z != 0.f || x.w != 0.f) atomicAdd(c < 4 ? G + 4 * (size_t)p + c : GS + p, x);
+      A.val[i][c] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    A.key[i] = kInvalid;
+  }
+  __syncwarp();
+}
+
+// The adjoint, one warp per 8x4 tile of ray slots (the forward's slot
+// numbering): the tiles [tile_begin, tile_end) of the launch's views, the
+// 32 rays of a tile one after the other, each round's entries across the
+// lanes; the tile's per-particle sums gather in the warp's table.
 template <bool CKPT_PIDX>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewDev* __restrict__ views,
-                                                                    uint32_t n_views, uint32_t total_tiles,
-                                                                    DevCounters* ctr, const __grid_constant__ FaceTable F,
+                                                                    uint32_t n_views, uint32_t tile_begin,
+                                                                    uint32_t tile_end, DevCounters* ctr,
+                                                                    const __grid_constant__ FaceTable F,
                                                                     const Ckpt ck) {
   __shared__ WarpScratch scratch[kWarpsPerBlock];
+  __shared__ AggTable tables[kWarpsPerBlock];
   const uint32_t lane = threadIdx.x & 31;
   WarpScratch& W = scratch[threadIdx.x >> 5];
+  AggTable& A = tables[threadIdx.x >> 5];
   RayStats& st = W.stats;
   if (lane == 0) st = RayStats{0, 0, 0, 0, 0, 0};
-  __syncwarp();
+  agg_clear(A, lane);
   uint32_t status = 0, rays = 0;
-  const uint32_t total = total_tiles * 32u;
   while (true) {
-    uint32_t item = 0;
-    if (lane == 0) item = atomicAdd(&ctr->work, 1u);
-    item = __shfl_sync(kFull, item, 0);
-    if (item >= total) break;
-    uint32_t tile = item >> 5, sl = item & 31u;
+    uint32_t tile = 0;
+    if (lane == 0) tile = atomicAdd(&ctr->work, 1u);
+    tile = __shfl_sync(kFull, tile, 0);
+    if (tile >= tile_end - tile_begin) break;
+    tile += tile_begin;
     const uint32_t vi = n_views == 1 ? 0u : find_view(views, n_views, tile);
     const ViewDev& V = views[vi];
-    uint32_t px, py;
-    tile_pixel(V.tiles_x, tile - V.tile_begin, sl, px, py);
-    if (px >= V.w || py >= V.h) continue;
-    uint32_t rec = ck.head[item];
-    if (rec == kInvalid) continue;
-    const float4 g4 = V.dL[(size_t)py * V.w + px];
-    if (g4.x == 0.f && g4.y == 0.f && g4.z == 0.f) continue;
-    const float g[3] = {g4.x, g4.y, g4.z};
-    V3 o, d;
-    ray_gen(V.u, V.w, V.h, px, py, o, d);
-    const BoxRay br = make_boxray(o, d, V.s.scene_mag);
-    const uint32_t k = V.u.k;
-    float R0 = 0.f, R1 = 0.f, R2 = 0.f;
-    ++rays;
-    // rounds from the last to the first along the record links
-    for (uint32_t guard = 0; rec != kInvalid && guard < ck.pool_cap; ++guard) {
-      const uint32_t* rr = ck.pool + (size_t)rec * (kCkptHeader + ck.kc);
-      const float2 ri = make_float2(__uint_as_float(rr[0]), __uint_as_float(rr[1]));
-      const uint32_t prev = rr[2], nrec = rr[3];
-      uint32_t p = kInvalid;
-      bool valid;
-      if (CKPT_PIDX) {
-        p = lane < ck.kc ? rr[kCkptHeader + lane] : kInvalid;
-        valid = lane < nrec && p != kInvalid;
-      } else {
-        KBuf<1> kb;
-        kbuf_init(kb, V.u.t_max);
-        traverse8<kCollect>(V.s, F, W, o, d, br, ri.x, V.u.t_max, kb, st, status, lane, (int)k, V.leaf_batch);
-        if (__reduce_or_sync(kFull, status) & (kStatusStackOverflow | kStatusVisitCap | kStatusHitOverflow)) break;
-        valid = lane < k && lane < nrec && kb.p[0] != kInvalid;
-        p = kb.p[0];
-      }
-      rec = prev;
-      const uint32_t vmask = __ballot_sync(kFull, valid);
-      const int n = __popc(vmask);
-      float alpha = 0.f, resp = 0.f;
-      float craw[3] = {0.f, 0.f, 0.f};
-      V3 q = mk(0.f, 0.f, 0.f);
-      Shade sd;
-      bool contrib = false;
-      if (valid) {
-        sd = load_shade(V.s.shade, p);
-        resp = response(sd, o, d, &q);
-        alpha = resp * sd.opacity;
-        contrib = V.u.alpha_min < alpha;
-        if (contrib) sh_radiance(V.s.sh, p, vnorm(vsub(sd.mu, o)), V.u.deg, craw);
-      }
-      const uint32_t cmask = __ballot_sync(kFull, contrib);
-      // transmittance before each entry, in entry order from the round's start
-      float T = ri.y, Tme = 0.f;
-      for (int e = 0; e < n; ++e) {
-        if ((int)lane == e) Tme = T;
-        float a = __shfl_sync(kFull, alpha, e);
-        if ((cmask >> e) & 1u) T = T * (1.0f - a);
-      }
-      // back to front
-      float ga = 0.f;
-      for (int e = n - 1; e >= 0; --e) {
-        float a = __shfl_sync(kFull, alpha, e);
-        float c0 = __shfl_sync(kFull, craw[0], e), c1 = __shfl_sync(kFull, craw[1], e),
-              c2 = __shfl_sync(kFull, craw[2], e);
-        float te = __shfl_sync(kFull, Tme, e);
-        if ((cmask >> e) & 1u) {
-          c0 = c0 > 0.f ? c0 : 0.f;
-          c1 = c1 > 0.f ? c1 : 0.f;
-          c2 = c2 > 0.f ? c2 : 0.f;
-          float gae = te * ((g[0] * c0 + g[1] * c1 + g[2] * c2) - (g[0] * R0 + g[1] * R1 + g[2] * R2));
-          if ((int)lane == e) ga = gae;
-          R0 = a * c0 + (1.f - a) * R0;
-          R1 = a * c1 + (1.f - a) * R1;
-          R2 = a * c2 + (1.f - a) * R2;
+    uint32_t nfill = 0;  // particles in the table
+    for (uint32_t sl = 0; sl < 32; ++sl) {
+      const uint32_t item = 32u * tile + sl;
+      uint32_t px, py;
+      tile_pixel(V.tiles_x, tile - V.tile_begin, sl, px, py);
+      if (px >= V.w || py >= V.h) continue;
+      uint32_t rec = ck.head[item];
+      if (rec == kInvalid) continue;
+      const float4 g4 = V.dL[(size_t)py * V.w + px];
+      if (g4.x == 0.f && g4.y == 0.f && g4.z == 0.f) continue;
+      const float g[3] = {g4.x, g4.y, g4.z};
+      V3 o, d;
+      ray_gen(V.u, V.w, V.h, px, py, o, d);
+      const BoxRay br = make_boxray(o, d, V.s.scene_mag);
+      const uint32_t k = V.u.k;
+      float R0 = 0.f, R1 = 0.f, R2 = 0.f;
+      ++rays;
+      // rounds from the last to the first along the record links
+      for (uint32_t guard = 0; rec != kInvalid && guard < ck.pool_cap; ++guard) {
+        const uint32_t* rr = ck.pool + (size_t)rec * (kCkptHeader + ck.kc);
+        const float2 ri = make_float2(__uint_as_float(rr[0]), __uint_as_float(rr[1]));
+        const uint32_t prev = rr[2], nrec = rr[3];
+        uint32_t p = kInvalid;
+        bool valid;
+        if (CKPT_PIDX) {
+          p = lane < ck.kc ? rr[kCkptHeader + lane] : kInvalid;
+          valid = lane < nrec && p != kInvalid;
+        } else {
+          KBuf<1> kb;
+          kbuf_init(kb, V.u.t_max);
+          traverse8<kCollect>(V.s, F, W, o, d, br, ri.x, V.u.t_max, kb, st, status, lane, (int)k, V.leaf_batch);
+          if (__reduce_or_sync(kFull, status) & (kStatusStackOverflow | kStatusVisitCap | kStatusHitOverflow)) break;
+          valid = lane < k && lane < nrec && kb.p[0] != kInvalid;
+          p = kb.p[0];
+        }
+        rec = prev;
+        const uint32_t vmask = __ballot_sync(kFull, valid);
+        const int n = __popc(vmask);
+        float alpha = 0.f, resp = 0.f;
+        float craw[3] = {0.f, 0.f, 0.f};
+        Shade sd;
+        bool contrib = false;
+        if (valid) {
+          sd = load_shade(V.s.shade, p);
+          resp = response(sd, o, d);
+          alpha = resp * sd.opacity;
+          contrib = V.u.alpha_min < alpha;
+          if (contrib) sh_radiance(V.s.sh, p, vnorm(vsub(sd.mu, o)), V.u.deg, craw);
+        }
+        const uint32_t cmask = __ballot_sync(kFull, contrib);
+        // transmittance before each entry, in entry order from the round's start
+        float T = ri.y, Tme = 0.f;
+        for (int e = 0; e < n; ++e) {
+          if ((int)lane == e) Tme = T;
+          float a = __shfl_sync(kFull, alpha, e);
+          if ((cmask >> e) & 1u) T = T * (1.0f - a);
+        }
+        // back to front
+        float ga = 0.f;
+        for (int e = n - 1; e >= 0; --e) {
+          float a = __shfl_sync(kFull, alpha, e);
+          float c0 = __shfl_sync(kFull, craw[0], e), c1 = __shfl_sync(kFull, craw[1], e),
+                c2 = __shfl_sync(kFull, craw[2], e);
+          float te = __shfl_sync(kFull, Tme, e);
+          if ((cmask >> e) & 1u) {
+            c0 = c0 > 0.f ? c0 : 0.f;
+            c1 = c1 > 0.f ? c1 : 0.f;
+            c2 = c2 > 0.f ? c2 : 0.f;
+            float gae = te * ((g[0] * c0 + g[1] * c1 + g[2] * c2) - (g[0] * R0 + g[1] * R1 + g[2] * R2));
+            if ((int)lane == e) ga = gae;
+            R0 = a * c0 + (1.f - a) * R0;
+            R1 = a * c1 + (1.f - a) * R1;
+            R2 = a * c2 + (1.f - a) * R2;
+          }
+        }
+        // room for this round's particles in the table
+        const uint32_t nc = (uint32_t)__popc(cmask);
+        if (nfill + nc > (uint32_t)kAggSlots) {
+          agg_flush(A, V.grad, V.grad_sh, lane);
+          nfill = 0;
+        }
+        bool fresh = false;
+        if (contrib) {
+          float v[20];
+          entry_terms(V.s, p, sd, o, d, Tme, alpha, resp, craw, ga, g, v);
+          fresh = agg_add(A, p, v, V.grad, V.grad_sh);
+        }
+        nfill += (uint32_t)__popc(__ballot_sync(kFull, fresh));
+        if (lane == 0) {
+          ++st.rounds;
+          st.entries += (unsigned)n;
+          st.contributing += nc;
         }
       }
-      if (contrib) entry_gradient(V.s, p, sd, o, d, Tme, alpha, resp, q, craw, ga, g, V.u.deg, V.grad);
-      if (lane == 0) {
-        ++st.rounds;
-        st.entries += (unsigned)n;
-        st.contributing += (unsigned)__popc(cmask);
-      }
     }
+    // the next tile may be another view's (other colour sums) or scene's
+    agg_flush(A, V.grad, V.grad_sh, lane);
   }
   flush_stats(ctr, st, rays, status);
 }
 
-// Parameter-major output: out[i * n + p] (+)= G[p * 60 + i], i < 59.
-__global__ void k_grad_out(const float* G, uint64_t n, float* out, bool accumulate) {
-  uint64_t idx = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (idx >= n * GT_PARAMS_PER_PARTICLE) return;
-  uint64_t i = idx / n, p = idx % n;
-  float v = G[p * kGradStride + i];
-  out[idx] = accumulate ? out[idx] + v : v;
+// One view's share of the SH terms of a scene's particles: the camera
+// position, the view's SH degree and its colour-weight sums (1 float4 a
+// particle).
+struct ExpandView {
+  float ox, oy, oz;
+  uint32_t deg;
+  const float4* gs;
+};
+
+// The 59 gradients of particle p from its sums (entry_terms), written
+// parameter-major: out[i * n + p] (+)= dL/dparam_i.
+__global__ void __launch_bounds__(128) k_expand(const float4* __restrict__ G, const ExpandView* __restrict__ ev,
+                                                uint32_t n_ev, SceneDev S, uint64_t n, float* __restrict__ out,
+                                                bool accumulate) {
+  const uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const float4 r0 = G[4 * p], r1 = G[4 * p + 1], r2 = G[4 * p + 2], r3 = G[4 * p + 3];
+  const float4 sa = __ldg(S.params + 2 * p), qa = __ldg(S.params + 2 * p + 1);
+  const float s[3] = {sa.x, sa.y, sa.z};
+  const float qw = qa.x, qx = qa.y, qy = qa.z, qz = qa.w;
+  float head[11];
+  head[0] = 2.f * r0.x;
+  head[1] = 2.f * r0.y;
+  head[2] = 2.f * r0.z;
+  head[10] = r0.w;
+  const float U[3] = {r1.x, r1.y, r1.z};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) head[3 + k] = 2.f * U[k] / (s[k] * s[k] * s[k]);
+  // sum gE q_r u_c, and GR = dL/dR(r, c) = -2 sum gE q_r u_c / s_c^2
+  const float M[3][3] = {{r1.w, r2.x, r2.y}, {r2.z, r2.w, r3.x}, {r3.y, r3.z, r3.w}};
+  float GR[3][3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) GR[r][c] = -2.f * M[r][c] / (s[c] * s[c]);
+  head[6] = 2.f * (-qz * GR[0][1] + qy * GR[0][2] + qz * GR[1][0] - qx * GR[1][2] - qy * GR[2][0] + qx * GR[2][1]);
+  head[7] = 2.f * (qy * GR[0][1] + qz * GR[0][2] + qy * GR[1][0] - 2.f * qx * GR[1][1] - qw * GR[1][2] +
+                   qz * GR[2][0] + qw * GR[2][1] - 2.f * qx * GR[2][2]);
+  head[8] = 2.f * (-2.f * qy * GR[0][0] + qx * GR[0][1] + qw * GR[0][2] + qx * GR[1][0] + qz * GR[1][2] -
+                   qw * GR[2][0] + qz * GR[2][1] - 2.f * qy * GR[2][2]);
+  head[9] = 2.f * (-2.f * qz * GR[0][0] - qw * GR[0][1] + qx * GR[0][2] + qw * GR[1][0] - 2.f * qz * GR[1][1] +
+                   qy * GR[1][2] + qx * GR[2][0] + qy * GR[2][1]);
+  // SH coefficients, B_k(dir) sum gc, and the position term of dir
+  float gsh[48];
+#pragma unroll
+  for (int i = 0; i < 48; ++i) gsh[i] = 0.f;
+  const float4 m4 = __ldg(S.shade + 3 * p);
+  const V3 mu = mk(m4.x, m4.y, m4.z);
+  for (uint32_t v = 0; v < n_ev; ++v) {
+    const float4 gc4 = ev[v].gs[p];
+    if (gc4.x == 0.f && gc4.y == 0.f && gc4.z == 0.f) continue;
+    const float gc[3] = {gc4.x, gc4.y, gc4.z};
+    const V3 d0 = vsub(mu, mk(ev[v].ox, ev[v].oy, ev[v].oz));
+    const float len = sqrtf(vdot(d0, d0));
+    const V3 dir = mk(d0.x / len, d0.y / len, d0.z / len);
+    float B[16], dB[16][3];
+    sh_basis(dir, ev[v].deg, B, dB);
+    const float4* shp = S.sh + 12 * p;
+    float dd0 = 0.f, dd1 = 0.f, dd2 = 0.f;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float4 c0 = __ldg(shp + 3 * i), c1 = __ldg(shp + 3 * i + 1), c2 = __ldg(shp + 3 * i + 2);
+      const float sv[12] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w, c2.x, c2.y, c2.z, c2.w};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int k = 4 * i + j;
+        const float sg = sv[3 * j] * gc[0] + sv[3 * j + 1] * gc[1] + sv[3 * j + 2] * gc[2];
+        dd0 += dB[k][0] * sg;
+        dd1 += dB[k][1] * sg;
+        dd2 += dB[k][2] * sg;
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) gsh[3 * k + ch] += B[k] * gc[ch];
+      }
+    }
+    const float dd = dd0 * dir.x + dd1 * dir.y + dd2 * dir.z;
+    head[0] += (dd0 - dir.x * dd) / len;
+    head[1] += (dd1 - dir.y * dd) / len;
+    head[2] += (dd2 - dir.z * dd) / len;
+  }
+#pragma unroll
+  for (int i = 0; i < 11; ++i) {
+    float* o = out + (uint64_t)i * n + p;
+    *o = accumulate ? *o + head[i] : head[i];
+  }
+#pragma unroll
+  for (int i = 0; i < 48; ++i) {
+    float* o = out + (uint64_t)(11 + i) * n + p;
+    *o = accumulate ? *o + gsh[i] : gsh[i];
+  }
 }
 
 // Writes the L2 loss gradient and per-block partial sums of the loss.
@@ -525,13 +665,7 @@ gt_status backward_impl(gt_context* ctx, const BwdView* views, uint32_t count, c
     fwd_ms = ctx->ckpt.fwd_ms;
   }
   const CkptStore& cs = ctx->ckpt;
-  // 2. per-scene accumulation buffers, dL on the device, the adjoint's view table
-  std::vector<float*> G(n_scenes, nullptr);
-  for (uint32_t s = 0; s < n_scenes; ++s) {
-    uint64_t n = std::max<uint64_t>(scenes[s]->n, 1);
-    BWD_TRY(talloc((void**)&G[s], (size_t)n * kGradStride * 4));
-    BWD_TRY(cudaMemsetAsync(G[s], 0, (size_t)n * kGradStride * 4, st));
-  }
+  // 2. dL on the device and the adjoint's view table
   float4* dl_dev = nullptr;
   if (!(flags & GT_FLAG_INPUT_DEVICE)) BWD_TRY(talloc((void**)&dl_dev, pixels * sizeof(float4)));
   gt_status sst = api_ensure_views(ctx, count);
@@ -540,6 +674,7 @@ gt_status backward_impl(gt_context* ctx, const BwdView* views, uint32_t count, c
     return sst;
   }
   std::vector<ViewDev> vd(count);
+  std::vector<uint32_t> vscene(count);
   uint32_t total_tiles = 0;
   size_t off = 0;
   for (uint32_t i = 0; i < count; ++i) {
@@ -555,51 +690,118 @@ gt_status backward_impl(gt_context* ctx, const BwdView* views, uint32_t count, c
     }
     uint32_t s = 0;
     while (s < n_scenes && scenes[s] != bv.scene) ++s;
-    vd[i].grad = G[s];
+    vscene[i] = s;
     off += px;
   }
+  // 3. per-scene sums of the response terms (4 float4 a particle) and per-view
+  //    colour sums (1 float4 a particle of the view's scene).  Views go in
+  //    groups whose colour sums fit the budget; each group is one adjoint
+  //    launch over its tile range and one expansion per scene.
+  std::vector<float4*> G(n_scenes, nullptr);
+  for (uint32_t s = 0; s < n_scenes; ++s)
+    BWD_TRY(talloc((void**)&G[s], (size_t)std::max<uint64_t>(scenes[s]->n, 1) * 4 * sizeof(float4)));
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  const size_t gs_budget =
+      (opts && opts->mem_budget) ? (size_t)opts->mem_budget : std::max<size_t>((size_t)256 << 20, free_b / 4);
+  std::vector<uint32_t> group_end;
+  size_t gs_max = 0;
+  {
+    size_t acc = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+      const size_t b = (size_t)std::max<uint64_t>(scenes[vscene[i]]->n, 1) * sizeof(float4);
+      if (acc > 0 && acc + b > gs_budget) {
+        group_end.push_back(i);
+        acc = 0;
+      }
+      acc += b;
+      gs_max = std::max(gs_max, acc);
+    }
+    group_end.push_back(count);
+  }
+  float4* gs_all = nullptr;
+  BWD_TRY(talloc((void**)&gs_all, gs_max));
+  ExpandView* d_ev = nullptr;
+  BWD_TRY(talloc((void**)&d_ev, sizeof(ExpandView) * count));
+  std::vector<ExpandView> hev(count);
   const LaunchShape shape = api_shape_for(ctx, views[0].scene, views[0].w, views[0].h, views[0].u.k);
   apply_shape(vd.data(), count, shape);
-  BWD_TRY(cudaMemcpyAsync(ctx->d_views, vd.data(), sizeof(ViewDev) * count, cudaMemcpyHostToDevice, st));
   Ckpt ck;
   ck.head = cs.head;
   ck.pool = cs.pool;
   ck.pool_next = cs.pool_next;
   ck.pool_cap = cs.pool_cap;
   ck.kc = cs.kc;
-  // 3. the adjoint
+  std::vector<float*> dev_out(n_scenes, nullptr);
+  for (uint32_t s = 0; s < n_scenes; ++s) {
+    const uint64_t n = scenes[s]->n;
+    dev_out[s] = outs[s];
+    if (n == 0 || (flags & GT_FLAG_OUTPUT_DEVICE)) continue;
+    BWD_TRY(talloc((void**)&dev_out[s], n * GT_PARAMS_PER_PARTICLE * 4));
+    if (flags & GT_FLAG_ACCUMULATE)
+      BWD_TRY(cudaMemcpyAsync(dev_out[s], outs[s], n * GT_PARAMS_PER_PARTICLE * 4, cudaMemcpyHostToDevice, st));
+  }
   float bwd_ms = 0.f;
   BWD_TRY(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), st));
   BWD_TRY(cudaEventRecord(ctx->int0, st));
-  {
-    uint32_t block = kWarpsPerBlock * 32;
-    uint32_t grid = (uint32_t)ctx->num_sms * std::max(1u, shape.blocks_per_sm);
-    uint64_t max_grid = ((uint64_t)total_tiles * 32u + kWarpsPerBlock - 1) / kWarpsPerBlock;
-    if (grid > max_grid) grid = (uint32_t)std::max<uint64_t>(1, max_grid);
-    if (cs.mode == 1)
-      k_backward<true><<<grid, block, 0, st>>>(ctx->d_views, count, total_tiles, ctx->d_ctr, ctx->faces, ck);
-    else
-      k_backward<false><<<grid, block, 0, st>>>(ctx->d_views, count, total_tiles, ctx->d_ctr, ctx->faces, ck);
-    ++ctx->launches;
-    BWD_TRY(cudaGetLastError());
-  }
-  // 4. parameter-major outputs
-  for (uint32_t s = 0; s < n_scenes; ++s) {
-    uint64_t n = scenes[s]->n;
-    if (n == 0) continue;
-    float* dst = outs[s];
-    float* dev_out = dst;
-    if (!(flags & GT_FLAG_OUTPUT_DEVICE)) {
-      BWD_TRY(talloc((void**)&dev_out, n * GT_PARAMS_PER_PARTICLE * 4));
-      if (flags & GT_FLAG_ACCUMULATE)
-        BWD_TRY(cudaMemcpyAsync(dev_out, dst, n * GT_PARAMS_PER_PARTICLE * 4, cudaMemcpyHostToDevice, st));
+  uint32_t g0 = 0;
+  for (size_t gi = 0; gi < group_end.size(); ++gi) {
+    const uint32_t g1 = group_end[gi];
+    size_t gs_off = 0;
+    for (uint32_t i = g0; i < g1; ++i) {
+      const ViewDev& v = vd[i];
+      const uint64_t n = std::max<uint64_t>(scenes[vscene[i]]->n, 1);
+      vd[i].grad = G[vscene[i]];
+      vd[i].grad_sh = gs_all + gs_off;
+      hev[i] = ExpandView{v.u.tw[12], v.u.tw[13], v.u.tw[14], v.u.deg, gs_all + gs_off};
+      gs_off += n;
     }
-    uint64_t total = n * GT_PARAMS_PER_PARTICLE;
-    k_grad_out<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(G[s], n, dev_out, (flags & GT_FLAG_ACCUMULATE) != 0);
-    ++ctx->launches;
-    BWD_TRY(cudaGetLastError());
-    if (!(flags & GT_FLAG_OUTPUT_DEVICE))
-      BWD_TRY(cudaMemcpyAsync(dst, dev_out, n * GT_PARAMS_PER_PARTICLE * 4, cudaMemcpyDeviceToHost, st));
+    for (uint32_t s = 0; s < n_scenes; ++s)
+      BWD_TRY(cudaMemsetAsync(G[s], 0, (size_t)std::max<uint64_t>(scenes[s]->n, 1) * 4 * sizeof(float4), st));
+    BWD_TRY(cudaMemsetAsync(gs_all, 0, gs_off * sizeof(float4), st));
+    BWD_TRY(cudaMemcpyAsync(ctx->d_views, vd.data(), sizeof(ViewDev) * count, cudaMemcpyHostToDevice, st));
+    BWD_TRY(cudaMemsetAsync(&ctx->d_ctr->work, 0, sizeof(uint32_t), st));
+    {
+      const uint32_t tile0 = vd[g0].tile_begin;
+      const uint32_t tile1 = vd[g1 - 1].tile_begin + vd[g1 - 1].n_tiles;
+      uint32_t block = kWarpsPerBlock * 32;
+      uint32_t grid = (uint32_t)ctx->num_sms * 4u;  // 4 resident blocks an SM (launch bounds)
+      uint64_t max_grid = ((uint64_t)(tile1 - tile0) + kWarpsPerBlock - 1) / kWarpsPerBlock;
+      if (grid > max_grid) grid = (uint32_t)std::max<uint64_t>(1, max_grid);
+      if (cs.mode == 1)
+        k_backward<true><<<grid, block, 0, st>>>(ctx->d_views, count, tile0, tile1, ctx->d_ctr, ctx->faces, ck);
+      else
+        k_backward<false><<<grid, block, 0, st>>>(ctx->d_views, count, tile0, tile1, ctx->d_ctr, ctx->faces, ck);
+      ++ctx->launches;
+      BWD_TRY(cudaGetLastError());
+    }
+    // 4. parameter-major gradients of each scene from its sums and its views' colour sums
+    for (uint32_t s = 0; s < n_scenes; ++s) {
+      const uint64_t n = scenes[s]->n;
+      if (n == 0) continue;
+      // this group's views of scene s, uploaded as one run of the table
+      std::vector<ExpandView> mine;
+      for (uint32_t i = g0; i < g1; ++i)
+        if (vscene[i] == s) mine.push_back(hev[i]);
+      ExpandView* evs = d_ev + g0;
+      if (!mine.empty())
+        BWD_TRY(cudaMemcpyAsync(evs, mine.data(), sizeof(ExpandView) * mine.size(), cudaMemcpyHostToDevice, st));
+      const bool acc = gi > 0 || (flags & GT_FLAG_ACCUMULATE);
+      SceneDev sd{};
+      sd.shade = scenes[s]->b.shade;
+      sd.sh = scenes[s]->b.sh;
+      sd.params = scenes[s]->b.params;
+      k_expand<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(G[s], evs, (uint32_t)mine.size(), sd, n, dev_out[s],
+                                                             acc);
+      ++ctx->launches;
+      BWD_TRY(cudaGetLastError());
+    }
+    g0 = g1;
+  }
+  for (uint32_t s = 0; s < n_scenes; ++s) {
+    const uint64_t n = scenes[s]->n;
+    if (n == 0 || (flags & GT_FLAG_OUTPUT_DEVICE)) continue;
+    BWD_TRY(cudaMemcpyAsync(outs[s], dev_out[s], n * GT_PARAMS_PER_PARTICLE * 4, cudaMemcpyDeviceToHost, st));
   }
   BWD_TRY(cudaEventRecord(ctx->int1, st));
   BWD_TRY(cudaMemcpyAsync(ctx->h_ctr, ctx->d_ctr, sizeof(DevCounters), cudaMemcpyDeviceToHost, st));

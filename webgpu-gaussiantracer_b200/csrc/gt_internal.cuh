@@ -123,7 +123,8 @@ struct ViewDev {
   uint32_t pkbuf;       // the tile-packet kernel's k-buffer entries per ray (k..64)
   uint32_t leaf_batch;  // queued leaves that trigger a batch of proxy tests (8..32)
   const float4* dL;     // backward: dL/drgba (w*h)
-  float* grad;          // backward: 59 x n parameter-major gradient
+  float4* grad;         // backward: the scene's per-particle sums of the response terms (4 float4 a particle)
+  float4* grad_sh;      // backward: this view's per-particle sums of the colour weights (1 float4 a particle)
   uint64_t n_particles;
 };
 
