@@ -219,6 +219,11 @@ def extra_batched(ctx, reps: int = 2):
             ctx.render_device(sc, u, w, h, ptr, asynchronous=True)
     batched()
     plain()
+    tdef = _time_device(ctx, batched, reps)  # the default shape
+    # the batch tuner picks k-buffer, hand-off and kernel for this batch shape;
+    # render_batch then uses its choice
+    tune = ctx.autotune_batch([(sc, u, w, h) for sc, u, w, h, _ in items])
+    batched()
     tb = _time_device(ctx, batched, reps)
     tp = _time_device(ctx, plain, reps)
     for ptr in bufs:
@@ -229,7 +234,11 @@ def extra_batched(ctx, reps: int = 2):
     return {"workload": f"8 scenes ({n_total} Gaussians in all, 100k-1M each, 64 clusters), 64 views 320-1920 x "
                         "240-1080, k=16, alpha_min per scene in {0.01, 0.05, 0.1}, camera radius 8-14",
             "rays": rays, "batched_ms": tb, "plain_ms": tp, "batched_mrays": rays / tb / 1e3,
-            "plain_mrays": rays / tp / 1e3}
+            "plain_mrays": rays / tp / 1e3, "default_shape_ms": tdef,
+            "shape": {"kernel": "tile packets" if tune["block_threads"] == 32 else "warp per ray",
+                      "kbuf": tune["kbuf"], "handoff_after": tune["handoff_after"],
+                      "blocks_per_sm": tune["blocks_per_sm"], "tile": "8x4", "stack": 256},
+            "tuner_default_ms": tune["default_ms"], "tuner_best_ms": tune["best_ms"]}
 
 
 def _train_step_single(ctx, scene, v, img, tgt, dl, gout):
@@ -331,6 +340,7 @@ def extra_batched_fwd_bwd(ctx, pg, amin, reps: int = 1):
     def plain():
         for s_, u_, w_, h_, p_ in items:
             ctx.render_device(s_, u_, w_, h_, p_, asynchronous=True)
+    tune = ctx.autotune_batch([(s_, u_, w_, h_) for s_, u_, w_, h_, _ in items])
     step()
     plain()
     tfb = _time_device(ctx, step, reps)
@@ -343,6 +353,8 @@ def extra_batched_fwd_bwd(ctx, pg, amin, reps: int = 1):
     return {"workload": "1M Gaussians (64 clusters), 32 views 640x480-1920x1080, k=16, L2 loss vs perturbed scene",
             "rays": rays, "batched_fwd_bwd_ms": tfb, "plain_fwd_ms": tp, "ratio": tfb / tp,
             "checkpoint_fwd_ms": tfc, "adjoint_ms": info.get("bwd_ms"),
+            "shape": {"kernel": "tile packets" if tune["block_threads"] == 32 else "warp per ray",
+                      "kbuf": tune["kbuf"], "handoff_after": tune["handoff_after"]},
             "mode": "checkpoint" if info.get("used_mode") == 1 else "replay"}
 
 
@@ -414,7 +426,9 @@ def main():
 
     from gtrace.tracer import Context, Scene
     ctx = Context(local)
+    t_sc = time.perf_counter()
     scene = Scene(ctx, pg.gaussiansBuffer, amin)
+    scene_wall_ms = (time.perf_counter() - t_sc) * 1e3
     info = scene.info()
     out_dev = ctx.device_alloc(rays * 16)
     # one synchronous render: counters for the algorithmic byte count
@@ -454,22 +468,33 @@ def main():
     ctx.device_free(out_dev)
 
     peak, peak_kind = load_peaks()
+    clocks = clk_summary = clk.summary()
     k_ms = statistics.mean(ktimes) if ktimes else ms_step
     achieved = alg_bytes / (k_ms * 1e-3) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "trace_traffic.json")
+    # per-render DRAM traffic, warp instructions and L2 hit rate of the trace
+    # launches from the committed ncu summary of this workload
+    prof = {}
+    tpath = os.path.join(ROOT, "profiles", "trace_profile.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get(args.workload)
+            prof = json.load(open(tpath)).get(args.workload, {}) or {}
         except Exception:
-            traffic = None
+            prof = {}
+    traffic = prof.get("dram_bytes_per_render")
+    issue = None
+    dev = ctx.device_attributes()
+    if prof.get("warp_inst_per_render"):
+        mhz = clk_summary["sm_mhz"] or dev["max_sm_mhz"]
+        slots = dev["sm_count"] * 4 * mhz * 1e6 * k_ms * 1e-3  # 4 schedulers an SM, one issue a clock each
+        issue = {"bound": "issue", "achieved_warp_inst": prof["warp_inst_per_render"], "slots": slots,
+                 "frac": prof["warp_inst_per_render"] / slots, "sm_count": dev["sm_count"], "sm_mhz": mhz,
+                 "source": prof.get("source")}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         mr, n, stride, dt, prep = cpu_port_throughput(pg, amin, v, budget_s=args.cpu_budget)
         cpu = {"value": mr, "unit": "Mrays/s", "cores": threads, "kind": "port",
                "sample": f"{n} pixels (every {stride}th pixel in x and y) of the {w}x{h} view, {dt:.1f} s; "
                          f"CPU restatement of the reference traversal"}
-    clocks = clk.summary()
     extras = None
     if rank == 0 and world == 1 and not args.no_extras and args.workload == "clusters-1m-1080p":
         extras = {"batched": extra_batched(ctx), "fwd_bwd": extra_fwd_bwd(ctx),
@@ -479,12 +504,14 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, no dataset)",
             "config": {"workload": desc, "width": w, "height": h, "n_gaussians": int(info["n_particles"]),
                        "n_proxies": int(info["n_kept"]), "k": 16 if "1m" in args.workload else None,
-                       "scene_build_ms": info["build_ms"], "bvh_depth": info["bvh_depth"],
+                       "scene_build_ms": info["build_ms"], "scene_upload_ms": info["upload_ms"],
+                       "scene_create_wall_ms": scene_wall_ms, "bvh_depth": info["bvh_depth"],
                        "l2": "inputs larger than L2 (scene %.0f MB > 126 MB), no flush" % (info["device_bytes"] / 1e6),
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "alg_bytes_per_launch": alg_bytes, "kernel_ms": k_ms,
+                         "l2_hit_pct": prof.get("l2_hit_pct"), "issue": issue,
                          "timed": "a render's trace launches (large views: the tile-packet kernel and the "
                                   "warp-per-ray launch that finishes the rays it hands over)"},
             "cpu_baseline": cpu,

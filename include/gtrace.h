@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define GT_ABI_VERSION 1u
+#define GT_ABI_VERSION 2u
 
 /* ---------------------------------------------------------------- status */
 typedef int32_t gt_status;
@@ -123,7 +123,7 @@ typedef struct gt_scene_info {
   uint32_t _pad;
   float build_ms;         /* device time of the GPU build                         */
   float bounds[6];        /* world AABB of the proxies: min xyz, max xyz          */
-  float _pad2;
+  float upload_ms;        /* host time of the host-to-device copy of the records  */
 } gt_scene_info;
 
 /* ============================================================ context */
@@ -404,10 +404,26 @@ typedef struct gt_tune_result {
   float default_ms;       /* trace time of the default launch shape             */
   uint32_t kbuf;          /* k-buffer entries (see above; raised to k)          */
   uint32_t leaf_batch;    /* queued leaves that start a batch of proxy tests    */
+  uint32_t handoff_after; /* block_threads 32: traversals after which a tile   *
+                           * hands its unfinished rays to a warp-per-ray       *
+                           * launch (0: the default, 3)                         */
+  uint32_t _pad;
 } gt_tune_result;
 
 gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const gt_uniforms* u,
                       uint32_t w, uint32_t h, gt_tune_result* result);
+/* Times launch shapes on a whole batch (the items of a gt_render_batch call:
+ * views, scenes and k as given; the images go to a scratch buffer of the
+ * context, out_rgba is not written) and caches the fastest for batches of
+ * that shape (the same view count, tile count and k bucket), which
+ * gt_render_batch and the checkpointing forward of a batch then use ahead of
+ * the per-view cache.  Tried: the tile packets with k-buffers of k, 24, 32,
+ * 48 and 64 entries and hand-offs after 2, 3, 4 and 6 traversals, and a warp
+ * per ray at 4 and 8 blocks per SM.  The tile (8 x 4) and the traversal stack
+ * (256 entries) are fixed: other tiles measured within 0.3 %, and a smaller
+ * stack would turn deep packets into GT_ERR_STACK_OVERFLOW. */
+gt_status gt_autotune_batch(gt_context* ctx, const gt_batch_item* items, uint32_t count,
+                            gt_tune_result* result);
 /* Installs a launch shape for the bucket of (scene, u->k, w x h) without
  * timing anything (for example one found by gt_autotune in an earlier run).
  * block_threads must be 32 or 128 and the tile 8 x 4; blocks_per_sm 1..32,
@@ -450,6 +466,10 @@ gt_status gt_timer_stop(gt_context* ctx, float* ms);
 gt_status gt_kernel_times(gt_context* ctx, float* out_ms, uint32_t max, uint32_t* n);
 /* Number of kernel launches the library has made on this context. */
 gt_status gt_launch_count(const gt_context* ctx, uint64_t* n);
+/* The context's GPU: streaming multiprocessors and the SM clock the driver
+ * reports as its maximum (kHz), for issue-rate rooflines.  Either pointer
+ * may be NULL. */
+gt_status gt_device_attributes(const gt_context* ctx, uint32_t* sm_count, uint32_t* max_sm_khz);
 
 #ifdef __cplusplus
 }

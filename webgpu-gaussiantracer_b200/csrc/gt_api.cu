@@ -5,10 +5,12 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
 #include <map>
 #include <mutex>
 #include <set>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -189,25 +191,36 @@ static std::tuple<uint64_t, uint32_t, uint32_t, uint32_t> tune_key(const gt_scen
                          (uint32_t)log2((double)std::max<uint64_t>((uint64_t)w * h, 1)), kmax_for(k), 0u);
 }
 
-static LaunchShape shape_for(gt_context* ctx, const gt_scene* s, uint32_t w, uint32_t h, uint32_t k) {
+// The launch shape a tuning result stands for.
+static LaunchShape shape_of(const gt_tune_result& r) {
   LaunchShape sh;
-  auto it = ctx->tune.find(tune_key(s, w, h, k));
-  if (it != ctx->tune.end()) {
-    // block_threads 32: tile packets with this k-buffer; 128: a warp per ray
-    sh.packet = it->second.block_threads == 32 ? 1u : 0u;
-    if (sh.packet)
-      sh.packet_kbuf = it->second.kbuf;
-    else
-      sh.kbuf = it->second.kbuf;
-    sh.blocks_per_sm = it->second.blocks_per_sm;
-    sh.leaf_batch = it->second.leaf_batch;
-  }
+  // block_threads 32: tile packets with this k-buffer; 128: a warp per ray
+  sh.packet = r.block_threads == 32 ? 1u : 0u;
+  if (sh.packet)
+    sh.packet_kbuf = r.kbuf;
+  else
+    sh.kbuf = r.kbuf;
+  sh.blocks_per_sm = r.blocks_per_sm;
+  sh.leaf_batch = r.leaf_batch;
+  if (r.handoff_after) sh.handoff_after = r.handoff_after;
   return sh;
+}
+
+static LaunchShape shape_for(gt_context* ctx, const gt_scene* s, uint32_t w, uint32_t h, uint32_t k) {
+  auto it = ctx->tune.find(tune_key(s, w, h, k));
+  return it != ctx->tune.end() ? shape_of(it->second) : LaunchShape();
 }
 
 namespace gt {
 LaunchShape api_shape_for(gt_context* ctx, const gt_scene* s, uint32_t w, uint32_t h, uint32_t k) {
   return shape_for(ctx, s, w, h, k);
+}
+LaunchShape api_batch_shape_for(gt_context* ctx, const gt_scene* const* scenes, const gt_uniforms* us,
+                                const uint32_t* ws, const uint32_t* hs, uint32_t count, uint32_t total_tiles) {
+  uint32_t kmax = 8;
+  for (uint32_t i = 0; i < count; ++i) kmax = std::max(kmax, kmax_for(us[i].k));
+  auto bt = ctx->batch_tune.find(std::make_tuple(count, total_tiles, kmax));
+  return bt != ctx->batch_tune.end() ? shape_of(bt->second) : shape_for(ctx, scenes[0], ws[0], hs[0], us[0].k);
 }
 void api_fill_stats(const DevCounters& c, gt_render_stats* st) { fill_stats(c, st); }
 gt_status api_ensure_views(gt_context* ctx, uint32_t n) { return ensure_views(ctx, n); }
@@ -284,6 +297,10 @@ extern "C" gt_status gt_context_destroy(gt_context* ctx) {
   cudaFree(ctx->d_handoff);
   cudaFreeHost(ctx->h_views);
   cudaFree(ctx->staging);
+  for (int b = 0; b < 2; ++b) {
+    if (ctx->up_pinned[b]) cudaFreeHost(ctx->up_pinned[b]);
+    if (ctx->up_done[b]) cudaEventDestroy(ctx->up_done[b]);
+  }
   for (cudaEvent_t ev : {ctx->call0, ctx->call1, ctx->timer0, ctx->timer1, ctx->int0, ctx->int1})
     if (ev) cudaEventDestroy(ev);
   for (int i = 0; i < 2 * kEventRing; ++i)
@@ -303,6 +320,50 @@ extern "C" gt_status gt_last_error(const gt_context* ctx, char* buf, size_t len)
 }
 
 // ================================================================ scene
+// Host-to-device copy of a host buffer through two pinned 16 MB chunks of the
+// context: the host copies chunk i into one pinned buffer (several threads)
+// while the DMA engine moves chunk i-1 out of the other, so a pageable
+// source streams at close to host memcpy speed instead of the driver's
+// staged pageable copy.  Each chunk is one cudaMemcpyAsync on the context
+// stream.
+constexpr size_t kUploadChunk = 16u << 20;
+
+static void host_copy_parallel(unsigned char* dst, const unsigned char* src, size_t bytes) {
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t nt = std::min<size_t>(std::min<unsigned>(hw, 8u), std::max<size_t>(1, bytes >> 21));
+  if (nt <= 1) {
+    memcpy(dst, src, bytes);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t per = (bytes + nt - 1) / nt;
+  for (size_t t = 0; t < nt; ++t) {
+    const size_t b = t * per, e = std::min(bytes, b + per);
+    if (b < e) th.emplace_back([=]() { memcpy(dst + b, src + b, e - b); });
+  }
+  for (auto& x : th) x.join();
+}
+
+static gt_status upload_host(gt_context* ctx, void* dst_dev, const void* src_host, size_t bytes) {
+  if (bytes == 0) return GT_OK;
+  for (int b = 0; b < 2; ++b) {
+    if (!ctx->up_pinned[b])
+      API_CUDA(ctx, cudaHostAlloc((void**)&ctx->up_pinned[b], kUploadChunk, cudaHostAllocDefault));
+    if (!ctx->up_done[b]) API_CUDA(ctx, cudaEventCreateWithFlags(&ctx->up_done[b], cudaEventDisableTiming));
+  }
+  const unsigned char* src = static_cast<const unsigned char*>(src_host);
+  unsigned char* dst = static_cast<unsigned char*>(dst_dev);
+  for (size_t off = 0, i = 0; off < bytes; off += kUploadChunk, ++i) {
+    const int b = (int)(i & 1);
+    const size_t len = std::min(kUploadChunk, bytes - off);
+    API_CUDA(ctx, cudaEventSynchronize(ctx->up_done[b]));  // the chunk's previous copy has left
+    host_copy_parallel(ctx->up_pinned[b], src + off, len);
+    API_CUDA(ctx, cudaMemcpyAsync(dst + off, ctx->up_pinned[b], len, cudaMemcpyHostToDevice, ctx->stream));
+    API_CUDA(ctx, cudaEventRecord(ctx->up_done[b], ctx->stream));
+  }
+  return GT_OK;
+}
+
 extern "C" gt_status gt_scene_create(gt_context* ctx, const void* packed, uint64_t n, uint32_t stride_bytes,
                                      double alpha_min, uint32_t flags, gt_scene** out) {
   return gt_scene_create_ex(ctx, packed, n, stride_bytes, alpha_min, nullptr, flags, out);
@@ -322,29 +383,41 @@ extern "C" gt_status gt_scene_create_ex(gt_context* ctx, const void* packed, uin
   API_CUDA(ctx, cudaSetDevice(ctx->device));
   const void* dev = packed;
   void* tmp = nullptr;
+  double* act_tmp = nullptr;
+  // stream-ordered temporaries (the context's pool keeps their memory cached)
+  auto drop_tmps = [&]() {
+    if (tmp) cudaFreeAsync(tmp, ctx->stream);
+    if (act_tmp) cudaFreeAsync(act_tmp, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+  };
+  const auto up0 = std::chrono::steady_clock::now();
   if (n > 0 && !(flags & GT_FLAG_INPUT_DEVICE)) {
-    API_CUDA(ctx, cudaMalloc(&tmp, n * (uint64_t)stride_bytes));
-    cudaError_t e = cudaMemcpyAsync(tmp, packed, n * (uint64_t)stride_bytes, cudaMemcpyHostToDevice, ctx->stream);
-    if (e != cudaSuccess) {
-      cudaFree(tmp);
-      return fail(ctx, GT_ERR_CUDA, std::string("upload of the packed buffer: ") + cudaGetErrorString(e));
+    API_CUDA(ctx, cudaMallocAsync(&tmp, n * (uint64_t)stride_bytes, ctx->stream));
+    gt_status ust = upload_host(ctx, tmp, packed, n * (uint64_t)stride_bytes);
+    if (ust != GT_OK) {
+      drop_tmps();
+      return ust;
     }
     dev = tmp;
   }
   const double* act = activated;
-  double* act_tmp = nullptr;
   if (n > 0 && activated && !(flags & GT_FLAG_INPUT_DEVICE)) {
-    cudaError_t e = cudaMalloc(&act_tmp, n * 8 * sizeof(double));
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(act_tmp, activated, n * 8 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream);
+    cudaError_t e = cudaMallocAsync((void**)&act_tmp, n * 8 * sizeof(double), ctx->stream);
     if (e != cudaSuccess) {
-      cudaFree(act_tmp);
-      cudaFree(tmp);
+      act_tmp = nullptr;
+      drop_tmps();
       return fail(ctx, e == cudaErrorMemoryAllocation ? GT_ERR_OOM : GT_ERR_CUDA,
                   std::string("upload of the activated values: ") + cudaGetErrorString(e));
     }
+    gt_status ust = upload_host(ctx, act_tmp, activated, n * 8 * sizeof(double));
+    if (ust != GT_OK) {
+      drop_tmps();
+      return ust;
+    }
     act = act_tmp;
   }
+  const float upload_ms =
+      std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - up0).count();
   gt_scene* s = new gt_scene();
   s->ctx = ctx;
   s->n = n;
@@ -354,15 +427,14 @@ extern "C" gt_status gt_scene_create_ex(gt_context* ctx, const void* packed, uin
   Err e = build_scene(dev, n, stride_bytes, alpha_min, ctx->stream, &s->b, &ctx->launches,
                       (flags & GT_FLAG_FAST_BUILD) != 0, act);
   cudaEventRecord(ctx->call1, ctx->stream);
-  cudaStreamSynchronize(ctx->stream);
-  if (tmp) cudaFree(tmp);
-  if (act_tmp) cudaFree(act_tmp);
+  drop_tmps();
   if (e.code != GT_OK) {
     free_scene(&s->b);
     delete s;
     return fail(ctx, e);
   }
   cudaEventElapsedTime(&s->build_ms, ctx->call0, ctx->call1);
+  s->upload_ms = upload_ms;
   ctx->scenes.insert(s);
   *out = s;
   return GT_OK;
@@ -412,6 +484,7 @@ extern "C" gt_status gt_scene_get_info(const gt_scene* s, gt_scene_info* info) {
   info->device_bytes = s->b.bytes;
   info->bvh_depth = s->b.depth;
   info->build_ms = s->build_ms;
+  info->upload_ms = s->upload_ms;
   for (int a = 0; a < 6; ++a) info->bounds[a] = s->b.bounds[a];
   return GT_OK;
 }
@@ -656,8 +729,11 @@ extern "C" gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items
   API_CUDA(ctx, cudaEventRecord(ctx->call0, ctx->stream));
   uint64_t slot = ring_slot(ctx);
   API_CUDA(ctx, cudaEventRecord(ctx->ring[2 * slot], ctx->stream));
-  // One graph per batch shape: counter reset + the persistent kernel.
-  LaunchShape shape = shape_for(ctx, items[0].scene, items[0].w, items[0].h, items[0].u.k);
+  // One graph per batch shape: counter reset + the persistent kernel.  A
+  // shape tuned for batches of this shape (gt_autotune_batch) comes first.
+  auto bt = ctx->batch_tune.find(std::make_tuple(count, total_tiles, kmax));
+  LaunchShape shape = bt != ctx->batch_tune.end() ? shape_of(bt->second)
+                                                  : shape_for(ctx, items[0].scene, items[0].w, items[0].h, items[0].u.k);
   // the view table is rebuilt on every call: it takes the shape's k-buffer
   // size and leaf batch here, and the graph's kernel matches its slot count
   const bool packet = packet_launch(ctx->h_views, count, total_tiles, ctx->num_sms, shape, false);
@@ -828,7 +904,122 @@ extern "C" gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const g
   r.default_ms = def;
   r.kbuf = std::max(best_sh.packet ? best_sh.packet_kbuf : best_sh.kbuf, k);
   r.leaf_batch = best_sh.leaf_batch;
+  r.handoff_after = best_sh.handoff_after;
   ctx->tune[tune_key(scene, w, h, k)] = r;
+  if (result) *result = r;
+  return GT_OK;
+}
+
+extern "C" gt_status gt_autotune_batch(gt_context* ctx, const gt_batch_item* items, uint32_t count,
+                                       gt_tune_result* result) {
+  if (!ctx) return fail(nullptr, GT_ERR_INVALID_ARG, "context is NULL");
+  if (count == 0 || !items) return fail(ctx, GT_ERR_INVALID_ARG, "empty batch");
+  API_CUDA(ctx, cudaSetDevice(ctx->device));
+  uint64_t slots_all = 0, pixels = 0;
+  uint32_t kmax = 8, kmin = 32;
+  for (uint32_t i = 0; i < count; ++i) {
+    const gt_batch_item& it = items[i];
+    if (!it.scene || it.scene->ctx != ctx) return fail(ctx, GT_ERR_INVALID_ARG, "batch item scene invalid");
+    gt_status st = check_uniforms(ctx, &it.u);
+    if (st != GT_OK) return st;
+    if (it.w == 0 || it.h == 0 || (uint64_t)it.w * it.h > (1ull << 31))
+      return fail(ctx, GT_ERR_INVALID_ARG, "batch item image invalid");
+    slots_all += view_slots(it.w, it.h);
+    if (slots_all > kMaxSlots) return fail(ctx, GT_ERR_INVALID_ARG, "batch larger than 2^31 work slots");
+    pixels += (uint64_t)it.w * it.h;
+    kmax = std::max(kmax, kmax_for(it.u.k));
+    kmin = std::min(kmin, std::max(1u, it.u.k));
+  }
+  gt_status st = ensure_views(ctx, count);
+  if (st != GT_OK) return st;
+  st = ensure_staging(ctx, pixels * sizeof(float4));
+  if (st != GT_OK) return st;
+  Handoff hand;
+  st = ensure_handoff(ctx, pixels, &hand);
+  if (st != GT_OK) return st;
+  // the view table as gt_render_batch builds it (views of one scene back to
+  // back), images into the scratch buffer
+  std::vector<uint32_t> order(count);
+  for (uint32_t i = 0; i < count; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](uint32_t a, uint32_t b) { return items[a].scene < items[b].scene; });
+  uint32_t total_tiles = 0;
+  size_t off = 0;
+  for (uint32_t q = 0; q < count; ++q) {
+    const gt_batch_item& it = items[order[q]];
+    ctx->h_views[q] = make_view(it.scene, it.u, it.w, it.h, ctx->staging + off, total_tiles);
+    total_tiles += ctx->h_views[q].n_tiles;
+    off += (size_t)it.w * it.h;
+  }
+  auto time_shape = [&](const LaunchShape& sh, int reps, float* out_ms) -> gt_status {
+    float ms_min = 1e30f;
+    for (int rep = 0; rep < reps; ++rep) {
+      API_CUDA(ctx, cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), ctx->stream));
+      API_CUDA(ctx, cudaEventRecord(ctx->int0, ctx->stream));
+      Err e = launch_trace(ctx->h_views, count, total_tiles, ctx->d_ctr, ctx->faces, sh, ctx->num_sms, ctx->stream,
+                           &ctx->launches, ctx->d_views, nullptr, &hand);
+      if (e.code != GT_OK) return fail(ctx, e);
+      API_CUDA(ctx, cudaEventRecord(ctx->int1, ctx->stream));
+      API_CUDA(ctx, cudaEventSynchronize(ctx->int1));
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, ctx->int0, ctx->int1);
+      ms_min = std::min(ms_min, ms);
+    }
+    *out_ms = ms_min;
+    return GT_OK;
+  };
+  // the shape gt_render_batch takes without a batch result
+  const LaunchShape def_sh = shape_for(ctx, items[0].scene, items[0].w, items[0].h, items[0].u.k);
+  float def = 0.0f;
+  st = time_shape(def_sh, 2, &def);  // (the first launches also warm the caches)
+  if (st != GT_OK) return st;
+  st = time_shape(def_sh, 2, &def);
+  if (st != GT_OK) return st;
+  LaunchShape best_sh = def_sh;
+  float best = def;
+  const uint32_t pkbufs[] = {kmin, 24u, 32u, 48u, 64u};
+  const uint32_t hands[] = {2u, 3u, 4u, 6u};
+  for (int i = 0; i < 5; ++i) {
+    if (pkbufs[i] < kmin || (i > 0 && pkbufs[i] == kmin)) continue;
+    for (uint32_t ha : hands) {
+      LaunchShape sh;
+      sh.packet = 1;
+      sh.packet_kbuf = std::min(kMaxPacketKbuf, pkbufs[i]);
+      sh.handoff_after = ha;
+      float ms = 0.0f;
+      st = time_shape(sh, 2, &ms);
+      if (st != GT_OK) return st;
+      if (ms < best) {
+        best = ms;
+        best_sh = sh;
+      }
+    }
+  }
+  for (uint32_t b : {4u, 8u}) {
+    LaunchShape sh;
+    sh.packet = 0;
+    sh.blocks_per_sm = b;
+    float ms = 0.0f;
+    st = time_shape(sh, 2, &ms);
+    if (st != GT_OK) return st;
+    if (ms < best) {
+      best = ms;
+      best_sh = sh;
+    }
+  }
+  gt_tune_result r;
+  memset(&r, 0, sizeof r);
+  const bool pk = packet_launch(ctx->h_views, count, total_tiles, ctx->num_sms, best_sh, false);
+  r.block_threads = pk ? 32u : 128u;
+  r.blocks_per_sm = best_sh.blocks_per_sm;
+  r.tile_w = 8;
+  r.tile_h = 4;
+  r.best_ms = best;
+  r.default_ms = def;
+  r.kbuf = pk ? best_sh.packet_kbuf : best_sh.kbuf;
+  r.leaf_batch = best_sh.leaf_batch;
+  r.handoff_after = best_sh.handoff_after;
+  ctx->batch_tune[std::make_tuple(count, total_tiles, kmax)] = r;
   if (result) *result = r;
   return GT_OK;
 }
@@ -845,6 +1036,7 @@ extern "C" gt_status gt_set_tune(gt_context* ctx, const gt_scene* scene, const g
   if (shape->blocks_per_sm < 1 || shape->blocks_per_sm > 32 || shape->kbuf < 1 || shape->kbuf > kMaxKbuf ||
       shape->leaf_batch < 1 || shape->leaf_batch > 32)
     return fail(ctx, GT_ERR_INVALID_ARG, "blocks_per_sm and leaf_batch must lie in 1..32, kbuf in 1..128");
+  if (shape->handoff_after > 64) return fail(ctx, GT_ERR_INVALID_ARG, "handoff_after must be at most 64");
   gt_tune_result r = *shape;
   ctx->tune[tune_key(scene, w, h, u->k)] = r;
   return GT_OK;
@@ -853,6 +1045,7 @@ extern "C" gt_status gt_set_tune(gt_context* ctx, const gt_scene* scene, const g
 extern "C" gt_status gt_autotune_reset(gt_context* ctx) {
   if (!ctx) return GT_ERR_INVALID_ARG;
   ctx->tune.clear();
+  ctx->batch_tune.clear();
   return GT_OK;
 }
 
@@ -929,5 +1122,19 @@ extern "C" gt_status gt_kernel_times(gt_context* ctx, float* out_ms, uint32_t ma
 extern "C" gt_status gt_launch_count(const gt_context* ctx, uint64_t* n) {
   if (!ctx || !n) return GT_ERR_INVALID_ARG;
   *n = ctx->launches;
+  return GT_OK;
+}
+
+extern "C" gt_status gt_device_attributes(const gt_context* ctx, uint32_t* sm_count, uint32_t* max_sm_khz) {
+  if (!ctx) return GT_ERR_INVALID_ARG;
+  if (sm_count) *sm_count = (uint32_t)ctx->num_sms;
+  if (max_sm_khz) {
+    int khz = 0;
+    if (cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, ctx->device) != cudaSuccess) {
+      (void)cudaGetLastError();
+      return GT_ERR_CUDA;
+    }
+    *max_sm_khz = (uint32_t)khz;
+  }
   return GT_OK;
 }

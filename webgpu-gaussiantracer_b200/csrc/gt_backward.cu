@@ -551,7 +551,7 @@ gt_status api_forward_ckpt(gt_context* ctx, const gt_scene* const* scenes, const
   if (!ck.pool_next) CK_TRY(cudaMalloc(&ck.pool_next, 4));
   sst = grow(ctx, (void**)&ck.head, &ck.head_bytes, slots * 4);
   if (sst != GT_OK) return sst;
-  LaunchShape shape = api_shape_for(ctx, scenes[0], ws[0], hs[0], us[0].k);
+  LaunchShape shape = api_batch_shape_for(ctx, scenes, us, ws, hs, count, total_tiles);
   Handoff hand;
   sst = api_ensure_handoff(ctx, rays, &hand);
   if (sst != GT_OK) return sst;

@@ -58,6 +58,9 @@ struct gt_context {
   uint32_t h_views_cap = 0;
   float4* staging = nullptr;
   size_t staging_bytes = 0;
+  // pinned chunks through which host records are uploaded (double-buffered)
+  unsigned char* up_pinned[2] = {nullptr, nullptr};
+  cudaEvent_t up_done[2] = {nullptr, nullptr};
   gt::HandoffRay* d_handoff = nullptr;  // rays tile packets hand to the warp-per-ray kernel
   uint32_t handoff_cap = 0;
   cudaEvent_t call0 = nullptr, call1 = nullptr, timer0 = nullptr, timer1 = nullptr;
@@ -66,6 +69,8 @@ struct gt_context {
   uint64_t ring_head = 0, ring_tail = 0;
   uint64_t launches = 0;
   std::map<std::tuple<uint64_t, uint32_t, uint32_t, uint32_t>, gt_tune_result> tune;
+  // gt_autotune_batch results by (views, tiles, k bucket) of a batch
+  std::map<std::tuple<uint32_t, uint32_t, uint32_t>, gt_tune_result> batch_tune;
   // batch graphs by (views, tiles, k bucket, blocks per SM, k-buffer slots)
   std::map<std::tuple<uint32_t, uint32_t, uint32_t, uint32_t, uint32_t>, gt::GraphEntry> graphs;
   std::set<gt_scene*> scenes;  // live scenes; destroyed with the context
@@ -79,6 +84,7 @@ struct gt_scene {
   uint32_t stride = 0;
   double alpha_min = 0.0;
   float build_ms = 0.0f;
+  float upload_ms = 0.0f;
 };
 
 namespace gt {
@@ -89,6 +95,10 @@ gt_status api_check_uniforms(gt_context* ctx, const gt_uniforms* u);
 ViewDev api_make_view(const gt_scene* s, const gt_uniforms& u, uint32_t w, uint32_t h, float4* out,
                       uint32_t tile_begin);
 LaunchShape api_shape_for(gt_context* ctx, const gt_scene* s, uint32_t w, uint32_t h, uint32_t k);
+// The shape of a batch launch: a gt_autotune_batch result for batches of its
+// shape, else the per-view choice of the first view.
+LaunchShape api_batch_shape_for(gt_context* ctx, const gt_scene* const* scenes, const gt_uniforms* us,
+                                const uint32_t* ws, const uint32_t* hs, uint32_t count, uint32_t total_tiles);
 void api_fill_stats(const DevCounters& c, gt_render_stats* st);
 gt_status api_ensure_views(gt_context* ctx, uint32_t n);
 gt_status api_ensure_handoff(gt_context* ctx, uint64_t rays, Handoff* out);

@@ -59,7 +59,7 @@ class RenderStats(C.Structure):
 class SceneInfo(C.Structure):
     _fields_ = [("n_particles", C.c_uint64), ("n_kept", C.c_uint64), ("device_bytes", C.c_uint64),
                 ("bvh_depth", C.c_uint32), ("_pad", C.c_uint32), ("build_ms", C.c_float),
-                ("bounds", C.c_float * 6), ("_pad2", C.c_float)]
+                ("bounds", C.c_float * 6), ("upload_ms", C.c_float)]
 
 
 class BwdOpts(C.Structure):
@@ -75,7 +75,8 @@ class BatchItem(C.Structure):
 class TuneResult(C.Structure):
     _fields_ = [("block_threads", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("tile_w", C.c_uint32),
                 ("tile_h", C.c_uint32), ("best_ms", C.c_float), ("default_ms", C.c_float),
-                ("kbuf", C.c_uint32), ("leaf_batch", C.c_uint32)]
+                ("kbuf", C.c_uint32), ("leaf_batch", C.c_uint32), ("handoff_after", C.c_uint32),
+                ("_pad", C.c_uint32)]
 
 
 class BvhInfo(C.Structure):
@@ -122,6 +123,7 @@ SIGNATURES = [
     ("gt_tonemap", _i32, [_vp, _vp, _u64, _u32, C.c_float, _vp, _u32]),
     ("gt_l2_loss", _i32, [_vp, _vp, _vp, _u64, _vp, C.POINTER(C.c_double)]),
     ("gt_autotune", _i32, [_vp, _vp, C.POINTER(Uniforms), _u32, _u32, C.POINTER(TuneResult)]),
+    ("gt_autotune_batch", _i32, [_vp, C.POINTER(BatchItem), _u32, C.POINTER(TuneResult)]),
     ("gt_set_tune", _i32, [_vp, _vp, C.POINTER(Uniforms), _u32, _u32, C.POINTER(TuneResult)]),
     ("gt_autotune_reset", _i32, [_vp]),
     ("gt_set_limits", _i32, [_vp, _u32, _u32, _u32]),
@@ -135,6 +137,7 @@ SIGNATURES = [
     ("gt_timer_stop", _i32, [_vp, C.POINTER(C.c_float)]),
     ("gt_kernel_times", _i32, [_vp, C.POINTER(C.c_float), _u32, C.POINTER(_u32)]),
     ("gt_launch_count", _i32, [_vp, C.POINTER(_u64)]),
+    ("gt_device_attributes", _i32, [_vp, C.POINTER(_u32), C.POINTER(_u32)]),
 ]
 
 _lib = None

@@ -222,14 +222,26 @@ class Context:
         r = L.TuneResult()
         self.check(self._lib.gt_autotune(self._h, scene.handle, C.byref(_uniforms(uniforms)), width, height,
                                          C.byref(r)))
-        return {name: getattr(r, name) for name, _ in r._fields_}
+        return {name: getattr(r, name) for name, _ in r._fields_ if not name.startswith("_")}
+
+    def autotune_batch(self, views):
+        """views: list of (scene, uniforms, width, height) -> the fastest launch
+        shape of that batch, cached for later render_batch calls of its shape."""
+        items = (L.BatchItem * len(views))()
+        for i, (scene, uniforms, w, h) in enumerate(views):
+            items[i].scene = scene.handle
+            items[i].u = _uniforms(uniforms)
+            items[i].w, items[i].h = w, h
+        r = L.TuneResult()
+        self.check(self._lib.gt_autotune_batch(self._h, items, len(views), C.byref(r)))
+        return {name: getattr(r, name) for name, _ in r._fields_ if not name.startswith("_")}
 
     def set_tune(self, scene: "Scene", uniforms, width: int, height: int, blocks_per_sm: int = 4,
                  kbuf: int = 32, leaf_batch: int = 32, block_threads: int = 128):
         """Installs a launch shape for this (scene, k, image size) bucket:
         block_threads 32 traces 8x4 tiles of rays per warp (kbuf entries per
         ray), 128 one ray per warp (gt_set_tune)."""
-        r = L.TuneResult(block_threads, blocks_per_sm, 8, 4, 0.0, 0.0, kbuf, leaf_batch)
+        r = L.TuneResult(block_threads, blocks_per_sm, 8, 4, 0.0, 0.0, kbuf, leaf_batch, 0, 0)
         self.check(self._lib.gt_set_tune(self._h, scene.handle, C.byref(_uniforms(uniforms)), width, height,
                                          C.byref(r)))
 
@@ -298,6 +310,12 @@ class Context:
         n = C.c_uint32()
         self.check(self._lib.gt_kernel_times(self._h, buf, max_n, C.byref(n)))
         return [buf[i] for i in range(n.value)]
+
+    def device_attributes(self) -> dict:
+        """SM count and the maximum SM clock (MHz) of the context's GPU."""
+        n, khz = C.c_uint32(), C.c_uint32()
+        self.check(self._lib.gt_device_attributes(self._h, C.byref(n), C.byref(khz)))
+        return {"sm_count": int(n.value), "max_sm_mhz": khz.value / 1000.0}
 
     def launch_count(self) -> int:
         n = C.c_uint64()
