@@ -5,10 +5,13 @@
 // sets, the same compositing arithmetic in the same order.  What differs is
 // how the work is shared out:
 //   * traversal: the warp walks the hierarchy once for all its rays.  A node
-//     is popped when its entry distance (the smallest over the rays that hit
-//     its box) is within the largest far bound of the packet; each lane tests
-//     its own ray against the node's children; an inner child hit by any ray
-//     is pushed (near-first by that entry distance).  Primary rays of one
+//     is popped when its entry distance (a lower bound over the packet's
+//     rays) is within the largest far bound of the packet; eight lanes test
+//     the node's children against the whole packet at once (interval slab
+//     test over the rays' common origin and range of directions, a superset
+//     of the children any ray hits); inner children that pass are pushed
+//     near-first, and each leaf child that passes gets the exact per-ray box
+//     test, whose ballot is the leaf's ray mask.  Primary rays of one
 //     tile are so coherent that the packet visits only ~1.13x the nodes of
 //     one of its rays, so a node visit serves ~28 rays.  The node's 256 bytes
 //     come in one coalesced load into shared memory, issued for the top of
@@ -62,10 +65,12 @@ struct PacketScratch {
   float hq[kMaxHitsPerProxy][32];  // hits of each lane's pair, column per lane
   float dx[32], dy[32], dz[32];    // ray directions
   float tlo[32], thi[32];          // ray intervals; thi = far bound
-  uint32_t hn[32];                 // heap sizes
+  uint8_t hn[32];                  // heap sizes
   float4 nbuf[16];                 // the node being visited
   RayStats stats;
 };
+// 12.7 KB for 32-entry heaps: with the 1 KB the SM reserves per block and
+// 117 registers a thread, 17 one-warp blocks fit an SM
 
 // float -> uint map that preserves order (for warp min/max reductions)
 __device__ __forceinline__ uint32_t ord_f(float x) {
@@ -121,7 +126,7 @@ __device__ __forceinline__ void heap_offer(PacketScratch<KB>& W, uint32_t r, uin
       i = par;
     }
     W.hk[i][r] = x;
-    W.hn[r] = n + 1;
+    W.hn[r] = (uint8_t)(n + 1);
     if (n + 1 == cap) W.thi[r] = key_t(W.hk[0][r]);
   } else {
     if (!(x < W.hk[0][r])) return;
@@ -142,6 +147,77 @@ __device__ __forceinline__ void heap_sort(PacketScratch<KB>& W, uint32_t r, uint
 
 __device__ __forceinline__ float warp_max_f(float x) { return unord_f(__reduce_max_sync(kFull, ord_f(x))); }
 
+// Box test of the whole packet.  All rays of a tile start at the camera, so
+// over the live rays the slab distances (x - o) i of an axis are linear in
+// the inverse direction i and take their extremes at the smallest and largest
+// i of the packet (when i has one sign; an axis whose directions change sign
+// culls nothing).  The interval [near, far] so found contains every live
+// ray's own padded slab interval: the padding pp is 1.25 times the largest
+// per-ray padding, whose extra quarter (>= 1e-6 (|o| + scene size) |i|) is
+// far above the few-ulp difference between (x - o) i rounded here and the
+// per-ray x i - o i.  So the packet test passes whenever some ray's box test
+// passes; it costs one lane per child instead of every lane per child.
+struct PacketBox {
+  float ox, oy, oz;
+  float ax0, ax1, ay0, ay1, az0, az1;  // smallest, largest inverse direction per axis
+  float ppx, ppy, ppz;                 // slab padding per axis
+  float tlo;                           // smallest t_curr of the live rays
+};
+
+__device__ __forceinline__ float warp_min_f(float x) { return unord_f(__reduce_min_sync(kFull, ord_f(x))); }
+
+__device__ __forceinline__ PacketBox make_packet_box(V3 o, const BoxRay& br, bool live, float tlo, float scene_mag) {
+  PacketBox P;
+  P.ox = o.x;
+  P.oy = o.y;
+  P.oz = o.z;
+  const float inf = CUDART_INF_F;
+  P.ax0 = warp_min_f(live ? br.ix : inf);
+  P.ax1 = warp_max_f(live ? br.ix : -inf);
+  P.ay0 = warp_min_f(live ? br.iy : inf);
+  P.ay1 = warp_max_f(live ? br.iy : -inf);
+  P.az0 = warp_min_f(live ? br.iz : inf);
+  P.az1 = warp_max_f(live ? br.iz : -inf);
+  P.tlo = warp_min_f(live ? tlo : inf);
+  // the per-ray padding (make_boxray) with the same origin for every ray
+  const float m = fmaxf(fmaxf(fabsf(o.x), fabsf(o.y)), fabsf(o.z));
+  const float pad = 1.25f * (4e-6f * (m + scene_mag) + 1e-7f);
+  P.ppx = pad * fmaxf(fabsf(P.ax0), fabsf(P.ax1));
+  P.ppy = pad * fmaxf(fabsf(P.ay0), fabsf(P.ay1));
+  P.ppz = pad * fmaxf(fabsf(P.az0), fabsf(P.az1));
+  return P;
+}
+
+__device__ __forceinline__ void packet_slab(float lo, float hi, float o, float i0, float i1, float pp, float& n,
+                                            float& f) {
+  const float dlo = lo - o, dhi = hi - o;
+  if (i0 > 0.f) {
+    n = fminf(dlo * i0, dlo * i1);
+    f = fmaxf(dhi * i0, dhi * i1);
+  } else if (i1 < 0.f) {
+    n = fminf(dhi * i0, dhi * i1);
+    f = fmaxf(dlo * i0, dlo * i1);
+  } else {
+    n = -CUDART_INF_F;
+    f = CUDART_INF_F;
+  }
+  n = n - pp;
+  f = f + pp;
+}
+
+// The per-ray padded box test of the tracers (child box a, b against ray br
+// with interval [tlo, thi]); returns the entry distance through tn.
+__device__ __forceinline__ bool ray_box(const float4 a, const float4 b, const BoxRay& br, float tlo, float thi,
+                                        float& tn) {
+  const float x0 = __fmaf_rn(a.x, br.ix, -br.ox), x1 = __fmaf_rn(a.w, br.ix, -br.ox);
+  const float y0 = __fmaf_rn(a.y, br.iy, -br.oy), y1 = __fmaf_rn(b.x, br.iy, -br.oy);
+  const float z0 = __fmaf_rn(a.z, br.iz, -br.oz), z1 = __fmaf_rn(b.y, br.iz, -br.oz);
+  tn = fmaxf(fmaxf(fminf(x0, x1) - br.px, fminf(y0, y1) - br.py), fmaxf(fminf(z0, z1) - br.pz, tlo));
+  const float tf =
+      fminf(fminf(fmaxf(x0, x1) + br.px, fmaxf(y0, y1) + br.py), fminf(fmaxf(z0, z1) + br.pz, thi));
+  return tn <= tf;
+}
+
 // One traversal of the packet: every live lane's ray collects the cap
 // smallest front-face hits with t in (its t_curr, t_max) into its heap.
 // Lanes that are not live take no part (far bound -inf).
@@ -156,6 +232,7 @@ __device__ __forceinline__ void packet_traverse(const SceneDev& S, const FaceTab
   W.hn[lane] = 0;
   if (S.n_kept == 0) return;
   float thi_max = warp_max_f(thi);
+  const PacketBox P = make_packet_box(o, br, live, tlo, S.scene_mag);
   RayStats& st = W.stats;
   int sp = 1, nq = 0, ns = 0;
   if (lane == 0) {
@@ -192,37 +269,61 @@ __device__ __forceinline__ void packet_traverse(const SceneDev& S, const FaceTab
         W.nbuf[lane] = pf;
       }
       __syncwarp();
-      int ni = 0;
-      float mykey = CUDART_INF_F;
-      uint32_t myref = 0;
-#pragma unroll
-      for (int c = 0; c < 8; ++c) {
+      // lanes 0..7: the packet test of one child each
+      bool phit = false, pleaf = false;
+      float ptn = CUDART_INF_F;
+      uint32_t pref = kInvalid;
+      if (lane < 8) {
+        const float4 a = W.nbuf[2 * lane], b = W.nbuf[2 * lane + 1];
+        pref = __float_as_uint(b.z);
+        float nx, fx, ny, fy, nz, fz;
+        packet_slab(a.x, a.w, P.ox, P.ax0, P.ax1, P.ppx, nx, fx);
+        packet_slab(a.y, b.x, P.oy, P.ay0, P.ay1, P.ppy, ny, fy);
+        packet_slab(a.z, b.y, P.oz, P.az0, P.az1, P.ppz, nz, fz);
+        ptn = fmaxf(fmaxf(nx, ny), fmaxf(nz, P.tlo));
+        const float ptf = fminf(fminf(fx, fy), fminf(fz, thi_max));
+        phit = pref != kInvalid && ptn <= ptf;  // empty slots (packed at the end) never hit
+        pleaf = (pref & kLeafBit) != 0;
+      }
+      // leaf children the packet may hit: each ray's own test gives its mask
+      uint32_t lmask = __ballot_sync(kFull, phit && pleaf);
+      while (lmask) {
+        const int c = __ffs(lmask) - 1;
+        lmask &= lmask - 1;
         const float4 a = W.nbuf[2 * c], b = W.nbuf[2 * c + 1];
-        const uint32_t ref = __float_as_uint(b.z);
-        const float x0 = __fmaf_rn(a.x, br.ix, -br.ox), x1 = __fmaf_rn(a.w, br.ix, -br.ox);
-        const float y0 = __fmaf_rn(a.y, br.iy, -br.oy), y1 = __fmaf_rn(b.x, br.iy, -br.oy);
-        const float z0 = __fmaf_rn(a.z, br.iz, -br.oz), z1 = __fmaf_rn(b.y, br.iz, -br.oz);
-        const float tn =
-            fmaxf(fmaxf(fminf(x0, x1) - br.px, fminf(y0, y1) - br.py), fmaxf(fminf(z0, z1) - br.pz, tlo));
-        const float tf =
-            fminf(fminf(fmaxf(x0, x1) + br.px, fmaxf(y0, y1) + br.py), fminf(fmaxf(z0, z1) + br.pz, thi));
-        const bool hit = ref != kInvalid && tn <= tf;  // empty slots (packed at the end) never hit
+        float tn;
+        const bool hit = ray_box(a, b, br, tlo, thi, tn);
         const uint32_t m = __ballot_sync(kFull, hit);
-        if (m == 0) continue;
-        if (ref & kLeafBit) {
+        if (m) {
           if (lane == 0) {
-            W.lj[nl] = ref & ~kLeafBit;
+            W.lj[nl] = __float_as_uint(b.z) & ~kLeafBit;
             W.lm[nl] = m;
           }
           ++nl;
-        } else {
-          const uint32_t key = __reduce_min_sync(kFull, hit ? ord_f(tn) : 0xFFFFFFFFu);
-          if ((int)lane == ni) {
-            mykey = unord_f(key);
-            myref = ref;
-          }
-          ++ni;
         }
+      }
+      // inner children the packet may hit, keyed by the packet's entry distance
+      const uint32_t imask = __ballot_sync(kFull, phit && !pleaf);
+      const int ni = __popc(imask);
+      float mykey = CUDART_INF_F;
+      uint32_t myref = 0;
+      if (ni > 0) {
+        if (sp + ni > (int)F.lim_stack) {
+          status |= kStatusStackOverflow;
+          return;
+        }
+        // gathered into lanes 0..ni-1 through the free stack slots above sp
+        if ((imask >> lane) & 1u) {
+          const int q = sp + __popc(imask & lt_mask);
+          W.skey[q] = ptn;
+          W.snode[q] = pref;
+        }
+        __syncwarp();
+        if ((int)lane < ni) {
+          mykey = W.skey[sp + (int)lane];
+          myref = W.snode[sp + (int)lane];
+        }
+        __syncwarp();
       }
       if (lane == 0) st.node_visits += 1;
       if (ni > 0) {
