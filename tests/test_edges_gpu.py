@@ -100,10 +100,22 @@ def _proxy_map(osc, j):
     return p, m
 
 
+def _bits(a):
+    """uint32 view of a float32 array with every NaN as one pattern: the
+    reference's float arithmetic turns some extreme proxies' alpha into NaN
+    on both implementations, whose default NaN payloads differ (the CPU's
+    0xFFC00000, the GPU's 0x7FFFFFFF)."""
+    a = np.ascontiguousarray(a, dtype=np.float32).copy()
+    b = a.view(np.uint32)
+    b[np.isnan(a)] = 0x7FC00000
+    return b
+
+
 def _check_views(ctx, rec, amin, views, need_hits=1):
     """Renders every (uniforms, w, h) view with both kernels and the oracle;
-    images bit for bit, hit records of the warp-per-ray kernel bit for bit.
-    Returns the total count of composited entries seen."""
+    images bit for bit, hit records of the warp-per-ray kernel bit for bit
+    (NaNs as one pattern).  Returns the total count of composited entries
+    seen."""
     g = Scene(ctx, rec, amin)
     o = oracle.Scene(rec, amin, "f32")
     total = 0
@@ -116,7 +128,7 @@ def _check_views(ctx, rec, amin, views, need_hits=1):
                     img = ctx.render(g, u, w, h)
                 finally:
                     ctx._lib.gt_autotune_reset(ctx._h)
-                np.testing.assert_array_equal(img.reshape(-1, 4).view(np.uint32), ref.view(np.uint32), err_msg=name)
+                np.testing.assert_array_equal(_bits(img.reshape(-1, 4)), _bits(ref), err_msg=name)
             pix = np.arange(w * h, dtype=np.uint32)
             got = ctx.render_hits(g, u, w, h, pix, max_entries=64)
             np.testing.assert_array_equal(got["count"], hits["count"])
@@ -124,9 +136,8 @@ def _check_views(ctx, rec, amin, views, need_hits=1):
             for q in range(w * h):
                 m = min(int(hits["count"][q]), 64)
                 np.testing.assert_array_equal(got["pidx"][q, :m], hits["pidx"][q, :m])
-                np.testing.assert_array_equal(got["t"][q, :m].view(np.uint32), hits["t"][q, :m].view(np.uint32))
-                np.testing.assert_array_equal(got["alpha"][q, :m].view(np.uint32),
-                                              hits["alpha"][q, :m].view(np.uint32))
+                np.testing.assert_array_equal(_bits(got["t"][q, :m]), _bits(hits["t"][q, :m]))
+                np.testing.assert_array_equal(_bits(got["alpha"][q, :m]), _bits(hits["alpha"][q, :m]))
             total += int(hits["count"].sum())
     finally:
         g.close()
@@ -228,7 +239,11 @@ def test_rays_nearly_in_a_face_plane(ctx):
 
 @pytest.mark.parametrize("ratio", [1e3, 1e4])
 def test_needle_and_disc_proxies(ctx, ratio):
-    """Scale ratios of 1e3 and 1e4 (needles and discs), random orientations."""
+    """Scale ratios of 1e3 and 1e4 (needles and discs), random orientations.
+    At 1e4 the response's float arithmetic (src/GS_shader.ts:111-136: the
+    precision matrix holds 1/s^2 ~ 1e10) loses E to cancellation, so some
+    entries get alpha > 1 and a few pixels NaN, identically on both sides
+    (the FP64 render has none)."""
     rng = np.random.default_rng(int(ratio))
     n = 600
     pos = rng.uniform(-0.6, 0.6, size=(n, 3))

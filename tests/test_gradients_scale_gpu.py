@@ -2,14 +2,16 @@
 
 1. The 200k-Gaussian, 800x800, k = 8 configuration: the CUDA adjoint of the
    L2 loss against the perturbed-scene target, checked against central
-   finite differences (h = 1e-4) of the FP64 oracle render on 256 random
-   (particle, parameter) pairs.  Each +h / -h render covers only the pixels
+   finite differences (h = 1e-4, and h/2 for a Richardson extrapolation) of
+   the FP64 oracle render on 256 random (particle, parameter) pairs.  Each
+   perturbed render covers only the pixels
    whose rays can reach the particle's proxy (its circumscribed sphere,
    sized for the perturbed parameter), which holds every pixel the
-   parameter can change; the oracle scene is rebuilt for each.  Samples
-   whose +h, -h or float hit sequences differ on those pixels (entry lists,
-   which entries pass alpha_min, round counts) straddle a discontinuity of
-   the piecewise-smooth image and are rejected; the test bounds how many.
+   parameter can change; the oracle scene is rebuilt for each.  Pixels
+   whose perturbed or float hit sequences differ (entry lists, which entries
+   pass alpha_min, round counts) straddle a discontinuity of the
+   piecewise-smooth image and are left out of both sides of the comparison;
+   the test reports how many and bounds the samples left without pixels.
 2. The batched forward + backward configuration: views of the 1M-Gaussian
    scene rendered in one checkpointing gt_render_batch and differentiated by
    one gt_backward_batch that sums all views, against the FP64 oracle
@@ -82,14 +84,18 @@ def signature(hits, amin, n):
 
 def fd_samples(rec, amin, u, w, h, g, picks, workers=None):
     """Central differences of sum over S of g * rgba for each (particle, row)
-    pick, S being the pixels of the particle's footprint whose hit sequence
-    (entries, which pass alpha_min, rounds) is the same in the +h and -h FP64
-    renders and in the float render (the one the CUDA kernels reproduce and
-    differentiate).  Pixels outside S sit on a discontinuity of the
-    piecewise-smooth image (or order two hits differently in float and
-    double).  g: (w*h, 4) float64 weights.  Returns (particle, row, fd, S)
-    per pick with a non-empty S, and the numbers of excluded pixels and of
-    picks left without pixels."""
+    pick, with steps h and h/2, and their Richardson extrapolation
+    (4 D(h/2) - D(h)) / 3, S being the pixels of the particle's footprint
+    whose hit sequence (entries, which pass alpha_min, rounds) is the same in
+    the four FP64 renders and in the float render (the one the CUDA kernels
+    reproduce and differentiate).  Pixels outside S sit on a discontinuity of
+    the piecewise-smooth image (or order two hits differently in float and
+    double).  The extrapolation matters for the smallest Gaussians: with
+    scales of e^-5 and rays at a few standard deviations, the h^2 term of a
+    plain central difference alone reaches 1e-3.  g: (w*h, 4) float64
+    weights.  Returns (particle, row, D(h), extrapolated, S) per pick with a
+    non-empty S, and the numbers of excluded pixels and of picks left
+    without pixels."""
     o, dirs = ray_dirs(u, w, h)
     base = oracle.Scene(rec, amin, "f32")
     max_e = 1024
@@ -108,31 +114,33 @@ def fd_samples(rec, amin, u, w, h, g, picks, workers=None):
         x = rec[p, col]
         _, h0 = base.render(u, w, h, pixels=pix, threads=1, max_entries=max_e)
         res = []
-        for step in (H_STEP, -H_STEP):
+        for step in (H_STEP, -H_STEP, 0.5 * H_STEP, -0.5 * H_STEP):
             r[p, col] = np.float32(x + step)
             s64 = oracle.Scene(r, amin, "f64")
             img, hh = s64.render(u, w, h, pixels=pix, threads=1, max_entries=max_e)
             res.append((float(r[p, col]), img, signature(hh, amin, len(pix)), int(hh["count"].max())))
             del s64
         r[p, col] = x
-        (xp, ip, sp, mp), (xm, im, sm, mm) = res
-        if max(mp, mm, int(h0["count"].max())) > max_e:
+        if max([m for *_, m in res] + [int(h0["count"].max())]) > max_e:
             return None
-        keep = np.array([a == b == c for a, b, c in zip(sp, sm, signature(h0, amin, len(pix)))], bool)
-        fd = float(((ip - im)[keep] * g[pix[keep]]).sum()) / (xp - xm)
-        return (p, i, fd, pix[keep], int((~keep).sum()))
+        sig0 = signature(h0, amin, len(pix))
+        keep = np.array([all(rr[2][q] == sig0[q] for rr in res) for q in range(len(pix))], bool)
+        gk = g[pix[keep]]
+        d1 = float(((res[0][1] - res[1][1])[keep] * gk).sum()) / (res[0][0] - res[1][0])
+        d2 = float(((res[2][1] - res[3][1])[keep] * gk).sum()) / (res[2][0] - res[3][0])
+        return (p, i, d1, (4.0 * d2 - d1) / 3.0, pix[keep], int((~keep).sum()))
 
     out, excluded, empty = [], 0, 0
     with cf.ThreadPoolExecutor(workers) as ex:
         for res in ex.map(one, picks):
             if res is None:
                 continue
-            p, i, fd, keep, nx = res
+            p, i, d1, dx, keep, nx = res
             excluded += nx
             if len(keep) == 0:
                 empty += 1
             else:
-                out.append((p, i, fd, keep))
+                out.append((p, i, d1, dx, keep))
     return out, excluded, empty
 
 
@@ -159,20 +167,25 @@ def test_fd_differentiable_config(ctx):
         # checkpoint of the render above reused
         gm = np.zeros_like(g)
         row_max = np.abs(grad).max(axis=1)
-        errs = []
-        for p, i, fd, keep in samples:
+        err_c, err_x, worst = [], [], []
+        for p, i, d1, dx, keep in samples:
             gm[keep] = g[keep]
             an = float(ctx.backward(s, v.uniforms, w, h, gm, reuse_checkpoint=True)[0][i, p])
             gm[keep] = 0.0
-            errs.append(abs(fd - an) / max(abs(fd), abs(an), 1e-4 * row_max[i]))
+            floor = 1e-4 * row_max[i]
+            err_c.append(abs(d1 - an) / max(abs(d1), abs(an), floor))
+            err_x.append(abs(dx - an) / max(abs(dx), abs(an), floor))
+            worst.append((err_x[-1], p, i, dx, d1, an))
     finally:
         s.close()
         t.close()
-    errs = np.array(errs)
+    err_c, err_x = np.array(err_c), np.array(err_x)
     print(f"FD at 200k/800x800: {len(samples)} of {len(picks)} samples, {excluded} footprint pixels excluded, "
-          f"{empty} samples without pixels; relative error max {errs.max():.2e}, median {np.median(errs):.2e}")
+          f"{empty} samples without pixels; relative error, central h = 1e-4: max {err_c.max():.2e}, median "
+          f"{np.median(err_c):.2e}; extrapolated from h and h/2: max {err_x.max():.2e}, median {np.median(err_x):.2e}")
     assert len(samples) >= 0.9 * len(picks), (len(samples), empty)
-    assert errs.max() <= 1e-3, errs.max()
+    assert err_x.max() <= 1e-3, sorted(worst, reverse=True)[:5]
+    assert np.median(err_c) <= 1e-4
 
 
 def _check_rows(got, ref, rel=1e-3):

@@ -372,6 +372,11 @@ __global__ void __launch_bounds__(128) k_expand(const float4* __restrict__ G, co
   const float s[3] = {sa.x, sa.y, sa.z};
   const float qw = qa.x, qx = qa.y, qy = qa.z, qz = qa.w;
   float head[11];
+  // particles without composited entries (among them those below the opacity
+  // cut, whose scales may be 0) have zero sums: their response terms are 0
+  const bool any = r0.x != 0.f || r0.y != 0.f || r0.z != 0.f || r0.w != 0.f || r1.x != 0.f || r1.y != 0.f ||
+                   r1.z != 0.f || r1.w != 0.f || r2.x != 0.f || r2.y != 0.f || r2.z != 0.f || r2.w != 0.f ||
+                   r3.x != 0.f || r3.y != 0.f || r3.z != 0.f || r3.w != 0.f;
   head[0] = 2.f * r0.x;
   head[1] = 2.f * r0.y;
   head[2] = 2.f * r0.z;
@@ -393,6 +398,9 @@ __global__ void __launch_bounds__(128) k_expand(const float4* __restrict__ G, co
                    qw * GR[2][0] + qz * GR[2][1] - 2.f * qy * GR[2][2]);
   head[9] = 2.f * (-2.f * qz * GR[0][0] - qw * GR[0][1] + qx * GR[0][2] + qw * GR[1][0] - 2.f * qz * GR[1][1] +
                    qy * GR[1][2] + qx * GR[2][0] + qy * GR[2][1]);
+  if (!any)
+#pragma unroll
+    for (int i = 3; i < 10; ++i) head[i] = 0.f;
   // SH coefficients, B_k(dir) sum gc, and the position term of dir
   float gsh[48];
 #pragma unroll
