@@ -224,18 +224,27 @@ __device__ __forceinline__ void agg_flush(AggTable& A, float4* G, float4* GS, ui
 }
 
 // The adjoint, one warp per 8x4 tile of ray slots (the forward's slot
-// numbering): the tiles [tile_begin, tile_end) of the launch's views, the
-// 32 rays of a tile one after the other, each round's entries across the
-// lanes; the tile's per-particle sums gather in the warp's table.
-template <bool CKPT_PIDX>
+// numbering): the tiles [tile_begin, tile_end) of the launch's views.  The
+// warp splits into 32 / SEG segments of SEG lanes, each walking one of the
+// tile's rays (a round's k <= SEG entries across its lanes), so that small k
+// keeps the lanes busy (k = 8: four rays at a time); the tile's per-particle
+// sums gather in the warp's table.  Replay mode (the entries found again by
+// a warp-wide traversal) runs with SEG = 32.
+template <bool CKPT_PIDX, int SEG>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewDev* __restrict__ views,
                                                                     uint32_t n_views, uint32_t tile_begin,
                                                                     uint32_t tile_end, DevCounters* ctr,
                                                                     const __grid_constant__ FaceTable F,
                                                                     const Ckpt ck) {
+  static_assert(SEG == 8 || SEG == 16 || SEG == 32, "segment width");
+  static_assert(CKPT_PIDX || SEG == 32, "replay traverses with the whole warp");
+  constexpr uint32_t kGroups = 32 / SEG;
   __shared__ WarpScratch scratch[kWarpsPerBlock];
   __shared__ AggTable tables[kWarpsPerBlock];
   const uint32_t lane = threadIdx.x & 31;
+  const uint32_t seg = lane / SEG, sl_lane = lane % SEG;
+  const uint32_t seg_shift = seg * SEG;
+  const uint32_t seg_bits = SEG == 32 ? kFull : ((1u << SEG) - 1u);
   WarpScratch& W = scratch[threadIdx.x >> 5];
   AggTable& A = tables[threadIdx.x >> 5];
   RayStats& st = W.stats;
@@ -250,44 +259,65 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewD
     tile += tile_begin;
     const uint32_t vi = n_views == 1 ? 0u : find_view(views, n_views, tile);
     const ViewDev& V = views[vi];
+    const uint32_t k = V.u.k;
     uint32_t nfill = 0;  // particles in the table
-    for (uint32_t sl = 0; sl < 32; ++sl) {
+    for (uint32_t base = 0; base < 32; base += kGroups) {
+      // this segment's ray
+      const uint32_t sl = base + seg;
       const uint32_t item = 32u * tile + sl;
       uint32_t px, py;
       tile_pixel(V.tiles_x, tile - V.tile_begin, sl, px, py);
-      if (px >= V.w || py >= V.h) continue;
-      uint32_t rec = ck.head[item];
-      if (rec == kInvalid) continue;
-      const float4 g4 = V.dL[(size_t)py * V.w + px];
-      if (g4.x == 0.f && g4.y == 0.f && g4.z == 0.f) continue;
-      const float g[3] = {g4.x, g4.y, g4.z};
-      V3 o, d;
-      ray_gen(V.u, V.w, V.h, px, py, o, d);
+      uint32_t rec = kInvalid;
+      float g[3] = {0.f, 0.f, 0.f};
+      if (px < V.w && py < V.h) {
+        const float4 g4 = V.dL[(size_t)py * V.w + px];
+        if (g4.x != 0.f || g4.y != 0.f || g4.z != 0.f) {
+          rec = ck.head[item];
+          g[0] = g4.x;
+          g[1] = g4.y;
+          g[2] = g4.z;
+        }
+      }
+      V3 o = mk(0.f, 0.f, 0.f), d = mk(0.f, 0.f, 1.f);
+      if (rec != kInvalid) ray_gen(V.u, V.w, V.h, px, py, o, d);
       const BoxRay br = make_boxray(o, d, V.s.scene_mag);
-      const uint32_t k = V.u.k;
+      if (rec != kInvalid && sl_lane == 0) ++rays;
       float R0 = 0.f, R1 = 0.f, R2 = 0.f;
-      ++rays;
-      // rounds from the last to the first along the record links
-      for (uint32_t guard = 0; rec != kInvalid && guard < ck.pool_cap; ++guard) {
-        const uint32_t* rr = ck.pool + (size_t)rec * (kCkptHeader + ck.kc);
-        const float2 ri = make_float2(__uint_as_float(rr[0]), __uint_as_float(rr[1]));
-        const uint32_t prev = rr[2], nrec = rr[3];
-        uint32_t p = kInvalid;
-        bool valid;
+      // rounds from the last to the first along the record links, all
+      // segments in step (a segment whose ray is done idles)
+      for (uint32_t guard = 0; guard < ck.pool_cap; ++guard) {
+        const bool active = rec != kInvalid;
+        if (!__any_sync(kFull, active)) break;
+        uint32_t p = kInvalid, nrec = 0;
+        float2 ri = make_float2(0.f, 0.f);
+        bool valid = false;
         if (CKPT_PIDX) {
-          p = lane < ck.kc ? rr[kCkptHeader + lane] : kInvalid;
-          valid = lane < nrec && p != kInvalid;
+          if (active) {
+            const uint32_t* rr = ck.pool + (size_t)rec * (kCkptHeader + ck.kc);
+            ri = make_float2(__uint_as_float(rr[0]), __uint_as_float(rr[1]));
+            nrec = rr[3];
+            p = sl_lane < ck.kc ? rr[kCkptHeader + sl_lane] : kInvalid;
+            valid = sl_lane < nrec && p != kInvalid;
+            rec = rr[2];
+          }
         } else {
+          const uint32_t* rr = ck.pool + (size_t)rec * (kCkptHeader + ck.kc);
+          ri = make_float2(__uint_as_float(rr[0]), __uint_as_float(rr[1]));
+          nrec = rr[3];
           KBuf<1> kb;
           kbuf_init(kb, V.u.t_max);
           traverse8<kCollect>(V.s, F, W, o, d, br, ri.x, V.u.t_max, kb, st, status, lane, (int)k, V.leaf_batch);
-          if (__reduce_or_sync(kFull, status) & (kStatusStackOverflow | kStatusVisitCap | kStatusHitOverflow)) break;
+          if (__reduce_or_sync(kFull, status) & (kStatusStackOverflow | kStatusVisitCap | kStatusHitOverflow)) {
+            rec = kInvalid;
+            break;
+          }
           valid = lane < k && lane < nrec && kb.p[0] != kInvalid;
           p = kb.p[0];
+          rec = rr[2];
         }
-        rec = prev;
-        const uint32_t vmask = __ballot_sync(kFull, valid);
+        const uint32_t vmask = (__ballot_sync(kFull, valid) >> seg_shift) & seg_bits;
         const int n = __popc(vmask);
+        const int nmax = __reduce_max_sync(kFull, (uint32_t)n);
         float alpha = 0.f, resp = 0.f;
         float craw[3] = {0.f, 0.f, 0.f};
         Shade sd;
@@ -299,35 +329,36 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewD
           contrib = V.u.alpha_min < alpha;
           if (contrib) sh_radiance(V.s.sh, p, vnorm(vsub(sd.mu, o)), V.u.deg, craw);
         }
-        const uint32_t cmask = __ballot_sync(kFull, contrib);
+        const uint32_t cballot = __ballot_sync(kFull, contrib);
+        const uint32_t cmask = (cballot >> seg_shift) & seg_bits;
         // transmittance before each entry, in entry order from the round's start
         float T = ri.y, Tme = 0.f;
-        for (int e = 0; e < n; ++e) {
-          if ((int)lane == e) Tme = T;
-          float a = __shfl_sync(kFull, alpha, e);
-          if ((cmask >> e) & 1u) T = T * (1.0f - a);
+        for (int e = 0; e < nmax; ++e) {
+          if ((int)sl_lane == e) Tme = T;
+          const float a = __shfl_sync(kFull, alpha, e, SEG);
+          if (e < n && ((cmask >> e) & 1u)) T = T * (1.0f - a);
         }
         // back to front
         float ga = 0.f;
-        for (int e = n - 1; e >= 0; --e) {
-          float a = __shfl_sync(kFull, alpha, e);
-          float c0 = __shfl_sync(kFull, craw[0], e), c1 = __shfl_sync(kFull, craw[1], e),
-                c2 = __shfl_sync(kFull, craw[2], e);
-          float te = __shfl_sync(kFull, Tme, e);
-          if ((cmask >> e) & 1u) {
+        for (int e = nmax - 1; e >= 0; --e) {
+          const float a = __shfl_sync(kFull, alpha, e, SEG);
+          float c0 = __shfl_sync(kFull, craw[0], e, SEG), c1 = __shfl_sync(kFull, craw[1], e, SEG),
+                c2 = __shfl_sync(kFull, craw[2], e, SEG);
+          const float te = __shfl_sync(kFull, Tme, e, SEG);
+          if (e < n && ((cmask >> e) & 1u)) {
             c0 = c0 > 0.f ? c0 : 0.f;
             c1 = c1 > 0.f ? c1 : 0.f;
             c2 = c2 > 0.f ? c2 : 0.f;
-            float gae = te * ((g[0] * c0 + g[1] * c1 + g[2] * c2) - (g[0] * R0 + g[1] * R1 + g[2] * R2));
-            if ((int)lane == e) ga = gae;
+            const float gae = te * ((g[0] * c0 + g[1] * c1 + g[2] * c2) - (g[0] * R0 + g[1] * R1 + g[2] * R2));
+            if ((int)sl_lane == e) ga = gae;
             R0 = a * c0 + (1.f - a) * R0;
             R1 = a * c1 + (1.f - a) * R1;
             R2 = a * c2 + (1.f - a) * R2;
           }
         }
-        // room for this round's particles in the table
-        const uint32_t nc = (uint32_t)__popc(cmask);
-        if (nfill + nc > (uint32_t)kAggSlots) {
+        // room for this step's particles (all segments) in the table
+        const uint32_t nc_all = (uint32_t)__popc(cballot);
+        if (nfill + nc_all > (uint32_t)kAggSlots) {
           agg_flush(A, V.grad, V.grad_sh, lane);
           nfill = 0;
         }
@@ -338,17 +369,23 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewD
           fresh = agg_add(A, p, v, V.grad, V.grad_sh);
         }
         nfill += (uint32_t)__popc(__ballot_sync(kFull, fresh));
-        if (lane == 0) {
-          ++st.rounds;
-          st.entries += (unsigned)n;
-          st.contributing += nc;
+        {
+          const bool lead = active && sl_lane == 0;
+          const uint32_t r_ = (uint32_t)__popc(__ballot_sync(kFull, lead));
+          const uint32_t e_ = __reduce_add_sync(kFull, lead ? (uint32_t)n : 0u);
+          const uint32_t c_ = __reduce_add_sync(kFull, lead ? (uint32_t)__popc(cmask) : 0u);
+          if (lane == 0) {
+            st.rounds += r_;
+            st.entries += e_;
+            st.contributing += c_;
+          }
         }
       }
     }
     // the next tile may be another view's (other colour sums) or scene's
     agg_flush(A, V.grad, V.grad_sh, lane);
   }
-  flush_stats(ctr, st, rays, status);
+  flush_stats(ctr, st, __reduce_add_sync(kFull, rays), status);
 }
 
 // One view's share of the SH terms of a scene's particles: the camera
@@ -776,10 +813,15 @@ gt_status backward_impl(gt_context* ctx, const BwdView* views, uint32_t count, c
       uint32_t grid = (uint32_t)ctx->num_sms * 4u;  // 4 resident blocks an SM (launch bounds)
       uint64_t max_grid = ((uint64_t)(tile1 - tile0) + kWarpsPerBlock - 1) / kWarpsPerBlock;
       if (grid > max_grid) grid = (uint32_t)std::max<uint64_t>(1, max_grid);
-      if (cs.mode == 1)
-        k_backward<true><<<grid, block, 0, st>>>(ctx->d_views, count, tile0, tile1, ctx->d_ctr, ctx->faces, ck);
+      // lanes per ray: the record's entry slots (the largest k of the views)
+      if (cs.mode == 1 && cs.kc <= 8)
+        k_backward<true, 8><<<grid, block, 0, st>>>(ctx->d_views, count, tile0, tile1, ctx->d_ctr, ctx->faces, ck);
+      else if (cs.mode == 1 && cs.kc <= 16)
+        k_backward<true, 16><<<grid, block, 0, st>>>(ctx->d_views, count, tile0, tile1, ctx->d_ctr, ctx->faces, ck);
+      else if (cs.mode == 1)
+        k_backward<true, 32><<<grid, block, 0, st>>>(ctx->d_views, count, tile0, tile1, ctx->d_ctr, ctx->faces, ck);
       else
-        k_backward<false><<<grid, block, 0, st>>>(ctx->d_views, count, tile0, tile1, ctx->d_ctr, ctx->faces, ck);
+        k_backward<false, 32><<<grid, block, 0, st>>>(ctx->d_views, count, tile0, tile1, ctx->d_ctr, ctx->faces, ck);
       ++ctx->launches;
       BWD_TRY(cudaGetLastError());
     }
