@@ -497,8 +497,12 @@ def main():
                          f"CPU restatement of the reference traversal"}
     extras = None
     if rank == 0 and world == 1 and not args.no_extras and args.workload == "clusters-1m-1080p":
-        extras = {"batched": extra_batched(ctx), "fwd_bwd": extra_fwd_bwd(ctx),
-                  "batched_fwd_bwd": extra_batched_fwd_bwd(ctx, pg, amin)}
+        extras = {}
+        for name, fn in (("fwd_bwd", lambda: extra_fwd_bwd(ctx)), ("batched", lambda: extra_batched(ctx)),
+                         ("batched_fwd_bwd", lambda: extra_batched_fwd_bwd(ctx, pg, amin))):
+            with ClockSampler(local) as eclk:
+                extras[name] = fn()
+            extras[name]["clocks"] = eclk.summary()
     line = {"metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, no dataset)",
