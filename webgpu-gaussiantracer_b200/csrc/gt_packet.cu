@@ -162,6 +162,7 @@ struct PacketBox {
   float ax0, ax1, ay0, ay1, az0, az1;  // smallest, largest inverse direction per axis
   float ppx, ppy, ppz;                 // slab padding per axis
   float tlo;                           // smallest t_curr of the live rays
+  bool straddle;                       // some axis's directions change sign
 };
 
 __device__ __forceinline__ float warp_min_f(float x) { return unord_f(__reduce_min_sync(kFull, ord_f(x))); }
@@ -185,6 +186,7 @@ __device__ __forceinline__ PacketBox make_packet_box(V3 o, const BoxRay& br, boo
   P.ppx = pad * fmaxf(fabsf(P.ax0), fabsf(P.ax1));
   P.ppy = pad * fmaxf(fabsf(P.ay0), fabsf(P.ay1));
   P.ppz = pad * fmaxf(fabsf(P.az0), fabsf(P.az1));
+  P.straddle = (P.ax0 < 0.f && P.ax1 > 0.f) || (P.ay0 < 0.f && P.ay1 > 0.f) || (P.az0 < 0.f && P.az1 > 0.f);
   return P;
 }
 
@@ -273,7 +275,35 @@ __device__ __forceinline__ void packet_traverse(const SceneDev& S, const FaceTab
       bool phit = false, pleaf = false;
       float ptn = CUDART_INF_F;
       uint32_t pref = kInvalid;
-      if (lane < 8) {
+      if (P.straddle) {
+        // a packet whose directions cross an axis plane gets no bound from
+        // that axis (rays nearly parallel to it): every ray tests every
+        // child, and a child's key is the smallest entry distance of the
+        // rays that hit it
+#pragma unroll 1
+        for (int c = 0; c < 8; ++c) {
+          const float4 a = W.nbuf[2 * c], b = W.nbuf[2 * c + 1];
+          const uint32_t ref = __float_as_uint(b.z);
+          float tn;
+          const bool hit = ref != kInvalid && ray_box(a, b, br, tlo, thi, tn);
+          const uint32_t m = __ballot_sync(kFull, hit);
+          if (m == 0) continue;
+          if (ref & kLeafBit) {
+            if (lane == 0) {
+              W.lj[nl] = ref & ~kLeafBit;
+              W.lm[nl] = m;
+            }
+            ++nl;
+          } else {
+            const uint32_t key = __reduce_min_sync(kFull, hit ? ord_f(tn) : 0xFFFFFFFFu);
+            if ((int)lane == c) {
+              phit = true;
+              ptn = unord_f(key);
+              pref = ref;
+            }
+          }
+        }
+      } else if (lane < 8) {
         const float4 a = W.nbuf[2 * lane], b = W.nbuf[2 * lane + 1];
         pref = __float_as_uint(b.z);
         float nx, fx, ny, fy, nz, fz;
@@ -443,7 +473,7 @@ __device__ __forceinline__ bool ray_more(const RayUniforms& u, float T, float t_
 // CKPT: write the round checkpoint the adjoint replays (gt_backward), with
 // the layout and slot numbering of k_trace8's.
 template <int KB, bool CKPT>
-__global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__ views, uint32_t n_views,
+__global__ void __maxnreg__(120) k_trace_packet(const ViewDev* __restrict__ views, uint32_t n_views,
                                                      uint32_t total_tiles, DevCounters* ctr,
                                                      const __grid_constant__ FaceTable F, const Handoff hand,
                                                      uint32_t hand_after, const Ckpt ck) {
