@@ -342,6 +342,7 @@ def extra_batched_fwd_bwd(ctx, pg, amin, reps: int = 1):
             ctx.render_device(s_, u_, w_, h_, p_, asynchronous=True)
     tune = ctx.autotune_batch([(s_, u_, w_, h_) for s_, u_, w_, h_, _ in items])
     step()
+    step()  # the second call sizes the round-record pool from the first one's count
     plain()
     tfb = _time_device(ctx, step, reps)
     tp = _time_device(ctx, plain, reps)

@@ -528,14 +528,17 @@ struct BwdView {
                       std::string(#expr) + ": " + cudaGetErrorString(e_));                               \
   } while (0)
 
-// Grows a context-owned device buffer to at least `bytes`.
+// Grows a context-owned device buffer to at least `bytes`, with a quarter
+// more room so that slowly growing needs (the round records of successive
+// checkpointing forwards) do not free and allocate on every call.
 gt_status grow(gt_context* ctx, void** p, size_t* have, size_t bytes) {
   if (*have >= bytes) return GT_OK;
   cudaFree(*p);
   *p = nullptr;
   *have = 0;
-  CK_TRY(cudaMalloc(p, bytes ? bytes : 16));
-  *have = bytes;
+  const size_t want = bytes + bytes / 4;
+  CK_TRY(cudaMalloc(p, want ? want : 16));
+  *have = want;
   return GT_OK;
 }
 
