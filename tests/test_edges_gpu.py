@@ -237,6 +237,38 @@ def test_rays_nearly_in_a_face_plane(ctx):
     _check_views(ctx, rec, 0.01, views, need_hits=20)
 
 
+def test_rays_through_edges_and_vertices(ctx):
+    """Narrow views (image span 1e-5 of the distance) aimed at points 1e-7 to
+    1e-2 (in units of the face) from an edge or a vertex of a face, seen from
+    random directions: the face test keeps for the exact triangle test only
+    the faces whose plane crossing lies within its rounding reach of the
+    latest one, and near an edge or a vertex two or more faces do."""
+    rng = np.random.default_rng(64)
+    v, faces = _icosahedron()
+    rec = _records([(0.0, 0.0, 0.0), (0.6, 0.2, -0.3), (-0.5, -0.4, 0.2)],
+                   [(0.1, 0.1, 0.1), (0.15, 0.05, 0.02), (0.01, 0.12, 0.06)],
+                   [(1.0, 0.0, 0.0, 0.0)] + list(_unit_quats(rng, 2)), [0.9, 0.6, 0.99], seed=64)
+    osc = oracle.Scene(rec, 0.01, "f64")
+    views = []
+    for j in range(osc.n_kept):
+        _, m = _proxy_map(osc, j)
+        lin = m[:3, :3]
+        for f in rng.choice(20, size=5, replace=False):
+            a, b, c = (lin @ v[list(faces[f])].T).T + m[:3, 3]
+            for off in (1e-7, 1e-5, 1e-3, 1e-2):
+                s_ = off * rng.choice([-1.0, 1.0])
+                edge = a + 0.4 * (b - a) + s_ * (c - a)            # beside edge ab
+                vert = a + off * (b - a) + abs(s_) * (c - a)         # beside vertex a
+                for x in (edge, vert):
+                    d = rng.normal(size=3)
+                    d /= np.linalg.norm(d)
+                    n = np.cross(b - a, c - a)
+                    if np.dot(d, n) * np.dot(n, a - m[:3, 3]) > 0:
+                        d = -d  # towards the face from outside
+                    views.append((_uniforms(x - 2.0 * d, d, (0.0, 1.0, 0.0), 9, 9, 1e-5), 9, 9))
+    _check_views(ctx, rec, 0.01, views, need_hits=50)
+
+
 @pytest.mark.parametrize("ratio", [1e3, 1e4])
 def test_needle_and_disc_proxies(ctx, ratio):
     """Scale ratios of 1e3 and 1e4 (needles and discs), random orientations.
