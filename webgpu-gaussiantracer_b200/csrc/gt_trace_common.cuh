@@ -131,8 +131,23 @@ __device__ __forceinline__ void proxy_test(const FaceTable& F, const float4* w2o
   const float tau = 1e-5f * F.nmax * s;
   const float mbase = 3e-5f * F.nmax * (l1o + 2.0f);
   const float trange = 1e-6f * (fabsf(tlo) + fminf(fabsf(thi), 1e30f));
-  // rolled on purpose: one copy of the triangle test and of the caller's
-  // k-buffer insertion keeps the kernel small enough for the instruction cache
+  // Candidate faces.  For front faces e, f (dn < -tau) with plane crossings
+  // t_e >= t_f, the ray at t_f lies outside plane e by (t_e - t_f)|dn_e|/|n|
+  // while triangle f lies inside it (the proxy is convex), so the crossing
+  // X_f is at least that far from triangle f.  The reference's triangle test
+  // accepts points only within its rounding of the triangle, about
+  // 10 u |od| |p0 - oo| / |dn_f| in barycentric units (u = 2^-24).  Hence a
+  // face can pass only if G = num_e dn_f - num_f dn_e = (t_e - t_f) dn_e dn_f
+  // stays below a few tens of u |od|_1 (|oo|_1 + 2); faces above 128 u times
+  // that are skipped (a CPU check of 4e7 adversarial rays, edges, vertices
+  // and grazing faces, found the first misses below 8).  One pass keeps the
+  // face with the largest crossing so far and every face within the bound of
+  // the face that was largest when it was seen, a superset of the faces the
+  // final largest allows; grazing pairs keep both faces.
+  const float gbound = 7.62939453125e-6f * (fabsf(od.x) + fabsf(od.y) + fabsf(od.z)) * (l1o + 2.0f);
+  uint32_t cand = 0;
+  int best = -1;
+  float bnum = 0.0f, bdn = 0.0f;
 #pragma unroll 1
   for (int pair = 0; pair < 10; ++pair) {
     const int fa = F.pa[pair];
@@ -144,22 +159,48 @@ __device__ __forceinline__ void proxy_test(const FaceTable& F, const float4* w2o
       const float dn = dna < 0.0f ? dna : -dna;
       const float no = __fmaf_rn(na.x, oo.x, __fmaf_rn(na.y, oo.y, na.z * oo.z));
       const float num = F.c[f] - (dna < 0.0f ? no : -no);
-      const float mg = __fmaf_rn(trange, fabsf(dn), mbase);
-      if (num >= __fmaf_rn(tlo, dn, mg) || num <= __fmaf_rn(thi, dn, -mg)) continue;
-      float t;
-      if (tri_test(F, f, oo, tlo, od, thi, dn, t) && front_facing(F, f, load_affine(w2o + 3 * (size_t)j), d))
-        on_hit(t, f);
+      if (best < 0) {
+        best = f;
+        bnum = num;
+        bdn = dn;
+        cand = 1u << f;
+      } else {
+        const float G = bnum * dn - num * bdn;
+        if (G < 0.0f) {  // f crosses its plane later: the new largest
+          if (-G > gbound) cand &= ~(1u << best);
+          best = f;
+          bnum = num;
+          bdn = dn;
+          cand |= 1u << f;
+        } else if (G <= gbound) {
+          cand |= 1u << f;
+        }
+      }
     } else {
       // grazing pair: both faces go to the exact test
-#pragma unroll 1
-      for (int c = 0; c < 2; ++c) {
-        const int f = c ? F.pb[pair] : fa;
-        const float dn = c ? -dna : dna;
-        float t;
-        if (tri_test(F, f, oo, tlo, od, thi, dn, t) && front_facing(F, f, load_affine(w2o + 3 * (size_t)j), d))
-          on_hit(t, f);
-      }
+      cand |= (1u << fa) | (1u << F.pb[pair]);
     }
+  }
+  // the exact tests of the candidates: t-range prefilter (faces whose facing
+  // is certain), then the reference's triangle test and facing rule
+#pragma unroll 1
+  while (cand) {
+    const int f = __ffs(cand) - 1;
+    cand &= cand - 1;
+    const V3 nf = mk(F.n[f][0], F.n[f][1], F.n[f][2]);
+    const float dn = vdot(nf, od);
+    if (fabsf(dn) > tau) {
+      // the t-range test: t times dn lies within E = 10 u nmax (|p0|_1 +
+      // |o|_1) of num = n.p0 - n.o, so a face with num >= tlo*dn + M or
+      // num <= thi*dn - M (dn < 0) has its t outside (tlo, thi)
+      const float no = __fmaf_rn(nf.x, oo.x, __fmaf_rn(nf.y, oo.y, nf.z * oo.z));
+      const float num = F.c[f] - no;
+      const float mg = __fmaf_rn(trange, fabsf(dn), mbase);
+      if (num >= __fmaf_rn(tlo, dn, mg) || num <= __fmaf_rn(thi, dn, -mg)) continue;
+    }
+    float t;
+    if (tri_test(F, f, oo, tlo, od, thi, dn, t) && front_facing(F, f, load_affine(w2o + 3 * (size_t)j), d))
+      on_hit(t, f);
   }
 }
 
