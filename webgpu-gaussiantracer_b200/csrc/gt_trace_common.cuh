@@ -163,7 +163,7 @@ __device__ __forceinline__ void proxy_test(const FaceTable& F, const float4* w2o
         best = f;
         bnum = num;
         bdn = dn;
-        cand = 1u << f;
+        cand |= 1u << f;
       } else {
         const float G = bnum * dn - num * bdn;
         if (G < 0.0f) {  // f crosses its plane later: the new largest
