@@ -86,7 +86,7 @@ __device__ __forceinline__ BoxRay make_boxray(V3 o, V3 d, float scene_mag) {
 //   * candidate faces (CULL): of the front faces, only those whose plane
 //     crossing lies within the triangle test's rounding reach of the latest
 //     crossing can pass it (the proxy is convex; see the bound below), so
-//     the triangle test runs on about 1.2 faces a proxy instead of 6.7.
+//     the triangle test runs on about 1.6 faces a proxy instead of 6.7.
 // The bounding-sphere filter of proxy_test on its own: false only when the
 // ray certainly misses proxy j.
 __device__ __forceinline__ bool proxy_sphere(const FaceTable& F, const float4* w2o, uint32_t j, V3 o, V3 d) {
