@@ -69,8 +69,8 @@ struct PacketScratch {
   float4 nbuf[16];                 // the node being visited
   RayStats stats;
 };
-// 12.7 KB for 32-entry heaps: with the 1 KB the SM reserves per block and
-// 117 registers a thread, 17 one-warp blocks fit an SM
+// 12.7 KB for 32-entry heaps (16 one-warp blocks an SM: each of the SM's four
+// schedulers holds 16K registers, four warps of up to 128 registers a thread)
 
 // float -> uint map that preserves order (for warp min/max reductions)
 __device__ __forceinline__ uint32_t ord_f(float x) {
@@ -473,7 +473,7 @@ __device__ __forceinline__ bool ray_more(const RayUniforms& u, float T, float t_
 // CKPT: write the round checkpoint the adjoint replays (gt_backward), with
 // the layout and slot numbering of k_trace8's.
 template <int KB, bool CKPT>
-__global__ void __maxnreg__(120) k_trace_packet(const ViewDev* __restrict__ views, uint32_t n_views,
+__global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__ views, uint32_t n_views,
                                                      uint32_t total_tiles, DevCounters* ctr,
                                                      const __grid_constant__ FaceTable F, const Handoff hand,
                                                      uint32_t hand_after, const Ckpt ck) {
