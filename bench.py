@@ -278,24 +278,18 @@ def extra_fwd_bwd(ctx, reps: int = 3):
             "checkpoint_fwd_ms": tck, "mode": "checkpoint" if info.get("used_mode") == 1 else "replay"}
 
 
-def extra_batched_fwd_bwd(ctx, pg, amin, reps: int = 1):
+def extra_batched_fwd_bwd(ctx, pg, amin, reps: int = 1, n_views: int = 32):
     """32 views (640x480 - 1920x1080) of the 1M scene: batched forward with
     checkpoint + per-view L2 loss + one batched adjoint accumulating all views,
-    against 32 plain forwards one by one."""
+    against 32 plain forwards one by one (n_views: the first n of the 32)."""
     import ctypes as C
     from gtrace import _lib as L
     from gtrace import synth
     from gtrace.tracer import Scene, _uniforms
-    rng = np.random.Generator(np.random.PCG64(synth.SEED_BASE + 4))
     scene = Scene(ctx, pg.gaussiansBuffer, amin)
     target_raw = synth.perturb(synth.raw_clusters(1_000_000, synth.SEED_BASE + 1), synth.SEED_BASE + 44)
     target = Scene(ctx, synth.pack(target_raw).gaussiansBuffer, amin)
-    views = []
-    for i in range(32):
-        w = int(rng.integers(640, 1921))
-        h = int(rng.integers(480, 1081))
-        pos = synth.random_sphere_camera(rng, 10.0, 14.0)
-        views.append(synth.view(w, h, pos, k=16))
+    views = synth.batched_fwd_bwd_views(n_views)
     imgs = [ctx.device_alloc(v.width * v.height * 16) for v in views]
     tgts = [ctx.device_alloc(v.width * v.height * 16) for v in views]
     dls = [ctx.device_alloc(v.width * v.height * 16) for v in views]
@@ -342,7 +336,7 @@ def extra_batched_fwd_bwd(ctx, pg, amin, reps: int = 1):
             ctx.render_device(s_, u_, w_, h_, p_, asynchronous=True)
     tune = ctx.autotune_batch([(s_, u_, w_, h_) for s_, u_, w_, h_, _ in items])
     step()
-    step()  # the second call sizes the round-record pool from the first one's count
+    step()  # the second call sizes the checkpoint pool from the first one's count
     plain()
     tfb = _time_device(ctx, step, reps)
     tp = _time_device(ctx, plain, reps)
@@ -351,7 +345,8 @@ def extra_batched_fwd_bwd(ctx, pg, amin, reps: int = 1):
         ctx.device_free(p)
     scene.close()
     target.close()
-    return {"workload": "1M Gaussians (64 clusters), 32 views 640x480-1920x1080, k=16, L2 loss vs perturbed scene",
+    return {"workload": f"1M Gaussians (64 clusters), {len(views)} views 640x480-1920x1080, k=16, "
+                        "L2 loss vs perturbed scene",
             "rays": rays, "batched_fwd_bwd_ms": tfb, "plain_fwd_ms": tp, "ratio": tfb / tp,
             "checkpoint_fwd_ms": tfc, "adjoint_ms": info.get("bwd_ms"),
             "shape": {"kernel": "tile packets" if tune["block_threads"] == 32 else "warp per ray",
@@ -372,6 +367,9 @@ def main():
                     help="--impl reference: seconds of CPU work per step (0: 60 s spread over the steps)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched and forward+backward measurements")
+    ap.add_argument("--extra", choices=["fwd_bwd", "batched", "batched_fwd_bwd"], default=None,
+                    help="run only this extra measurement (one GPU) and print its result as the line")
+    ap.add_argument("--views", type=int, default=32, help="--extra batched_fwd_bwd: views of the batch")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -381,6 +379,21 @@ def main():
     w, h = v.width, v.height
     rays = w * h
     threads = os.cpu_count() or 1
+
+    if args.extra:
+        # one extra measurement on its own (the profiling runs); rank 0 only
+        if rank == 0:
+            from gtrace.tracer import Context
+            ctx = Context(local)
+            fn = {"fwd_bwd": lambda: extra_fwd_bwd(ctx), "batched": lambda: extra_batched(ctx),
+                  "batched_fwd_bwd": lambda: extra_batched_fwd_bwd(ctx, pg, amin, n_views=args.views)}[args.extra]
+            with ClockSampler(local) as eclk:
+                res = fn()
+            res["clocks"] = eclk.summary()
+            print(json.dumps({"extra": args.extra, **res}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
 
     if args.impl == "reference":
         if rank != 0:

@@ -291,9 +291,11 @@ gt_status gt_tonemap(gt_context* ctx, const float* rgba, uint64_t n_pixels, uint
  * No counterpart in the reference (it has no training path, README.md:69). */
 typedef struct gt_bwd_opts {
   uint32_t mode;          /* 0 = auto (checkpoint if it fits), 1 = checkpoint, 2 = replay */
-  uint32_t max_rounds;    /* in: expected rounds per ray, sizes the first checkpoint pool
+  uint32_t max_rounds;    /* in: expected records per ray, sizes the first checkpoint pool
                              (0 = the previous call's count, else 4); the pool grows to
-                             the rounds actually traced.  out: round records used     */
+                             the records actually written.  A record holds up to 16
+                             contributing entries of a ray (checkpoint mode) or one
+                             round (replay mode).  out: records used                  */
   uint64_t mem_budget;    /* bytes the checkpoint may use (0 = 1/2 of free device memory),
                              and the adjoint's per-view colour sums (16 bytes a particle
                              a view; 0 = 1/4 of free memory): views whose sums do not fit
@@ -346,7 +348,7 @@ gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items, uint32_t 
  *   - outputs must be device buffers: GT_FLAG_OUTPUT_DEVICE is required
  *     (host outputs would need a staging allocation); GT_FLAG_ANTIALIAS
  *     blends into them as in gt_render_batch; GT_FLAG_CHECKPOINT is
- *     rejected (the round records would need an allocation);
+ *     rejected (the checkpoint records would need an allocation);
  *   - stats (optional) carries the counters and the kernel and call times;
  *   - at most 256 views per call; larger counts are rejected with
  *     GT_ERR_INVALID_ARG;

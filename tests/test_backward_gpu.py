@@ -58,13 +58,46 @@ def test_checkpoint_and_replay_agree_and_grow(ctx):
     pg = small_scene(n=2000, seed=42)
     s = Scene(ctx, pg.gaussiansBuffer, 0.01)
     w, h = 40, 30
-    v = view(w, h, k=2)  # many rounds per ray: the pool outgrows a 1-round-per-ray guess
+    v = view(w, h, k=2)  # many rounds per ray
     g = np.random.default_rng(3).normal(size=(h, w, 4)).astype(np.float32)
     a, ia = ctx.backward(s, v.uniforms, w, h, g, mode=1, max_rounds=1)
     b, ib = ctx.backward(s, v.uniforms, w, h, g, mode=2, max_rounds=1)
     assert ia["used_mode"] == 1 and ib["used_mode"] == 2
-    assert ia["max_rounds"] > w * h and ia["max_rounds"] == ib["max_rounds"]  # records: > 1 round per ray
+    # replay records one per round (> 1 a ray); checkpoint records hold up to
+    # 16 contributing entries each, across rounds, so there are fewer
+    assert ib["max_rounds"] > w * h and 0 < ia["max_rounds"] < ib["max_rounds"]
     np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-6 * np.abs(a).max())
+
+
+def test_checkpoint_records_across_handoff_and_pool_growth(ctx):
+    """Checkpoint records take a ray's contributing entries across round
+    boundaries, and a ray's open record passes from its tile packet to the
+    warp-per-ray kernel at the handoff: forced tile packets with 8-entry
+    buffers and k = 2 hand rays over after three traversals.  A fresh context
+    sizes its first pool from the call before (one pixel), so the forward
+    overflows it, counts the records it needed and runs again.  The gradient
+    equals the warp-per-ray path's and the FP64 oracle's."""
+    from gtrace.tracer import Context
+    pg = small_scene(n=2000, seed=42)
+    rec = pg.gaussiansBuffer
+    w, h = 64, 48
+    v = view(w, h, k=2)
+    g = np.random.default_rng(5).normal(size=(h, w, 4)).astype(np.float32)
+    ref_cuda, _ = ctx.backward(Scene(ctx, rec, 0.01), v.uniforms, w, h, g, mode=1)
+    c2 = Context(0)
+    try:
+        s2 = Scene(c2, rec, 0.01)
+        one = view(1, 1, k=2)
+        c2.backward(s2, one.uniforms, 1, 1, np.zeros((1, 1, 4), np.float32), mode=1)
+        c2.set_tune(s2, v.uniforms, w, h, kbuf=8, block_threads=32)
+        got, info = c2.backward(s2, v.uniforms, w, h, g, mode=1)
+        assert info["used_mode"] == 1
+        assert info["max_rounds"] > 1025  # more records than the first pool held
+        got = got.copy()
+    finally:
+        c2.close()
+    np.testing.assert_allclose(got, ref_cuda, rtol=1e-5, atol=1e-6 * np.abs(ref_cuda).max())
+    _check(got, _ref_grad(rec, 0.01, v.uniforms, w, h, g))
 
 
 def test_l2_loss_against_perturbed_target(ctx):

@@ -168,15 +168,17 @@ __device__ __forceinline__ void entry_terms(const SceneDev& S, uint32_t p, const
 // per entry.
 constexpr int kAggSlots = 64;
 struct AggTable {
-  uint32_t key[kAggSlots];   // particle index, kInvalid when empty
-  float4 val[kAggSlots][5];  // the 16 response sums, then the 3 colour sums and 0
+  uint32_t key[kAggSlots];     // particle index, kInvalid when empty
+  float val[20][kAggSlots];    // sum i of slot h at val[i][h]: the 16 response sums, the 3 colour sums, 0
 };
+// (component-major: lanes adding to different slots meet in one bank only
+// when their slots are 32 apart)
 
 __device__ __forceinline__ void agg_clear(AggTable& A, uint32_t lane) {
   for (uint32_t i = lane; i < (uint32_t)kAggSlots; i += 32) {
     A.key[i] = kInvalid;
 #pragma unroll
-    for (int c = 0; c < 5; ++c) A.val[i][c] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int c = 0; c < 20; ++c) A.val[c][i] = 0.f;
   }
   __syncwarp();
 }
@@ -190,10 +192,9 @@ __device__ __forceinline__ bool agg_add(AggTable& A, uint32_t p, const float v[2
   for (int step = 0; step < kAggSlots; ++step) {
     const uint32_t prev = atomicCAS(&A.key[h], kInvalid, p);
     if (prev == kInvalid || prev == p) {
-      float* d = reinterpret_cast<float*>(&A.val[h][0]);
 #pragma unroll
       for (int i = 0; i < 19; ++i)
-        if (v[i] != 0.f) atomicAdd(d + i, v[i]);
+        if (v[i] != 0.f) atomicAdd(&A.val[i][h], v[i]);
       return prev == kInvalid;
     }
     h = (h + 1) & (kAggSlots - 1);
@@ -214,9 +215,12 @@ __device__ __forceinline__ void agg_flush(AggTable& A, float4* G, float4* GS, ui
     if (p == kInvalid) continue;
 #pragma unroll
     for (int c = 0; c < 5; ++c) {
-      const float4 x = A.val[i][c];
+      const float4 x = make_float4(A.val[4 * c][i], A.val[4 * c + 1][i], A.val[4 * c + 2][i], A.val[4 * c + 3][i]);
       if (x.x != 0.f || x.y != 0.f || x.z != 0.f || x.w != 0.f) atomicAdd(c < 4 ? G + 4 * (size_t)p + c : GS + p, x);
-      A.val[i][c] = make_float4(0.f, 0.f, 0.f, 0.f);
+      A.val[4 * c][i] = 0.f;
+      A.val[4 * c + 1][i] = 0.f;
+      A.val[4 * c + 2][i] = 0.f;
+      A.val[4 * c + 3][i] = 0.f;
     }
     A.key[i] = kInvalid;
   }
@@ -226,10 +230,9 @@ __device__ __forceinline__ void agg_flush(AggTable& A, float4* G, float4* GS, ui
 // The adjoint, one warp per 8x4 tile of ray slots (the forward's slot
 // numbering): the tiles [tile_begin, tile_end) of the launch's views.  The
 // warp splits into 32 / SEG segments of SEG lanes, each walking one of the
-// tile's rays (a round's k <= SEG entries across its lanes), so that small k
-// keeps the lanes busy (k = 8: four rays at a time); the tile's per-particle
-// sums gather in the warp's table.  Replay mode (the entries found again by
-// a warp-wide traversal) runs with SEG = 32.
+// tile's rays (a record's up to SEG contributing entries across its lanes);
+// the tile's per-particle sums gather in the warp's table.  Replay mode (a
+// round's entries found again by a warp-wide traversal) runs with SEG = 32.
 template <bool CKPT_PIDX, int SEG>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewDev* __restrict__ views,
                                                                     uint32_t n_views, uint32_t tile_begin,
@@ -250,7 +253,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewD
   RayStats& st = W.stats;
   if (lane == 0) st = RayStats{0, 0, 0, 0, 0, 0};
   agg_clear(A, lane);
-  uint32_t status = 0, rays = 0;
+  uint32_t status = 0, rays = 0, n_rounds = 0, n_entries = 0, n_contrib = 0;
   while (true) {
     uint32_t tile = 0;
     if (lane == 0) tile = atomicAdd(&ctr->work, 1u);
@@ -282,9 +285,9 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewD
       if (rec != kInvalid) ray_gen(V.u, V.w, V.h, px, py, o, d);
       const BoxRay br = make_boxray(o, d, V.s.scene_mag);
       if (rec != kInvalid && sl_lane == 0) ++rays;
-      float R0 = 0.f, R1 = 0.f, R2 = 0.f;
-      // rounds from the last to the first along the record links, all
-      // segments in step (a segment whose ray is done idles)
+      float S = 0.f;  // g.R: the colour composited behind the current round, dotted with g
+      // records from the last to the first along their links, all segments
+      // in step (a segment whose ray is done idles)
       for (uint32_t guard = 0; guard < ck.pool_cap; ++guard) {
         const bool active = rec != kInvalid;
         if (!__any_sync(kFull, active)) break;
@@ -317,7 +320,6 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewD
         }
         const uint32_t vmask = (__ballot_sync(kFull, valid) >> seg_shift) & seg_bits;
         const int n = __popc(vmask);
-        const int nmax = __reduce_max_sync(kFull, (uint32_t)n);
         float alpha = 0.f, resp = 0.f;
         float craw[3] = {0.f, 0.f, 0.f};
         Shade sd;
@@ -331,31 +333,47 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewD
         }
         const uint32_t cballot = __ballot_sync(kFull, contrib);
         const uint32_t cmask = (cballot >> seg_shift) & seg_bits;
-        // transmittance before each entry, in entry order from the round's start
-        float T = ri.y, Tme = 0.f;
-        for (int e = 0; e < nmax; ++e) {
-          if ((int)sl_lane == e) Tme = T;
-          const float a = __shfl_sync(kFull, alpha, e, SEG);
-          if (e < n && ((cmask >> e) & 1u)) T = T * (1.0f - a);
+        // transmittance before each entry: the round's starting T times the
+        // product of (1 - alpha) over the contributing entries ahead of it
+        // (an exclusive product scan across the segment's lanes)
+        const float keep = contrib ? 1.0f - alpha : 1.0f;
+        float pre = keep;
+#pragma unroll
+        for (int off = 1; off < SEG; off <<= 1) {
+          const float x = __shfl_up_sync(kFull, pre, off, SEG);
+          if ((int)sl_lane >= off) pre *= x;
         }
-        // back to front
-        float ga = 0.f;
-        for (int e = nmax - 1; e >= 0; --e) {
-          const float a = __shfl_sync(kFull, alpha, e, SEG);
-          float c0 = __shfl_sync(kFull, craw[0], e, SEG), c1 = __shfl_sync(kFull, craw[1], e, SEG),
-                c2 = __shfl_sync(kFull, craw[2], e, SEG);
-          const float te = __shfl_sync(kFull, Tme, e, SEG);
-          if (e < n && ((cmask >> e) & 1u)) {
-            c0 = c0 > 0.f ? c0 : 0.f;
-            c1 = c1 > 0.f ? c1 : 0.f;
-            c2 = c2 > 0.f ? c2 : 0.f;
-            const float gae = te * ((g[0] * c0 + g[1] * c1 + g[2] * c2) - (g[0] * R0 + g[1] * R1 + g[2] * R2));
-            if ((int)sl_lane == e) ga = gae;
-            R0 = a * c0 + (1.f - a) * R0;
-            R1 = a * c1 + (1.f - a) * R1;
-            R2 = a * c2 + (1.f - a) * R2;
+        float ahead = __shfl_up_sync(kFull, pre, 1, SEG);
+        if (sl_lane == 0) ahead = 1.0f;
+        const float Tme = ri.y * ahead;
+        // dL/dalpha of entry e: T_e (g.c_e - g.R_e), R_e the colour composited
+        // behind e (normalised by T_e (1 - a_e)), i.e. the entries after e in
+        // this round and the later rounds' S.  Behind-colours follow
+        // x -> a_e s_e + (1 - a_e) x from the back, so they are an inclusive
+        // suffix scan of these affine maps (composed through shuffles).
+        float sv = 0.f;
+        if (contrib) {
+          const float c0 = craw[0] > 0.f ? craw[0] : 0.f, c1 = craw[1] > 0.f ? craw[1] : 0.f,
+                      c2 = craw[2] > 0.f ? craw[2] : 0.f;
+          sv = g[0] * c0 + g[1] * c1 + g[2] * c2;
+        }
+        float fm = keep, fb = contrib ? alpha * sv : 0.f;  // map of entries e.. (from e to the round's end)
+#pragma unroll
+        for (int off = 1; off < SEG; off <<= 1) {
+          const float xm = __shfl_down_sync(kFull, fm, off, SEG);
+          const float xb = __shfl_down_sync(kFull, fb, off, SEG);
+          if ((int)sl_lane + off < SEG) {
+            fb = __fmaf_rn(fm, xb, fb);
+            fm = fm * xm;
           }
         }
+        float nm = __shfl_down_sync(kFull, fm, 1, SEG), nb = __shfl_down_sync(kFull, fb, 1, SEG);
+        if ((int)sl_lane + 1 >= SEG) {
+          nm = 1.0f;
+          nb = 0.0f;
+        }
+        const float ga = contrib ? Tme * (sv - __fmaf_rn(nm, S, nb)) : 0.f;
+        S = __fmaf_rn(__shfl_sync(kFull, fm, 0, SEG), S, __shfl_sync(kFull, fb, 0, SEG));
         // room for this step's particles (all segments) in the table
         const uint32_t nc_all = (uint32_t)__popc(cballot);
         if (nfill + nc_all > (uint32_t)kAggSlots) {
@@ -369,21 +387,25 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewD
           fresh = agg_add(A, p, v, V.grad, V.grad_sh);
         }
         nfill += (uint32_t)__popc(__ballot_sync(kFull, fresh));
-        {
-          const bool lead = active && sl_lane == 0;
-          const uint32_t r_ = (uint32_t)__popc(__ballot_sync(kFull, lead));
-          const uint32_t e_ = __reduce_add_sync(kFull, lead ? (uint32_t)n : 0u);
-          const uint32_t c_ = __reduce_add_sync(kFull, lead ? (uint32_t)__popc(cmask) : 0u);
-          if (lane == 0) {
-            st.rounds += r_;
-            st.entries += e_;
-            st.contributing += c_;
-          }
+        if (active && sl_lane == 0) {
+          ++n_rounds;
+          n_entries += (uint32_t)n;
+          n_contrib += (uint32_t)__popc(cmask);
         }
       }
     }
     // the next tile may be another view's (other colour sums) or scene's
     agg_flush(A, V.grad, V.grad_sh, lane);
+  }
+  {
+    const uint32_t r_ = __reduce_add_sync(kFull, n_rounds), e_ = __reduce_add_sync(kFull, n_entries),
+                   c_ = __reduce_add_sync(kFull, n_contrib);
+    if (lane == 0) {
+      st.rounds += r_;
+      st.entries += e_;
+      st.contributing += c_;
+    }
+    __syncwarp();
   }
   flush_stats(ctr, st, __reduce_add_sync(kFull, rays), status);
 }
@@ -529,7 +551,7 @@ struct BwdView {
   } while (0)
 
 // Grows a context-owned device buffer to at least `bytes`, with a quarter
-// more room so that slowly growing needs (the round records of successive
+// more room so that slowly growing needs (the records of successive
 // checkpointing forwards) do not free and allocate on every call.
 gt_status grow(gt_context* ctx, void** p, size_t* have, size_t bytes) {
   if (*have >= bytes) return GT_OK;
@@ -579,12 +601,11 @@ gt_status api_forward_ckpt(gt_context* ctx, const gt_scene* const* scenes, const
   gt_status sst = api_ensure_views(ctx, count);
   if (sst != GT_OK) return sst;
   std::vector<ViewDev> vd(count);
-  uint32_t total_tiles = 0, kmax = 1;
+  uint32_t total_tiles = 0;
   uint64_t rays = 0;
   for (uint32_t i = 0; i < count; ++i) {
     vd[i] = api_make_view(scenes[i], us[i], ws[i], hs[i], outs[i], total_tiles);
     total_tiles += vd[i].n_tiles;
-    kmax = std::max(kmax, us[i].k);
     rays += (uint64_t)ws[i] * hs[i];
   }
   const uint64_t slots = (uint64_t)total_tiles * 32u;
@@ -593,7 +614,7 @@ gt_status api_forward_ckpt(gt_context* ctx, const gt_scene* const* scenes, const
     cudaMemGetInfo(&free_b, &total_b);
     budget = free_b / 2 + ck.pool_bytes;  // the pool we hold counts as available
   }
-  // first guess of the records: the last call's count, else 4 rounds a ray
+  // first guess of the records: the last call's count, else 4 a ray
   uint64_t want = ck.last_records ? ck.last_records + ck.last_records / 8 + 1024 : rays * 4 + 1024;
   if (cap) want = std::max<uint64_t>(want, rays * (uint64_t)cap);
   if (!ck.pool_next) CK_TRY(cudaMalloc(&ck.pool_next, 4));
@@ -604,9 +625,9 @@ gt_status api_forward_ckpt(gt_context* ctx, const gt_scene* const* scenes, const
   sst = api_ensure_handoff(ctx, rays, &hand);
   if (sst != GT_OK) return sst;
   for (int attempt = 0; attempt < 3; ++attempt) {
-    if (want > 0xFFFFFFF0ull) return api_fail(ctx, GT_ERR_OOM, "checkpoint needs more than 2^32 round records");
-    uint32_t m = mode == 1 ? 1u : (mode == 2 ? 2u : (want * (kCkptHeader + kmax) * 4 <= budget ? 1u : 2u));
-    const uint32_t kc = m == 1 ? kmax : 0u;
+    if (want > 0xFFFFFFF0ull) return api_fail(ctx, GT_ERR_OOM, "checkpoint needs more than 2^32 records");
+    uint32_t m = mode == 1 ? 1u : (mode == 2 ? 2u : (want * (kCkptHeader + kCkptChunk) * 4 <= budget ? 1u : 2u));
+    const uint32_t kc = m == 1 ? kCkptChunk : 0u;
     sst = grow(ctx, (void**)&ck.pool, &ck.pool_bytes, want * (kCkptHeader + kc) * 4);
     if (sst != GT_OK) return sst;
     Ckpt c;
@@ -816,7 +837,7 @@ gt_status backward_impl(gt_context* ctx, const BwdView* views, uint32_t count, c
       uint32_t grid = (uint32_t)ctx->num_sms * 4u;  // 4 resident blocks an SM (launch bounds)
       uint64_t max_grid = ((uint64_t)(tile1 - tile0) + kWarpsPerBlock - 1) / kWarpsPerBlock;
       if (grid > max_grid) grid = (uint32_t)std::max<uint64_t>(1, max_grid);
-      // lanes per ray: the record's entry slots (the largest k of the views)
+      // lanes per ray: the record's entry slots
       if (cs.mode == 1 && cs.kc <= 8)
         k_backward<true, 8><<<grid, block, 0, st>>>(ctx->d_views, count, tile0, tile1, ctx->d_ctr, ctx->faces, ck);
       else if (cs.mode == 1 && cs.kc <= 16)

@@ -29,7 +29,7 @@ struct CkptKey {
 };
 struct CkptStore {
   uint32_t* head = nullptr;       // [slots]
-  uint32_t* pool = nullptr;       // round records
+  uint32_t* pool = nullptr;       // checkpoint records
   uint32_t* pool_next = nullptr;  // device allocation counter
   size_t head_bytes = 0, pool_bytes = 0;
   uint64_t slots = 0;

@@ -217,14 +217,21 @@ Err build_ploc(const float* leaf_box, uint32_t m, cudaStream_t st, float4* nodes
 Err scan_exclusive(const uint32_t* in, uint32_t* out, uint64_t n, cudaStream_t st, uint64_t* launches);
 void free_scene(SceneBuffers* b);
 
-// Round checkpoint written by the forward pass of gt_backward.  Each traced
-// round gets one record from a shared pool (one atomic per round); records of
-// a ray are linked from its last round to its first, the order the adjoint
-// walks them, so memory follows the rounds actually traced.
-// Record layout (uint32 words): [0] t_curr at the round start (float bits),
-// [1] T at the round start (float bits), [2] previous record of the ray
+// Checkpoint written by the forward pass of gt_backward, in records from a
+// shared pool; the records of a ray are linked from its last to its first,
+// the order the adjoint walks them, so memory follows the work actually done.
+// Record layout (uint32 words): [0] t_curr when the record opened (float
+// bits), [1] T at that point (float bits), [2] previous record of the ray
 // (kInvalid for the first), [3] number of entries, [4, 4 + kc) particle
-// indices of the entries (checkpoint mode only; kc == 0 in replay mode).
+// indices.
+//   * checkpoint mode (kc > 0): a record holds the next kc contributing
+//     entries of the ray in compositing order (alpha above alpha_min; the
+//     others change neither T nor the colour), across round boundaries, and
+//     [1] is the transmittance before its first entry.  The forward opens a
+//     record when an entry contributes and the ray has none open or a full
+//     one (warp-aggregated allocation);
+//   * replay mode (kc == 0): one record per round ([0], [1] at the round's
+//     start), the adjoint traces the round's entries again.
 struct Ckpt {
   uint32_t* head = nullptr;       // [slots] last record of the ray, kInvalid if none
   uint32_t* pool = nullptr;       // [pool_cap][4 + kc]
@@ -232,6 +239,8 @@ struct Ckpt {
   uint32_t pool_cap = 0;          // records
   uint32_t kc = 0;                // particle indices stored per record (0: replay mode)
 };
+// contributing entries a checkpoint record holds (the adjoint's segment width)
+constexpr uint32_t kCkptChunk = 16;
 constexpr uint32_t kCkptHeader = 4;
 
 // A ray that a tile packet hands over part way: its work slot (32 * tile +
@@ -239,7 +248,8 @@ constexpr uint32_t kCkptHeader = 4;
 struct HandoffRay {
   uint32_t item, step;
   float t_curr, T, L0, L1, L2;
-  uint32_t ck_head;  // checkpointing launches: the ray's last round record
+  uint32_t ck_head;  // checkpointing launches: the ray's last record
+  uint32_t ck_fill;  // entries in that record (checkpoint mode; kc when none is open)
 };
 // The handoff buffer of a launch (rays == nullptr: no handoff).
 struct Handoff {

@@ -510,6 +510,7 @@ __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__
     bool handed = false;
     uint32_t n_trav = 0;
     uint32_t ck_head = kInvalid;
+    uint32_t ck_fill = ck.kc;  // entries in the open record (checkpoint mode; kc: none open)
     while (__any_sync(kFull, live)) {
       if (hand.rays && n_trav == hand_after) {
         // hand the rays that still need hits to the warp-per-ray kernel
@@ -519,7 +520,7 @@ __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__
         base = __shfl_sync(kFull, base, 0);
         const uint32_t idx = base + (uint32_t)__popc(hm & ((1u << lane) - 1u));
         if (live && idx < hand.cap) {
-          hand.rays[idx] = HandoffRay{32u * tile + lane, step, t_curr, T, L0, L1, L2, ck_head};
+          hand.rays[idx] = HandoffRay{32u * tile + lane, step, t_curr, T, L0, L1, L2, ck_head, ck_fill};
           live = false;
           handed = true;
         }
@@ -559,7 +560,8 @@ __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__
         }
         const uint32_t am = __ballot_sync(kFull, act);
         if (am == 0) break;
-        if (CKPT) {
+        if (CKPT && ck.kc == 0) {
+          // replay mode: one record a round
           uint32_t base = 0;
           if (lane == 0) base = atomicAdd(ck.pool_next, (uint32_t)__popc(am));
           base = __shfl_sync(kFull, base, 0);
@@ -570,11 +572,71 @@ __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__
             r[1] = __float_as_uint(T);
             r[2] = ck_head;
             r[3] = n;
-            for (uint32_t e = 0; e < ck.kc; ++e) r[kCkptHeader + e] = e < n ? key_p(W.hk[head + e][lane]) : kInvalid;
             ck_head = rec;
           }
         }
-        if (act) {
+        if (CKPT && ck.kc) {
+          // checkpoint mode: the same accumulation with the rays' entries in
+          // step, so that records open with one allocation for the warp
+          const uint32_t nmax = __reduce_max_sync(kFull, act ? n : 0u);
+          if (act) {
+            ++step;
+            ++n_rounds;
+            n_entries += n;
+          }
+          for (uint32_t e = 0; e < nmax; ++e) {
+            bool contrib = false;
+            uint32_t ep = 0;
+            float alpha = 0.f, x0 = 0.f, x1 = 0.f, x2 = 0.f;
+            if (act && e < n) {
+              ep = key_p(W.hk[head + e][lane]);
+              const Shade sd = load_shade(V.s.shade, ep);
+              alpha = response(sd, o, d) * sd.opacity;
+              if (V.u.alpha_min < alpha) {
+                contrib = true;
+                const V3 dir = vnorm(vsub(sd.mu, o));
+                float c[3];
+                sh_radiance(V.s.sh, ep, dir, V.u.deg, c);
+                x0 = c[0] > 0.f ? c[0] : 0.f;
+                x1 = c[1] > 0.f ? c[1] : 0.f;
+                x2 = c[2] > 0.f ? c[2] : 0.f;
+              }
+            }
+            const bool open = contrib && ck_fill >= ck.kc;
+            const uint32_t om = __ballot_sync(kFull, open);
+            if (om) {
+              const int leader = __ffs(om) - 1;
+              uint32_t base = 0;
+              if ((int)lane == leader) base = atomicAdd(ck.pool_next, (uint32_t)__popc(om));
+              base = __shfl_sync(kFull, base, leader);
+              if (open) {
+                const uint32_t rec = base + (uint32_t)__popc(om & ((1u << lane) - 1u));
+                if (rec < ck.pool_cap) {  // past the pool the host sizes it up and runs again
+                  uint32_t* r = ck.pool + (size_t)rec * (kCkptHeader + ck.kc);
+                  r[0] = __float_as_uint(t_curr);
+                  r[1] = __float_as_uint(T);
+                  r[2] = ck_head;
+                }
+                ck_head = rec;
+                ck_fill = 0;
+              }
+            }
+            if (contrib) {
+              if (ck_head < ck.pool_cap) {
+                uint32_t* r = ck.pool + (size_t)ck_head * (kCkptHeader + ck.kc);
+                r[kCkptHeader + ck_fill] = ep;
+                r[3] = ck_fill + 1;
+              }
+              ++ck_fill;
+              const float ta = T * alpha;
+              L0 = L0 + ta * x0;
+              L1 = L1 + ta * x1;
+              L2 = L2 + ta * x2;
+              T = T * (1.0f - alpha);
+              ++n_contrib;
+            }
+          }
+        } else if (act) {
           ++step;
           ++n_rounds;
           n_entries += n;
@@ -598,6 +660,8 @@ __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__
               ++n_contrib;
             }
           }
+        }
+        if (act) {
           head += n;
           t_curr = new_t;
           if (step >= F.lim_rounds && ray_more(V.u, T, t_curr, step)) {
@@ -611,7 +675,7 @@ __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__
       }
       __syncwarp();
     }
-    if (CKPT && valid && !handed) ck.head[32u * tile + lane] = ck_head;
+    if (CKPT && valid && !handed) ck.head[32u * tile + lane] = ck_head < ck.pool_cap ? ck_head : kInvalid;
     if (valid && !handed) {
       const float4 r = make_float4(L0, L1, L2, 1.0f);
       float4* dst = V.out + (size_t)py * V.w + px;

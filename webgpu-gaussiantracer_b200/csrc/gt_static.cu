@@ -70,7 +70,7 @@ extern "C" gt_status gt_render_batch_noalloc(gt_context* ctx, const gt_batch_ite
                     "would need a staging allocation");
   if (flags & GT_FLAG_CHECKPOINT)
     return api_fail(ctx, GT_ERR_INVALID_ARG,
-                    "gt_render_batch_noalloc does not checkpoint: the round records need an allocation");
+                    "gt_render_batch_noalloc does not checkpoint: the checkpoint records need an allocation");
   const bool aa = (flags & GT_FLAG_ANTIALIAS) != 0;
   uint32_t total_tiles = 0;
   uint64_t slots_all = 0;

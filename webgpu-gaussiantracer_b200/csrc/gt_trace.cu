@@ -109,6 +109,7 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
   R.step = 0;
   R.n_entries = 0;
   uint32_t ck_head = kInvalid;
+  uint32_t ck_fill = ck.kc;  // entries in the open record (checkpoint mode; kc: none open)
   if (!RECORD && init) {
     R.L0 = init->L0;
     R.L1 = init->L1;
@@ -117,6 +118,7 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
     R.t_curr = init->t_curr;
     R.step = init->step;
     ck_head = init->ck_head;
+    ck_fill = init->ck_fill;
   }
   const uint32_t k = V.u.k;
   while (wray_more(V, R)) {
@@ -138,6 +140,7 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
       vu[0] = R.step;
       vu[1] = R.n_entries;
       vu[2] = ck_head;
+      if (CKPT) vu[3] = ck_fill;
     }
     traverse8<kCollect>(V.s, F, W, R.o, R.d, R.br, R.t_curr, t_max, kb, st, status, lane, kbuf, V.leaf_batch);
     {
@@ -151,6 +154,7 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
       R.step = vu[0];
       R.n_entries = vu[1];
       ck_head = vu[2];
+      if (CKPT) ck_fill = vu[3];
     }
     // status bits may be set in single lanes: reduce before branching on them
     if (__reduce_or_sync(kFull, status) & (kStatusStackOverflow | kStatusVisitCap | kStatusHitOverflow)) break;
@@ -185,7 +189,8 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
           ep = xp;
         }
       }
-      if (CKPT) {
+      if (CKPT && ck.kc == 0) {
+        // replay mode: one record a round
         uint32_t rec = 0;
         if (lane == 0) rec = atomicAdd(ck.pool_next, 1u);
         rec = __shfl_sync(kFull, rec, 0);
@@ -197,7 +202,6 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
             r[2] = ck_head;
             r[3] = n;
           }
-          if (lane < ck.kc) r[kCkptHeader + lane] = lane < n ? ep : kInvalid;
           ck_head = rec;
         }
       }
@@ -241,6 +245,29 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
         float x1 = __shfl_sync(kFull, c1, (int)e);
         float x2 = __shfl_sync(kFull, c2, (int)e);
         if ((cmask >> e) & 1u) {
+          if (CKPT && ck.kc) {
+            // checkpoint mode: the entry goes to the ray's open record
+            const uint32_t pe = __shfl_sync(kFull, ep, (int)e);
+            if (ck_fill >= ck.kc) {
+              uint32_t rec = 0;
+              if (lane == 0) rec = atomicAdd(ck.pool_next, 1u);
+              rec = __shfl_sync(kFull, rec, 0);
+              if (lane == 0 && rec < ck.pool_cap) {  // past the pool the host sizes it up and runs again
+                uint32_t* r = ck.pool + (size_t)rec * (kCkptHeader + ck.kc);
+                r[0] = __float_as_uint(R.t_curr);
+                r[1] = __float_as_uint(R.T);
+                r[2] = ck_head;
+              }
+              ck_head = rec;
+              ck_fill = 0;
+            }
+            if (lane == 0 && ck_head < ck.pool_cap) {
+              uint32_t* r = ck.pool + (size_t)ck_head * (kCkptHeader + ck.kc);
+              r[kCkptHeader + ck_fill] = pe;
+              r[3] = ck_fill + 1;
+            }
+            ++ck_fill;
+          }
           float ta = R.T * a;
           R.L0 = R.L0 + ta * x0;
           R.L1 = R.L1 + ta * x1;
@@ -260,7 +287,7 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
     ho.count[slot] = R.n_entries;
     ho.rounds[slot] = R.step;
   }
-  if (CKPT && lane == 0) ck.head[slot] = ck_head;
+  if (CKPT && lane == 0) ck.head[slot] = ck_head < ck.pool_cap ? ck_head : kInvalid;
   return make_float4(R.L0, R.L1, R.L2, 1.0f);
 }
 
