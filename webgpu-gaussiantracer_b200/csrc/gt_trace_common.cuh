@@ -159,10 +159,14 @@ __device__ __forceinline__ void proxy_test(const FaceTable& F, const float4* w2o
     const float dna = vdot(na, od);
     if (fabsf(dna) > tau) {
       // exactly one face of the pair can face the ray
-      const int f = dna < 0.0f ? fa : F.pb[pair];
+      // both plane offsets by the pair's (warp-uniform) index: a load indexed
+      // by the lane's face would be served once per distinct face
+      const int fb = F.pb[pair];
+      const float ca = F.c[fa], cb = F.c[fb];
+      const int f = dna < 0.0f ? fa : fb;
       const float dn = dna < 0.0f ? dna : -dna;
       const float no = __fmaf_rn(na.x, oo.x, __fmaf_rn(na.y, oo.y, na.z * oo.z));
-      const float num = F.c[f] - (dna < 0.0f ? no : -no);
+      const float num = (dna < 0.0f ? ca : cb) - (dna < 0.0f ? no : -no);
       if (best < 0) {
         best = f;
         bnum = num;
