@@ -112,7 +112,10 @@ typedef struct gt_render_stats {
   uint64_t node_visits;   /* BVH nodes popped                                     */
   uint64_t anyhits;       /* front-face proxy hits offered to the k-buffer         */
   uint32_t status_flags;  /* device status word (0 = clean)                       */
-  uint32_t _pad;
+  uint32_t handed;        /* rays that reached the tile packets' traversal limit: the
+                             warp-per-ray kernel finishes those that fit the handoff
+                             buffer (a quarter of the launch's rays), the packets the
+                             rest (0 when the warp-per-ray kernel traced the views)   */
 } gt_render_stats;
 
 typedef struct gt_scene_info {

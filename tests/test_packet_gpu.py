@@ -114,6 +114,32 @@ def test_batch_of_views_and_scenes(ctx):
     assert st["rays"] == 37 * 21 + 24 * 40 + 16 * 16
 
 
+def test_handoff_across_views(ctx):
+    """Rays that reach the packets' traversal limit go to the warp-per-ray
+    kernel with their compositing state, in a batch of views of two scenes.
+    Dense scenes, k = 2 and 8-entry buffers make most rays reach it; every
+    view must equal the oracle bit for bit."""
+    pa = small_scene(n=12000, seed=57)
+    pb = small_scene(n=9000, seed=58)
+    ga, gb = Scene(ctx, pa.gaussiansBuffer, 0.01), Scene(ctx, pb.gaussiansBuffer, 0.01)
+    oa, ob = oracle.Scene(pa.gaussiansBuffer, 0.01, "f32"), oracle.Scene(pb.gaussiansBuffer, 0.01, "f32")
+    views = [(ga, view(40, 24, k=2, T_min=0.0001).uniforms, 40, 24),
+             (gb, view(24, 40, k=2, T_min=0.0001).uniforms, 24, 40),
+             (ga, view(33, 17, pos=(1.0, 2.0, 3.5), k=2, T_min=0.0001).uniforms, 33, 17),
+             (gb, view(16, 24, pos=(-2.0, 0.5, 3.0), k=2, T_min=0.0001).uniforms, 16, 24)]
+    ctx.set_tune(views[0][0], views[0][1], 40, 24, kbuf=8, block_threads=32)
+    try:
+        outs, st = ctx.render_batch(views)
+    finally:
+        ctx._lib.gt_autotune_reset(ctx._h)
+    for (sc, u, w, h), out in zip(views, outs):
+        ref, _ = (oa if sc is ga else ob).render(u, w, h)
+        assert np.array_equal(_bits(out), ref.view(np.uint32))
+    rays = sum(w * h for _, _, w, h in views)
+    assert st["rays"] == rays
+    assert st["handed"] > rays // 4, st["handed"]
+
+
 @pytest.mark.parametrize("mode", [1, 2])
 def test_checkpointing_forward_and_gradients(ctx, mode):
     """gt_backward's checkpointing forward as tile packets (with rays handed

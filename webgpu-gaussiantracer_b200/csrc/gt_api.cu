@@ -183,6 +183,7 @@ static void fill_stats(const DevCounters& c, gt_render_stats* st) {
   st->node_visits = c.node_visits;
   st->anyhits = c.anyhits;
   st->status_flags = c.status;
+  st->handed = c.handoff;
 }
 
 static std::tuple<uint64_t, uint32_t, uint32_t, uint32_t> tune_key(const gt_scene* s, uint32_t w, uint32_t h,

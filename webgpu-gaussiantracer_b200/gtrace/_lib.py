@@ -50,7 +50,7 @@ class RenderStats(C.Structure):
     _fields_ = [("kernel_ms", C.c_float), ("total_ms", C.c_float), ("rays", C.c_uint64), ("rounds", C.c_uint64),
                 ("entries", C.c_uint64), ("contributing", C.c_uint64), ("proxy_tests", C.c_uint64),
                 ("node_visits", C.c_uint64), ("anyhits", C.c_uint64), ("status_flags", C.c_uint32),
-                ("_pad", C.c_uint32)]
+                ("handed", C.c_uint32)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_ if not name.startswith("_")}
