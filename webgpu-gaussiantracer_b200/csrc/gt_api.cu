@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
 #include <map>
 #include <mutex>
 #include <set>
@@ -16,6 +17,72 @@
 
 #include "gt_handles.h"
 #include "gt_internal.cuh"
+
+// Host threads that copy a pageable buffer into a pinned chunk together,
+// kept for the context's life: starting threads for every chunk cost about as
+// much as a chunk's copy.  The calling thread takes a share as well.
+struct CopyPool {
+  explicit CopyPool(unsigned workers) {
+    for (unsigned t = 0; t < workers; ++t) th_.emplace_back([this, t] { run(t); });
+  }
+  ~CopyPool() {
+    {
+      std::lock_guard<std::mutex> l(m_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& x : th_) x.join();
+  }
+  void copy(unsigned char* dst, const unsigned char* src, size_t bytes) {
+    if (th_.empty() || bytes < (4u << 20)) {
+      memcpy(dst, src, bytes);
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> l(m_);
+      dst_ = dst;
+      src_ = src;
+      bytes_ = bytes;
+      left_ = (unsigned)th_.size();
+      ++gen_;
+    }
+    cv_.notify_all();
+    slice((unsigned)th_.size());
+    std::unique_lock<std::mutex> l(m_);
+    done_.wait(l, [&] { return left_ == 0; });
+  }
+
+ private:
+  void slice(unsigned t) {
+    const size_t parts = th_.size() + 1, per = (bytes_ + parts - 1) / parts;
+    const size_t b = t * per, e = std::min(bytes_, b + per);
+    if (b < e) memcpy(dst_ + b, src_ + b, e - b);
+  }
+  void run(unsigned t) {
+    uint64_t seen = 0;
+    while (true) {
+      {
+        std::unique_lock<std::mutex> l(m_);
+        cv_.wait(l, [&] { return stop_ || gen_ != seen; });
+        if (stop_) return;
+        seen = gen_;
+      }
+      slice(t);
+      std::lock_guard<std::mutex> l(m_);
+      if (--left_ == 0) done_.notify_one();
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex m_;
+  std::condition_variable cv_, done_;
+  unsigned char* dst_ = nullptr;
+  const unsigned char* src_ = nullptr;
+  size_t bytes_ = 0;
+  unsigned left_ = 0;
+  uint64_t gen_ = 0;
+  bool stop_ = false;
+};
+
 
 using namespace gt;
 
@@ -288,16 +355,18 @@ extern "C" gt_status gt_context_destroy(gt_context* ctx) {
   drop_graphs(ctx);
   api_free_ckpt(ctx);
   for (gt_scene* s : ctx->scenes) {
-    free_scene(&s->b);
+    free_scene(&s->b, ctx->stream);
     delete s;
   }
   ctx->scenes.clear();
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);  // the frees are stream-ordered
   cudaFree(ctx->d_ctr);
   cudaFreeHost(ctx->h_ctr);
   cudaFree(ctx->d_views);
   cudaFree(ctx->d_handoff);
   cudaFreeHost(ctx->h_views);
   cudaFree(ctx->staging);
+  delete ctx->copy_pool;
   for (int b = 0; b < 2; ++b) {
     if (ctx->up_pinned[b]) cudaFreeHost(ctx->up_pinned[b]);
     if (ctx->up_done[b]) cudaEventDestroy(ctx->up_done[b]);
@@ -329,24 +398,12 @@ extern "C" gt_status gt_last_error(const gt_context* ctx, char* buf, size_t len)
 // stream.
 constexpr size_t kUploadChunk = 16u << 20;
 
-static void host_copy_parallel(unsigned char* dst, const unsigned char* src, size_t bytes) {
-  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-  const size_t nt = std::min<size_t>(std::min<unsigned>(hw, 8u), std::max<size_t>(1, bytes >> 21));
-  if (nt <= 1) {
-    memcpy(dst, src, bytes);
-    return;
-  }
-  std::vector<std::thread> th;
-  const size_t per = (bytes + nt - 1) / nt;
-  for (size_t t = 0; t < nt; ++t) {
-    const size_t b = t * per, e = std::min(bytes, b + per);
-    if (b < e) th.emplace_back([=]() { memcpy(dst + b, src + b, e - b); });
-  }
-  for (auto& x : th) x.join();
-}
-
 static gt_status upload_host(gt_context* ctx, void* dst_dev, const void* src_host, size_t bytes) {
   if (bytes == 0) return GT_OK;
+  if (!ctx->copy_pool) {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    ctx->copy_pool = new CopyPool(std::min(hw, 8u) - 1);
+  }
   for (int b = 0; b < 2; ++b) {
     if (!ctx->up_pinned[b])
       API_CUDA(ctx, cudaHostAlloc((void**)&ctx->up_pinned[b], kUploadChunk, cudaHostAllocDefault));
@@ -358,7 +415,7 @@ static gt_status upload_host(gt_context* ctx, void* dst_dev, const void* src_hos
     const int b = (int)(i & 1);
     const size_t len = std::min(kUploadChunk, bytes - off);
     API_CUDA(ctx, cudaEventSynchronize(ctx->up_done[b]));  // the chunk's previous copy has left
-    host_copy_parallel(ctx->up_pinned[b], src + off, len);
+    ctx->copy_pool->copy(ctx->up_pinned[b], src + off, len);
     API_CUDA(ctx, cudaMemcpyAsync(dst + off, ctx->up_pinned[b], len, cudaMemcpyHostToDevice, ctx->stream));
     API_CUDA(ctx, cudaEventRecord(ctx->up_done[b], ctx->stream));
   }
@@ -430,7 +487,7 @@ extern "C" gt_status gt_scene_create_ex(gt_context* ctx, const void* packed, uin
   cudaEventRecord(ctx->call1, ctx->stream);
   drop_tmps();
   if (e.code != GT_OK) {
-    free_scene(&s->b);
+    free_scene(&s->b, ctx->stream);
     delete s;
     return fail(ctx, e);
   }
@@ -448,7 +505,7 @@ extern "C" gt_status gt_scene_destroy(gt_scene* s) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   ctx->scenes.erase(s);
-  free_scene(&s->b);
+  free_scene(&s->b, ctx->stream);
   delete s;
   return GT_OK;
 }

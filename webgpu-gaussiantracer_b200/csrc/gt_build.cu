@@ -758,7 +758,7 @@ static Err collapse_bvh8(const float4* bn, const float* leaf_box, uint32_t m, cu
       std::swap(fn, nn);
     }
   }
-  GT_CUDA_TRY(cudaMalloc(out8, (size_t)total * 16 * sizeof(float4)));
+  GT_CUDA_TRY(cudaMallocAsync(out8, (size_t)total * 16 * sizeof(float4), st));
   GT_CUDA_TRY(cudaMemcpyAsync(*out8, tmp, (size_t)total * 16 * sizeof(float4), cudaMemcpyDeviceToDevice, st));
   cudaFreeAsync(tmp, st);
   cudaFreeAsync(fb, st);
@@ -771,14 +771,13 @@ static Err collapse_bvh8(const float4* bn, const float* leaf_box, uint32_t m, cu
 }
 
 // -------------------------------------------------------------- driver
-void free_scene(SceneBuffers* b) {
-  cudaFree(b->nodes);
-  cudaFree(b->nodes8);
-  cudaFree(b->w2o);
-  cudaFree(b->leaf_pidx);
-  cudaFree(b->shade);
-  cudaFree(b->sh);
-  cudaFree(b->params);
+// The scene's buffers come from the device's stream-ordered pool (which the
+// context keeps from releasing), so a scene built after another was freed
+// reuses its memory instead of mapping new pages.
+void free_scene(SceneBuffers* b, cudaStream_t st) {
+  for (void* p : {(void*)b->nodes, (void*)b->nodes8, (void*)b->w2o, (void*)b->leaf_pidx, (void*)b->shade,
+                  (void*)b->sh, (void*)b->params})
+    if (p) cudaFreeAsync(p, st);
   *b = SceneBuffers{};
 }
 
@@ -795,9 +794,9 @@ Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride, double alph
   }
   if (n >= (1ull << 31)) return Err{GT_ERR_INVALID_ARG, "scene larger than 2^31 particles"};
   // shading records (every particle slot; only kept ones are written/read)
-  GT_CUDA_TRY(cudaMalloc(&b.shade, n * 3 * sizeof(float4)));
-  GT_CUDA_TRY(cudaMalloc(&b.sh, n * 12 * sizeof(float4)));
-  GT_CUDA_TRY(cudaMalloc(&b.params, n * 2 * sizeof(float4)));
+  GT_CUDA_TRY(cudaMallocAsync(&b.shade, n * 3 * sizeof(float4), st));
+  GT_CUDA_TRY(cudaMallocAsync(&b.sh, n * 12 * sizeof(float4), st));
+  GT_CUDA_TRY(cudaMallocAsync(&b.params, n * 2 * sizeof(float4), st));
   b.bytes += n * 17 * sizeof(float4);
   uint32_t *flags = nullptr, *slots = nullptr, *bounds = nullptr;
   GT_CUDA_TRY(cudaMallocAsync(&flags, n * 4, st));
@@ -847,9 +846,9 @@ Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride, double alph
   if (e.code != GT_OK) return e;
   // scene records
   uint32_t n_int = m > 1 ? m - 1 : 0;
-  GT_CUDA_TRY(cudaMalloc(&b.w2o, (size_t)m * 3 * sizeof(float4)));
-  GT_CUDA_TRY(cudaMalloc(&b.leaf_pidx, (size_t)m * 4));
-  GT_CUDA_TRY(cudaMalloc(&b.nodes, (size_t)std::max<uint32_t>(n_int, 1) * 4 * sizeof(float4)));
+  GT_CUDA_TRY(cudaMallocAsync(&b.w2o, (size_t)m * 3 * sizeof(float4), st));
+  GT_CUDA_TRY(cudaMallocAsync(&b.leaf_pidx, (size_t)m * 4, st));
+  GT_CUDA_TRY(cudaMallocAsync(&b.nodes, (size_t)std::max<uint32_t>(n_int, 1) * 4 * sizeof(float4), st));
   b.bytes += (uint64_t)m * (3 * sizeof(float4) + 4) + (uint64_t)std::max<uint32_t>(n_int, 1) * 4 * sizeof(float4);
   float *leaf_box = nullptr, *ibox = nullptr;
   uint32_t *parent_int = nullptr, *parent_leaf = nullptr, *arrive = nullptr, *depth = nullptr;
@@ -894,8 +893,7 @@ Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride, double alph
     if (ce.code != GT_OK) return ce;
     b.bytes += (uint64_t)b.n_nodes8 * 16 * sizeof(float4);
     // traversal reads only the 8-wide nodes: the binary hierarchy goes
-    GT_CUDA_TRY(cudaStreamSynchronize(st));
-    cudaFree(b.nodes);
+    cudaFreeAsync(b.nodes, st);
     b.nodes = nullptr;
     b.bytes -= (uint64_t)std::max<uint32_t>(n_int, 1) * 4 * sizeof(float4);
   }
@@ -924,11 +922,11 @@ Err build_scene(const void* packed_dev, uint64_t n, uint32_t stride, double alph
   cudaFreeAsync(depth, st);
   GT_CUDA_TRY(cudaStreamSynchronize(st));
   if (bo[7] != 0) {
-    free_scene(&b);
+    free_scene(&b, st);
     return Err{GT_ERR_CUDA, "internal error: the built hierarchy is not a tree"};
   }
   if (b.depth > kMaxDepth) {
-    free_scene(&b);
+    free_scene(&b, st);
     return Err{GT_ERR_UNSUPPORTED, "BVH deeper than the traversal stack allows"};
   }
   *out = b;

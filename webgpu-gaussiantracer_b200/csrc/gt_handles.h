@@ -59,6 +59,7 @@ struct gt_context {
   float4* staging = nullptr;
   size_t staging_bytes = 0;
   // pinned chunks through which host records are uploaded (double-buffered)
+  struct CopyPool* copy_pool = nullptr;  // host threads of the pinned uploads (gt_api.cu)
   unsigned char* up_pinned[2] = {nullptr, nullptr};
   cudaEvent_t up_done[2] = {nullptr, nullptr};
   gt::HandoffRay* d_handoff = nullptr;  // rays tile packets hand to the warp-per-ray kernel

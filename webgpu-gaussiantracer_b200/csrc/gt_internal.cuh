@@ -215,7 +215,7 @@ Err build_ploc(const float* leaf_box, uint32_t m, cudaStream_t st, float4* nodes
                uint32_t* parent_leaf, uint64_t* launches);
 // Exclusive prefix sum of n words (gt_build.cu).
 Err scan_exclusive(const uint32_t* in, uint32_t* out, uint64_t n, cudaStream_t st, uint64_t* launches);
-void free_scene(SceneBuffers* b);
+void free_scene(SceneBuffers* b, cudaStream_t st);
 
 // Checkpoint written by the forward pass of gt_backward, in records from a
 // shared pool; the records of a ray are linked from its last to its first,
