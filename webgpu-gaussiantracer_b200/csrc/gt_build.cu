@@ -109,6 +109,11 @@ void make_face_table(FaceTable* F) {
     }
   }
   F->npairs = q;
+  for (int r = 0; r < q; ++r) {
+    for (int a = 0; a < 3; ++a) F->pn[r][a] = F->n[F->pa[r]][a];
+    F->pca[r] = F->c[F->pa[r]];
+    F->pcb[r] = F->c[F->pb[r]];
+  }
   F->lim_steps = 0xFFFFFFFFu;
   F->lim_stack = kWarpStack;
   F->lim_rounds = kMaxRounds;

@@ -45,6 +45,8 @@ struct FaceTable {
   float emax;      // max L1 norm of the edge vectors e0, e1
   float c[20];     // plane offsets n . p0 (pre-check only)
   int pa[10], pb[10];  // antipodal face pairs: n[pb[q]] == -n[pa[q]] bit for bit
+  float pn[10][3];     // n[pa[q]], pair-major: the unrolled candidate pass reads them
+  float pca[10], pcb[10];  // c[pa[q]], c[pb[q]]   at fixed parameter offsets
   int npairs;          // 10 (checked when the context is created)
   // Device loop limits of the trace kernels (this table is a kernel
   // parameter, so they cost no registers).  gt_set_limits lowers them to

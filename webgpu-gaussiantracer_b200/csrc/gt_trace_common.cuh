@@ -152,17 +152,18 @@ __device__ __forceinline__ void proxy_test(const FaceTable& F, const float4* w2o
   uint32_t cand = 0;
   int best = -1;
   float bnum = 0.0f, bdn = 0.0f;
-#pragma unroll 1
+#pragma unroll
   for (int pair = 0; pair < 10; ++pair) {
     const int fa = F.pa[pair];
-    const V3 na = mk(F.n[fa][0], F.n[fa][1], F.n[fa][2]);
+    const V3 na = mk(F.pn[pair][0], F.pn[pair][1], F.pn[pair][2]);
     const float dna = vdot(na, od);
     if (fabsf(dna) > tau) {
       // exactly one face of the pair can face the ray
-      // both plane offsets by the pair's (warp-uniform) index: a load indexed
-      // by the lane's face would be served once per distinct face
+      // the pair's values sit at fixed offsets of the table (the loop is
+      // unrolled): no indexed loads, and the pairs' independent products
+      // can overlap
       const int fb = F.pb[pair];
-      const float ca = F.c[fa], cb = F.c[fb];
+      const float ca = F.pca[pair], cb = F.pcb[pair];
       const int f = dna < 0.0f ? fa : fb;
       const float dn = dna < 0.0f ? dna : -dna;
       const float no = __fmaf_rn(na.x, oo.x, __fmaf_rn(na.y, oo.y, na.z * oo.z));
