@@ -197,6 +197,20 @@ def _time_device(ctx, fn, reps: int):
     return ctx.timer_stop() / reps
 
 
+def _time_device_median(ctx, fn, reps: int):
+    """Median over reps calls of fn of each call's device time (CUDA events on
+    the library stream around the call): a step of host-synchronous calls
+    (forward, loss, adjoint) is timed one at a time, so that one slow host
+    turn-around does not stand for the rest."""
+    ts = []
+    for _ in range(reps):
+        ctx.synchronize()
+        ctx.timer_start()
+        fn()
+        ts.append(ctx.timer_stop())
+    return statistics.median(ts)
+
+
 def extra_batched(ctx, reps: int = 2):
     """8 scenes (100k-1M Gaussians, log-uniform), 64 views of uneven size: one
     batched launch against the 64 views rendered one by one."""
@@ -247,7 +261,7 @@ def _train_step_single(ctx, scene, v, img, tgt, dl, gout):
     return ctx.backward_device(scene, v.uniforms, v.width, v.height, dl, gout, reuse_checkpoint=True)
 
 
-def extra_fwd_bwd(ctx, reps: int = 3):
+def extra_fwd_bwd(ctx, reps: int = 9):
     """200k Gaussians, 800x800, k=8, L2 loss against a render of the perturbed
     scene: plain forward vs forward + loss + backward."""
     from gtrace import synth
@@ -266,9 +280,9 @@ def extra_fwd_bwd(ctx, reps: int = 3):
     ckpt = lambda: ctx.render_device(scene, v.uniforms, v.width, v.height, img, checkpoint=True)  # noqa: E731
     fwd()
     step()
-    tf = _time_device(ctx, fwd, reps)
-    tfb = _time_device(ctx, step, reps)
-    tck = _time_device(ctx, ckpt, reps)
+    tf = _time_device_median(ctx, fwd, reps)
+    tfb = _time_device_median(ctx, step, reps)
+    tck = _time_device_median(ctx, ckpt, reps)
     for p in (img, tgt, dl, gout):
         ctx.device_free(p)
     scene.close()
@@ -444,13 +458,14 @@ def main():
     scene = Scene(ctx, pg.gaussiansBuffer, amin)
     scene_wall_ms = (time.perf_counter() - t_sc) * 1e3
     info = scene.info()
-    # the same scene created again: the steady cost of a scene once the context
-    # holds its kernels, memory pool and pinned upload chunks
+    # the scene built again in its place (as a training loop rebuilds it): the
+    # steady cost once the context holds its kernels, memory pool and pinned
+    # upload chunks; this copy is the one rendered
+    scene.close()
     t_sc = time.perf_counter()
-    again = Scene(ctx, pg.gaussiansBuffer, amin)
+    scene = Scene(ctx, pg.gaussiansBuffer, amin)
     warm_wall_ms = (time.perf_counter() - t_sc) * 1e3
-    warm_info = again.info()
-    again.close()
+    warm_info = scene.info()
     out_dev = ctx.device_alloc(rays * 16)
     # one synchronous render: counters for the algorithmic byte count
     st0 = ctx.render_device(scene, v.uniforms, w, h, out_dev)

@@ -155,9 +155,10 @@ constexpr uint32_t kMaxPacketKbuf = 64;
 // A tile packet is a coarse work item: a few tiles whose rays have many
 // hits take several times the mean, so with few tiles per resident warp (16
 // warps an SM) their tail outweighs the packets' gain even with the handoff
-// (1M-Gaussian view, ms as packets / a ray per warp: 480x270, 1.7 tiles a
-// warp, 8.3 / 5.0; 960x540, 6.8 tiles a warp, 17.2 / 18.6).
-constexpr uint32_t kPacketTilesPerSm = 80;
+// (1M-Gaussian view, ms as packets / a ray per warp, with the early handoff
+// once every tile is taken: 480x270 (35 tiles an SM) 14.9 / 5.2; 640x360
+// (52) 7.6 / 8.8; 800x450 (97) 9.7 / 13.7; 960x540 (109) 12.5 / 19.3).
+constexpr uint32_t kPacketTilesPerSm = 48;
 
 // ----------------------------------------------------------- host helpers
 // Work slots of a w x h view: 32 per 8 x 4 tile of its tile grid, padded to
