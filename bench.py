@@ -467,6 +467,15 @@ def main():
     warm_wall_ms = (time.perf_counter() - t_sc) * 1e3
     warm_info = scene.info()
     out_dev = ctx.device_alloc(rays * 16)
+    # the launch shape for this view from the library's tuner (gt_autotune:
+    # k-buffer size and hand-off point of the tile packets, blocks, k-buffer
+    # and leaf batch of the warp-per-ray kernel), cached by the context and
+    # used by every render below
+    tune = ctx.autotune(scene, v.uniforms, w, h)
+    shape = {"kernel": "tile packets" if tune["block_threads"] == 32 else "warp per ray", "kbuf": tune["kbuf"],
+             "handoff_after": tune["handoff_after"] if tune["block_threads"] == 32 else None,
+             "blocks_per_sm": tune["blocks_per_sm"] if tune["block_threads"] == 128 else None,
+             "tuned_ms": tune["best_ms"], "default_shape_ms": tune["default_ms"]}
     # one synchronous render: counters for the algorithmic byte count
     st0 = ctx.render_device(scene, v.uniforms, w, h, out_dev)
     alg_bytes = 16 * st0["rays"] + 44 * st0["entries"] + 192 * st0["contributing"]
@@ -551,7 +560,7 @@ def main():
                        "scene_create_wall_ms": warm_wall_ms,
                        "scene_first_create": {"build_ms": info["build_ms"], "upload_ms": info["upload_ms"],
                                               "create_wall_ms": scene_wall_ms},
-                       "bvh_depth": info["bvh_depth"],
+                       "bvh_depth": info["bvh_depth"], "shape": shape,
                        "l2": "inputs larger than L2 (scene %.0f MB > 126 MB), no flush" % (info["device_bytes"] / 1e6),
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

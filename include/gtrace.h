@@ -387,17 +387,19 @@ gt_status gt_l2_loss(gt_context* ctx, const float* rgba, const float* target, ui
  * bucket, k).  gt_render and gt_render_batch use the cached choice.
  * Two kernels render the plain image (debugMode 0), with identical results:
  *   block_threads 32:  a warp traces the 32 rays of an 8x4 tile together;
- *                      kbuf = k-buffer entries per ray (k..64, default 32);
- *                      blocks_per_sm and leaf_batch are not used (the grid
- *                      fills the SMs);
+ *                      kbuf = k-buffer entries per ray (k..64, default 32),
+ *                      handoff_after as below (the tuner times 2 to 8
+ *                      and 64 for the fastest kbuf); blocks_per_sm and leaf_batch are
+ *                      not used (the grid fills the SMs);
  *   block_threads 128: a warp traces one ray; kbuf = k-buffer entries of a
  *                      traversal (k..128, default 64), blocks_per_sm and
  *                      leaf_batch as below.
  * Without a cached shape a launch takes the first kernel when it has at
- * least 80 8x4 tiles per SM (about 0.38 Mpixels on a 148-SM B200) and the
+ * least 48 8x4 tiles per SM (about 0.23 Mpixels on a 148-SM B200) and the
  * second otherwise: tiles are coarse work items, and with few of them per
  * warp the slowest ones decide the time.  With the first kernel, the rays
- * of a tile that still need hits after three traversals are finished by
+ * of a tile that still need hits after three traversals (or after the
+ * current one, once every tile of the launch is taken) are finished by
  * the second one (a second launch).  The same choice holds for the
  * checkpointing forward of gt_backward; debug modes and hit recording
  * always use the second kernel. */

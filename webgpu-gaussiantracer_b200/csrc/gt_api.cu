@@ -898,7 +898,8 @@ extern "C" gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const g
   float best = 1e30f, def = 0.0f;
   st = time_shape(LaunchShape(), 3, &def);
   if (st != GT_OK) return st;
-  // 1. tile packets: k-buffer entries per ray
+  // 1. tile packets: k-buffer entries per ray, then the hand-off point of
+  // the fastest
   const uint32_t pkbufs[] = {k, 24u, 32u, 48u, 64u};
   for (int i = 0; i < 5; ++i) {
     const uint32_t kb = pkbufs[i];
@@ -912,6 +913,21 @@ extern "C" gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const g
     if (ms < best) {
       best = ms;
       best_sh = sh;
+    }
+  }
+  if (best_sh.packet == 1) {
+    const LaunchShape kb_sh = best_sh;
+    // (64: only once every tile of the launch is taken)
+    for (uint32_t ha : {2u, 4u, 6u, 8u, 64u}) {
+      LaunchShape sh = kb_sh;
+      sh.handoff_after = ha;
+      float ms = 0.0f;
+      st = time_shape(sh, 3, &ms);
+      if (st != GT_OK) return st;
+      if (ms < best) {
+        best = ms;
+        best_sh = sh;
+      }
     }
   }
   // 2. a warp per ray: resident blocks per SM, then k-buffer size and leaf batch

@@ -24,9 +24,9 @@
 //     bounded by shared memory, and more of them hide more latency;
 //   * k-buffer: each ray keeps the kbuf smallest (t, particle) hits in a
 //     max-heap of its own (a column of a shared-memory array of 64-bit keys
-//     that order like (t, particle)); its root is the ray's far bound.  Hits
-//     of one face-test batch are inserted by one lane per target ray at a
-//     time (__match_any_sync groups the lanes);
+//     that order like (t, particle)); its root is the ray's far bound.  The
+//     hits of one face-test batch are inserted by one lane per target ray
+//     (__match_any_sync groups the lanes whose pairs test that ray);
 //   * rounds and compositing: after the traversal each lane sorts its heap
 //     (heapsort) and runs the rounds of its own ray serially, in entry
 //     order.  Rays whose buffer ran out traverse again (with the packet's
@@ -55,8 +55,7 @@ constexpr int kSurvCap = 64;  // pairs that passed the sphere filter (< kSurvivo
 template <int KB>
 struct PacketScratch {
   unsigned long long hk[KB][32];  // heap of ray r in column r: hit keys, max at row 0
-  uint32_t snode[kWarpStack];
-  float skey[kWarpStack];
+  uint2 stk[kWarpStack];  // node stack: (node, bits of its entry distance)
   uint32_t lj[8];  // leaf children of the visited node that some ray hit,
   uint32_t lm[8];  // with the mask of those rays
   uint32_t pj[kPairCap];
@@ -64,6 +63,8 @@ struct PacketScratch {
   uint32_t svj[kSurvCap];
   uint8_t svr[kSurvCap];
   float hq[kMaxHitsPerProxy][32];  // hits of each lane's pair, column per lane
+  uint32_t hp[32];                 // the particle of each lane's pair
+  uint8_t hc[32];                  // and its hit count
   float dx[32], dy[32], dz[32];    // ray directions
   float tlo[32], thi[32];          // ray intervals; thi = far bound
   uint8_t hn[32];                  // heap sizes
@@ -239,8 +240,7 @@ __device__ __forceinline__ void packet_traverse(const SceneDev& S, const FaceTab
   RayStats& st = W.stats;
   int sp = 1, nq = 0, ns = 0;
   if (lane == 0) {
-    W.snode[0] = 0;
-    W.skey[0] = -CUDART_INF_F;
+    W.stk[0] = make_uint2(0u, __float_as_uint(-CUDART_INF_F));
   }
   __syncwarp();
   uint32_t iters = 0;
@@ -259,9 +259,9 @@ __device__ __forceinline__ void packet_traverse(const SceneDev& S, const FaceTab
     uint32_t node = kInvalid;
     while (sp > 0) {
       --sp;
-      const uint32_t n = W.snode[sp];
-      if (W.skey[sp] <= thi_max) {
-        node = n;
+      const uint2 e = W.stk[sp];
+      if (__uint_as_float(e.y) <= thi_max) {
+        node = e.x;
         break;
       }
     }
@@ -336,42 +336,41 @@ __device__ __forceinline__ void packet_traverse(const SceneDev& S, const FaceTab
       // inner children the packet may hit, keyed by the packet's entry distance
       const uint32_t imask = __ballot_sync(kFull, phit && !pleaf);
       const int ni = __popc(imask);
-      float mykey = CUDART_INF_F;
-      uint32_t myref = 0;
+      uint32_t top = 0;  // the child that goes on top of the stack (nearest)
       if (ni > 0) {
         if (sp + ni > (int)F.lim_stack) {
           status |= kStatusStackOverflow;
           return;
         }
-        // gathered into lanes 0..ni-1 through the free stack slots above sp
-        if ((imask >> lane) & 1u) {
-          const int q = sp + __popc(imask & lt_mask);
-          W.skey[q] = ptn;
-          W.snode[q] = pref;
-        }
-        __syncwarp();
-        if ((int)lane < ni) {
-          mykey = W.skey[sp + (int)lane];
-          myref = W.snode[sp + (int)lane];
-        }
-        __syncwarp();
-      }
-      if (lane == 0) st.node_visits += 1;
-      if (ni > 0) {
-        if (sp + ni > (int)F.lim_stack) {
-          status |= kStatusStackOverflow;
-          return;
-        }
-        if (ni > 1) warp_sort_prefix(mykey, myref, lane, ni);
-        if ((int)lane < ni) {
-          W.snode[sp + ni - 1 - (int)lane] = myref;
-          W.skey[sp + ni - 1 - (int)lane] = mykey;
+        if (ni == 1) {
+          if ((imask >> lane) & 1u) W.stk[sp] = make_uint2(pref, __float_as_uint(ptn));
+          top = __shfl_sync(kFull, pref, __ffs(imask) - 1);
+        } else {
+          // gathered into lanes 0..ni-1 through the free stack slots above
+          // sp, sorted, and pushed farthest first
+          float mykey = CUDART_INF_F;
+          uint32_t myref = 0;
+          if ((imask >> lane) & 1u) {
+            const int q = sp + __popc(imask & lt_mask);
+            W.stk[q] = make_uint2(pref, __float_as_uint(ptn));
+          }
+          __syncwarp();
+          if ((int)lane < ni) {
+            const uint2 e = W.stk[sp + (int)lane];
+            mykey = __uint_as_float(e.y);
+            myref = e.x;
+          }
+          __syncwarp();
+          warp_sort_prefix(mykey, myref, lane, ni);
+          if ((int)lane < ni) W.stk[sp + ni - 1 - (int)lane] = make_uint2(myref, __float_as_uint(mykey));
+          top = __shfl_sync(kFull, myref, 0);
         }
         sp += ni;
       }
+      if (lane == 0) st.node_visits += 1;
       __syncwarp();
       if (sp > 0) {
-        pf_node = W.snode[sp - 1];
+        pf_node = ni > 0 ? top : W.stk[sp - 1].x;
         if (lane < 16) pf = __ldg(S.nodes8 + 16 * (size_t)pf_node + lane);
       }
     }
@@ -408,19 +407,22 @@ __device__ __forceinline__ void packet_traverse(const SceneDev& S, const FaceTab
         const uint32_t found = __reduce_add_sync(kFull, (uint32_t)nh);
         if (lane == 0) st.anyhits += found;
         if (found) {
+          // the lowest lane of the lanes whose pairs target one ray inserts
+          // all their hits (lane by lane, each lane's last hit first)
+          const uint32_t peers = __match_any_sync(kFull, nh ? r : 64u + lane);
+          W.hp[lane] = nh ? __ldg(S.leaf_pidx + j) : 0u;
+          W.hc[lane] = (uint8_t)nh;
           __syncwarp();
-          const uint32_t p = nh ? __ldg(S.leaf_pidx + j) : 0u;
-          // one lane per target ray inserts at a time
-          while (true) {
-            const bool pend = nh > 0;
-            if (!__any_sync(kFull, pend)) break;
-            const uint32_t peers = __match_any_sync(kFull, pend ? r : 64u + lane);
-            if (pend && (int)lane == __ffs(peers) - 1) {
-              heap_offer(W, r, cap, hit_key(W.hq[nh - 1][lane], p));
-              --nh;
+          if (nh && (int)lane == __ffs(peers) - 1) {
+            uint32_t m = peers;
+            while (m) {
+              const int q = __ffs(m) - 1;
+              m &= m - 1;
+              const uint32_t pq = W.hp[q];
+              for (int h = (int)W.hc[q] - 1; h >= 0; --h) heap_offer(W, r, cap, hit_key(W.hq[h][q], pq));
             }
-            __syncwarp();
           }
+          __syncwarp();
           thi = W.thi[lane];
           thi_max = warp_max_f(thi);
         }
@@ -652,10 +654,21 @@ __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__
           ++step;
           ++n_rounds;
           n_entries += n;
-          // front-to-back accumulation in entry order (src/GS_shader.ts:250-269)
+          // front-to-back accumulation in entry order (src/GS_shader.ts:250-269);
+          // the next entry's shading record is loaded while this one is shaded
+          uint32_t nep = 0;
+          Shade nsd{};
+          if (n) {
+            nep = key_p(W.hk[head][lane]);
+            nsd = load_shade(V.s.shade, nep);
+          }
           for (uint32_t e = 0; e < n; ++e) {
-            const uint32_t ep = key_p(W.hk[head + e][lane]);
-            const Shade sd = load_shade(V.s.shade, ep);
+            const uint32_t ep = nep;
+            const Shade sd = nsd;
+            if (e + 1 < n) {
+              nep = key_p(W.hk[head + e + 1][lane]);
+              nsd = load_shade(V.s.shade, nep);
+            }
             const float alpha = response(sd, o, d) * sd.opacity;
             if (V.u.alpha_min < alpha) {
               const V3 dir = vnorm(vsub(sd.mu, o));

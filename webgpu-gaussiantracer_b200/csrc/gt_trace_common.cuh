@@ -191,14 +191,18 @@ __device__ __forceinline__ void proxy_test(const FaceTable& F, const float4* w2o
     }
   }
   // the exact tests of the candidates: t-range prefilter (faces whose facing
-  // is certain), then the reference's triangle test and facing rule
+  // is certain), then the reference's triangle test and facing rule.  The
+  // candidates of non-grazing pairs have dn < -tau: the reference's facing
+  // product (within 12 u nmax s of dn, tau = 1e-5 nmax s) is then negative,
+  // so only the grazing pairs' faces need it computed.
 #pragma unroll 1
   while (cand) {
     const int f = __ffs(cand) - 1;
     cand &= cand - 1;
     const V3 nf = mk(F.n[f][0], F.n[f][1], F.n[f][2]);
     const float dn = vdot(nf, od);
-    if (fabsf(dn) > tau) {
+    const bool sure = fabsf(dn) > tau;
+    if (sure) {
       // the t-range test: t times dn lies within E = 10 u nmax (|p0|_1 +
       // |o|_1) of num = n.p0 - n.o, so a face with num >= tlo*dn + M or
       // num <= thi*dn - M (dn < 0) has its t outside (tlo, thi)
@@ -208,7 +212,8 @@ __device__ __forceinline__ void proxy_test(const FaceTable& F, const float4* w2o
       if (num >= __fmaf_rn(tlo, dn, mg) || num <= __fmaf_rn(thi, dn, -mg)) continue;
     }
     float t;
-    if (tri_test(F, f, oo, tlo, od, thi, dn, t) && front_facing(F, f, load_affine(w2o + 3 * (size_t)j), d))
+    if (tri_test(F, f, oo, tlo, od, thi, dn, t) &&
+        (sure ? dn < 0.0f : front_facing(F, f, load_affine(w2o + 3 * (size_t)j), d)))
       on_hit(t, f);
   }
 }
