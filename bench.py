@@ -379,6 +379,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-step-budget", type=float, default=0.0,
                     help="--impl reference: seconds of CPU work per step (0: 60 s spread over the steps)")
+    ap.add_argument("--shape", default=None,
+                    help="packets:KBUF:HANDOFF_AFTER or warp:KBUF: this launch shape instead of the tuner's")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched and forward+backward measurements")
     ap.add_argument("--extra", choices=["fwd_bwd", "batched", "batched_fwd_bwd"], default=None,
@@ -471,11 +473,22 @@ def main():
     # k-buffer size and hand-off point of the tile packets, blocks, k-buffer
     # and leaf batch of the warp-per-ray kernel), cached by the context and
     # used by every render below
-    tune = ctx.autotune(scene, v.uniforms, w, h)
+    # (--shape installs a given shape instead, without the tuner's launches:
+    # the profiling commands use it so that their launch lists hold renders)
+    if args.shape:
+        kind, kb, ha = (args.shape.split(":") + ["0", "0"])[:3]
+        bt = 32 if kind == "packets" else 128
+        ctx.set_tune(scene, v.uniforms, w, h, block_threads=bt, kbuf=int(kb) or (32 if bt == 32 else 64),
+                     handoff_after=int(ha), blocks_per_sm=8)
+        tune = {"block_threads": bt, "kbuf": int(kb), "handoff_after": int(ha), "blocks_per_sm": 8,
+                "best_ms": None, "default_ms": None}
+    else:
+        tune = ctx.autotune(scene, v.uniforms, w, h)
     shape = {"kernel": "tile packets" if tune["block_threads"] == 32 else "warp per ray", "kbuf": tune["kbuf"],
              "handoff_after": tune["handoff_after"] if tune["block_threads"] == 32 else None,
              "blocks_per_sm": tune["blocks_per_sm"] if tune["block_threads"] == 128 else None,
-             "tuned_ms": tune["best_ms"], "default_shape_ms": tune["default_ms"]}
+             "tuned_ms": tune["best_ms"], "default_shape_ms": tune["default_ms"],
+             "source": "--shape " + args.shape if args.shape else "gt_autotune"}
     # one synchronous render: counters for the algorithmic byte count
     st0 = ctx.render_device(scene, v.uniforms, w, h, out_dev)
     alg_bytes = 16 * st0["rays"] + 44 * st0["entries"] + 192 * st0["contributing"]

@@ -237,11 +237,12 @@ class Context:
         return {name: getattr(r, name) for name, _ in r._fields_ if not name.startswith("_")}
 
     def set_tune(self, scene: "Scene", uniforms, width: int, height: int, blocks_per_sm: int = 4,
-                 kbuf: int = 32, leaf_batch: int = 32, block_threads: int = 128):
+                 kbuf: int = 32, leaf_batch: int = 32, block_threads: int = 128, handoff_after: int = 0):
         """Installs a launch shape for this (scene, k, image size) bucket:
         block_threads 32 traces 8x4 tiles of rays per warp (kbuf entries per
-        ray), 128 one ray per warp (gt_set_tune)."""
-        r = L.TuneResult(block_threads, blocks_per_sm, 8, 4, 0.0, 0.0, kbuf, leaf_batch, 0, 0)
+        ray, rays handed to a warp-per-ray launch after handoff_after
+        traversals, 0: the default), 128 one ray per warp (gt_set_tune)."""
+        r = L.TuneResult(block_threads, blocks_per_sm, 8, 4, 0.0, 0.0, kbuf, leaf_batch, handoff_after, 0)
         self.check(self._lib.gt_set_tune(self._h, scene.handle, C.byref(_uniforms(uniforms)), width, height,
                                          C.byref(r)))
 
