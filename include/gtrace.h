@@ -249,7 +249,11 @@ gt_status gt_scene_create_from_ply_file(gt_context* ctx, const char* path, doubl
  *   u          the 112-byte uniform block (debug_mode 0, 1 and 2 are supported)
  *   w, h       image size; any value >= 1 (the reference needs multiples of 8)
  *   out_rgba   w*h*4 floats, pixel (x, y) at index 4*(w*y + x); RGB = radiance,
- *              A = 1 (src/GS_shader.ts:300-301)
+ *              A = 1 (src/GS_shader.ts:300-301).  A host buffer that is
+ *              page-locked for this GPU (gt_host_alloc, cudaHostAlloc,
+ *              cudaMallocHost, cudaHostRegister) is written by the kernels
+ *              directly, tile by tile; any other host buffer receives one copy
+ *              after the render
  *   flags      GT_FLAG_OUTPUT_DEVICE, GT_FLAG_ASYNC, GT_FLAG_ANTIALIAS (out_rgba
  *              then also holds the running average of the earlier frames),
  *              GT_FLAG_CHECKPOINT (not with GT_FLAG_ANTIALIAS)

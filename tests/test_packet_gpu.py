@@ -114,11 +114,13 @@ def test_batch_of_views_and_scenes(ctx):
     assert st["rays"] == 37 * 21 + 24 * 40 + 16 * 16
 
 
-def test_handoff_across_views(ctx):
+@pytest.mark.parametrize("handoff_after", [0, 1, 6, 64])
+def test_handoff_across_views(ctx, handoff_after):
     """Rays that reach the packets' traversal limit go to the warp-per-ray
     kernel with their compositing state, in a batch of views of two scenes.
     Dense scenes, k = 2 and 8-entry buffers make most rays reach it; every
-    view must equal the oracle bit for bit."""
+    view must equal the oracle bit for bit, for the default hand-off point
+    (0: after 3 traversals) and others the tuner may choose."""
     pa = small_scene(n=12000, seed=57)
     pb = small_scene(n=9000, seed=58)
     ga, gb = Scene(ctx, pa.gaussiansBuffer, 0.01), Scene(ctx, pb.gaussiansBuffer, 0.01)
@@ -127,7 +129,7 @@ def test_handoff_across_views(ctx):
              (gb, view(24, 40, k=2, T_min=0.0001).uniforms, 24, 40),
              (ga, view(33, 17, pos=(1.0, 2.0, 3.5), k=2, T_min=0.0001).uniforms, 33, 17),
              (gb, view(16, 24, pos=(-2.0, 0.5, 3.0), k=2, T_min=0.0001).uniforms, 16, 24)]
-    ctx.set_tune(views[0][0], views[0][1], 40, 24, kbuf=8, block_threads=32)
+    ctx.set_tune(views[0][0], views[0][1], 40, 24, kbuf=8, block_threads=32, handoff_after=handoff_after)
     try:
         outs, st = ctx.render_batch(views)
     finally:
@@ -137,6 +139,8 @@ def test_handoff_across_views(ctx):
         assert np.array_equal(_bits(out), ref.view(np.uint32))
     rays = sum(w * h for _, _, w, h in views)
     assert st["rays"] == rays
+    # (the packets hand over once every tile of the launch is taken, so even
+    # the latest hand-off point hands rays over at these sizes)
     assert st["handed"] > rays // 4, st["handed"]
 
 

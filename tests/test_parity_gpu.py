@@ -196,6 +196,40 @@ def test_device_output_and_async(ctx):
     np.testing.assert_array_equal(out, host)
 
 
+@pytest.mark.parametrize("block_threads", [128, 32])
+def test_page_locked_host_output(ctx, block_threads):
+    """A page-locked host buffer is written by the trace kernels directly
+    (no staging copy); the image equals the one a pageable buffer receives
+    through the copy, bit for bit, for both forward kernels, with pixels
+    handed between them, and for an anti-aliased frame (which takes the
+    staging path)."""
+    pg = small_scene(n=6000, seed=16)
+    g = Scene(ctx, pg.gaussiansBuffer, 0.01)
+    w, h = 45, 29
+    v = view(w, h, k=4, T_min=0.0001)
+    ctx.set_tune(g, v.uniforms, w, h, kbuf=8 if block_threads == 32 else 64, block_threads=block_threads,
+                 handoff_after=1)
+    pinned = ctx.host_alloc(w * h * 16, np.float32, (h, w, 4))
+    try:
+        ref = ctx.render(g, v.uniforms, w, h)
+        pinned[...] = np.nan
+        st = ctx.render(g, v.uniforms, w, h, out=pinned, stats=True)[1]
+        assert st["rays"] == w * h
+        np.testing.assert_array_equal(pinned.view(np.uint32), ref.view(np.uint32))
+        if block_threads == 32:
+            assert st["handed"] > 0
+        # anti-aliased frames 0 and 1 into the page-locked buffer
+        page = np.zeros((h, w, 4), np.float32)
+        for f in (0, 1):
+            u = with_fields(v.uniforms, accumulated_frames=f)
+            ctx.render(g, u, w, h, out=page, antialias=True)
+            ctx.render(g, u, w, h, out=pinned, antialias=True)
+        np.testing.assert_array_equal(pinned.view(np.uint32), page.view(np.uint32))
+    finally:
+        ctx._lib.gt_autotune_reset(ctx._h)
+        ctx.host_free(pinned)
+
+
 def test_scene_from_device_buffer(ctx):
     pg = small_scene(n=700, seed=15)
     rec = np.ascontiguousarray(pg.gaussiansBuffer)
@@ -332,6 +366,15 @@ def test_clusters_1m_stratified_subset(ctx):
     r64, _ = oracle.Scene(pg.gaussiansBuffer, amin, "f64").render(v.uniforms, w, h, pixels=pix)
     rmse = float(np.sqrt(np.mean((img[pix, :3] - r64[:, :3]) ** 2)))
     assert rmse < 1e-4, rmse
+    # the tile packets' later hand-off points (the tuner's choices at this
+    # size) give the whole image of the default bit for bit
+    for ha in (6, 64):
+        ctx.set_tune(g, v.uniforms, w, h, kbuf=32, block_threads=32, handoff_after=ha)
+        try:
+            other = ctx.render(g, v.uniforms, w, h).reshape(-1, 4)
+        finally:
+            ctx._lib.gt_autotune_reset(ctx._h)
+        np.testing.assert_array_equal(other.view(np.uint32), img.view(np.uint32), err_msg=f"handoff_after={ha}")
 
 
 def test_batched_config_shape(ctx):

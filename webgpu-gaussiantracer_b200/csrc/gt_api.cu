@@ -580,7 +580,26 @@ extern "C" gt_status gt_render(gt_context* ctx, const gt_scene* scene, const gt_
   API_CUDA(ctx, cudaSetDevice(ctx->device));
   size_t bytes = (size_t)w * h * sizeof(float4);
   float4* out = reinterpret_cast<float4*>(out_rgba);
-  if (!(flags & GT_FLAG_OUTPUT_DEVICE)) {
+  // A page-locked host buffer of this GPU (cudaHostAlloc, cudaMallocHost or
+  // cudaHostRegister with a device mapping) is written by the trace kernels
+  // directly: each tile's pixels cross the host link when the tile is done,
+  // instead of the whole image in one copy after the render.  Anti-aliased
+  // frames (which read the previous average) and checkpointing renders take
+  // the staging buffer.
+  bool direct = false;
+  if (!(flags & GT_FLAG_OUTPUT_DEVICE) && !aa && !(flags & GT_FLAG_CHECKPOINT)) {
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, out_rgba) == cudaSuccess) {
+      if (pa.type == cudaMemoryTypeHost && pa.device == ctx->device && pa.devicePointer &&
+          (uintptr_t)pa.devicePointer % 16 == 0) {
+        out = reinterpret_cast<float4*>(pa.devicePointer);
+        direct = true;
+      }
+    } else {
+      (void)cudaGetLastError();  // (an unknown pointer: the staging path)
+    }
+  }
+  if (!(flags & GT_FLAG_OUTPUT_DEVICE) && !direct) {
     st = ensure_staging(ctx, bytes);
     if (st != GT_OK) return st;
     out = ctx->staging;
@@ -617,7 +636,7 @@ extern "C" gt_status gt_render(gt_context* ctx, const gt_scene* scene, const gt_
                        ctx->d_views, nullptr, &hand);
   if (e.code != GT_OK) return fail(ctx, e);
   API_CUDA(ctx, cudaEventRecord(ctx->ring[2 * slot + 1], ctx->stream));
-  if (!(flags & GT_FLAG_OUTPUT_DEVICE))
+  if (!(flags & GT_FLAG_OUTPUT_DEVICE) && !direct)
     API_CUDA(ctx, cudaMemcpyAsync(out_rgba, out, bytes, cudaMemcpyDeviceToHost, ctx->stream));
   if (flags & GT_FLAG_ASYNC) return GT_OK;
   return finish_call(ctx, stats, slot);

@@ -23,7 +23,7 @@
 //     the queue (and the shared memory of a warp) small: warps per SM are
 //     bounded by shared memory, and more of them hide more latency;
 //   * k-buffer: each ray keeps the kbuf smallest (t, particle) hits in a
-//     max-heap of its own (a column of a shared-memory array of 64-bit keys
+//     4-ary max-heap of its own (a column of a shared-memory array of 64-bit keys
 //     that order like (t, particle)); its root is the ray's far bound.  The
 //     hits of one face-test batch are inserted by one lane per target ray
 //     (__match_any_sync groups the lanes whose pairs test that ray);
@@ -54,7 +54,7 @@ constexpr int kSurvCap = 64;  // pairs that passed the sphere filter (< kSurvivo
 
 template <int KB>
 struct PacketScratch {
-  unsigned long long hk[KB][32];  // heap of ray r in column r: hit keys, max at row 0
+  unsigned long long hk[KB][32];  // 4-ary heap of ray r in column r: hit keys, max at row 0
   uint2 stk[kWarpStack];  // node stack: (node, bits of its entry distance)
   uint32_t lj[8];  // leaf children of the visited node that some ray hit,
   uint32_t lm[8];  // with the mask of those rays
@@ -91,24 +91,30 @@ __device__ __forceinline__ unsigned long long hit_key(float t, uint32_t p) {
 __device__ __forceinline__ float key_t(unsigned long long k) { return unord_f((uint32_t)(k >> 32)); }
 __device__ __forceinline__ uint32_t key_p(unsigned long long k) { return (uint32_t)k; }
 
+// The k-buffer of ray r is a 4-ary max-heap in column r (children of row i:
+// rows 4i+1 .. 4i+4): 32 entries are 3 levels deep instead of 5, and the
+// four children of a row are loaded together, so a sift waits on 3 rounds
+// of shared-memory latency instead of 5.
+
 // Sift key x down from row i of heap column r holding n entries.
 template <int KB>
 __device__ __forceinline__ void heap_sift(PacketScratch<KB>& W, uint32_t r, uint32_t i, uint32_t n,
                                           unsigned long long x) {
   while (true) {
-    uint32_t c = 2 * i + 1;
+    const uint32_t c = 4 * i + 1;
     if (c >= n) break;
-    unsigned long long ck = W.hk[c][r];
-    if (c + 1 < n) {
-      const unsigned long long c2 = W.hk[c + 1][r];
-      if (ck < c2) {
-        c = c + 1;
-        ck = c2;
-      }
-    }
+    // the last child is clamped to the last entry (a repeated child changes
+    // nothing: ties keep the first)
+    const uint32_t c1 = min(c + 1, n - 1), c2 = min(c + 2, n - 1), c3 = min(c + 3, n - 1);
+    const unsigned long long k0 = W.hk[c][r], k1 = W.hk[c1][r], k2 = W.hk[c2][r], k3 = W.hk[c3][r];
+    const bool s01 = k0 < k1, s23 = k2 < k3;
+    const unsigned long long m01 = s01 ? k1 : k0, m23 = s23 ? k3 : k2;
+    const uint32_t i01 = s01 ? c1 : c, i23 = s23 ? c3 : c2;
+    const bool s = m01 < m23;
+    const unsigned long long ck = s ? m23 : m01;
     if (!(x < ck)) break;
     W.hk[i][r] = ck;
-    i = c;
+    i = s ? i23 : i01;
   }
   W.hk[i][r] = x;
 }
@@ -121,7 +127,7 @@ __device__ __forceinline__ void heap_offer(PacketScratch<KB>& W, uint32_t r, uin
   if (n < cap) {
     uint32_t i = n;
     while (i > 0) {
-      const uint32_t par = (i - 1) >> 1;
+      const uint32_t par = (i - 1) >> 2;
       const unsigned long long pk = W.hk[par][r];
       if (!(pk < x)) break;
       W.hk[i][r] = pk;
