@@ -96,10 +96,13 @@ __device__ __forceinline__ uint32_t key_p(unsigned long long k) { return (uint32
 // four children of a row are loaded together, so a sift waits on 3 rounds
 // of shared-memory latency instead of 5.
 
-// Sift key x down from row i of heap column r holding n entries.
+// Sift key x down from row i of heap column r holding n entries; returns
+// the key that ends in row i (x, or the largest child that moved up).
 template <int KB>
-__device__ __forceinline__ void heap_sift(PacketScratch<KB>& W, uint32_t r, uint32_t i, uint32_t n,
-                                          unsigned long long x) {
+__device__ __forceinline__ unsigned long long heap_sift(PacketScratch<KB>& W, uint32_t r, uint32_t i, uint32_t n,
+                                                        unsigned long long x) {
+  const uint32_t i0 = i;
+  unsigned long long top = x;
   while (true) {
     const uint32_t c = 4 * i + 1;
     if (c >= n) break;
@@ -114,33 +117,47 @@ __device__ __forceinline__ void heap_sift(PacketScratch<KB>& W, uint32_t r, uint
     const unsigned long long ck = s ? m23 : m01;
     if (!(x < ck)) break;
     W.hk[i][r] = ck;
+    if (i == i0) top = ck;
     i = s ? i23 : i01;
   }
   W.hk[i][r] = x;
+  return top;
 }
 
-// Offers hit key x to the k-buffer of ray r (capacity cap): kept when the
-// buffer is not full or x is below its largest entry.
+// Offers the hits of the lanes in `peers` (all of them hits of ray r, hc[q]
+// keys of particle hp[q] in column q of hq) to the k-buffer of ray r
+// (capacity cap), lane by lane and each lane's last hit first: a hit is kept
+// when the buffer is not full or it is below the buffer's largest entry.
+// The heap size and root stay in registers over the run; the ray's far bound
+// (the root of a full buffer) is written once at the end.
 template <int KB>
-__device__ __forceinline__ void heap_offer(PacketScratch<KB>& W, uint32_t r, uint32_t cap, unsigned long long x) {
-  const uint32_t n = W.hn[r];
-  if (n < cap) {
-    uint32_t i = n;
-    while (i > 0) {
-      const uint32_t par = (i - 1) >> 2;
-      const unsigned long long pk = W.hk[par][r];
-      if (!(pk < x)) break;
-      W.hk[i][r] = pk;
-      i = par;
+__device__ __forceinline__ void heap_offer_run(PacketScratch<KB>& W, uint32_t r, uint32_t cap, uint32_t peers) {
+  uint32_t n = W.hn[r];
+  unsigned long long root = n == cap ? W.hk[0][r] : 0ull;
+  while (peers) {
+    const int q = __ffs(peers) - 1;
+    peers &= peers - 1;
+    const uint32_t pq = W.hp[q];
+    for (int h = (int)W.hc[q] - 1; h >= 0; --h) {
+      const unsigned long long x = hit_key(W.hq[h][q], pq);
+      if (n < cap) {
+        uint32_t i = n;
+        while (i > 0) {
+          const uint32_t par = (i - 1) >> 2;
+          const unsigned long long pk = W.hk[par][r];
+          if (!(pk < x)) break;
+          W.hk[i][r] = pk;
+          i = par;
+        }
+        W.hk[i][r] = x;
+        if (++n == cap) root = W.hk[0][r];
+      } else if (x < root) {
+        root = heap_sift(W, r, 0, n, x);
+      }
     }
-    W.hk[i][r] = x;
-    W.hn[r] = (uint8_t)(n + 1);
-    if (n + 1 == cap) W.thi[r] = key_t(W.hk[0][r]);
-  } else {
-    if (!(x < W.hk[0][r])) return;
-    heap_sift(W, r, 0, n, x);
-    W.thi[r] = key_t(W.hk[0][r]);
   }
+  W.hn[r] = (uint8_t)n;
+  if (n == cap) W.thi[r] = key_t(root);
 }
 
 // Sorts heap column r (n entries) ascending.
@@ -419,15 +436,7 @@ __device__ __forceinline__ void packet_traverse(const SceneDev& S, const FaceTab
           W.hp[lane] = nh ? __ldg(S.leaf_pidx + j) : 0u;
           W.hc[lane] = (uint8_t)nh;
           __syncwarp();
-          if (nh && (int)lane == __ffs(peers) - 1) {
-            uint32_t m = peers;
-            while (m) {
-              const int q = __ffs(m) - 1;
-              m &= m - 1;
-              const uint32_t pq = W.hp[q];
-              for (int h = (int)W.hc[q] - 1; h >= 0; --h) heap_offer(W, r, cap, hit_key(W.hq[h][q], pq));
-            }
-          }
+          if (nh && (int)lane == __ffs(peers) - 1) heap_offer_run(W, r, cap, peers);
           __syncwarp();
           thi = W.thi[lane];
           thi_max = warp_max_f(thi);
