@@ -195,6 +195,40 @@ static gt_status ensure_staging(gt_context* ctx, size_t bytes) {
   return GT_OK;
 }
 
+// Gives every plain-render view of a launch its own particle colour table
+// (ViewDev::rgb, filled by k_view_colours before the trace kernels) in the
+// context's colour buffer, grown as needed.  A launch whose tables would
+// take more than kColourBudget bytes, or that has more views than a grid has
+// rows, keeps the per-entry evaluation (same image bits either way).
+constexpr uint64_t kColourBudget = 2ull << 30;
+static gt_status assign_colours(gt_context* ctx, ViewDev* views, uint32_t n) {
+  uint64_t need = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    views[i].rgb = nullptr;
+    if (views[i].u.debug == 0) need += views[i].n_particles;
+  }
+  if (need == 0 || n > 65535u || need * sizeof(float4) > kColourBudget) return GT_OK;
+  if (need > ctx->colours_cap) {
+    API_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    cudaFree(ctx->colours);
+    ctx->colours = nullptr;
+    ctx->colours_cap = 0;
+    if (cudaMalloc(&ctx->colours, need * sizeof(float4)) != cudaSuccess) {
+      (void)cudaGetLastError();
+      ctx->colours = nullptr;
+      return GT_OK;  // (no room: the per-entry evaluation)
+    }
+    ctx->colours_cap = need;
+  }
+  uint64_t at = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (views[i].u.debug != 0) continue;
+    views[i].rgb = ctx->colours + at;
+    at += views[i].n_particles;
+  }
+  return GT_OK;
+}
+
 static SceneDev scene_dev(const gt_scene* s) {
   SceneDev d;
   d.nodes8 = s->b.nodes8;
@@ -366,6 +400,7 @@ extern "C" gt_status gt_context_destroy(gt_context* ctx) {
   cudaFree(ctx->d_handoff);
   cudaFreeHost(ctx->h_views);
   cudaFree(ctx->staging);
+  cudaFree(ctx->colours);
   delete ctx->copy_pool;
   for (int b = 0; b < 2; ++b) {
     if (ctx->up_pinned[b]) cudaFreeHost(ctx->up_pinned[b]);
@@ -624,6 +659,8 @@ extern "C" gt_status gt_render(gt_context* ctx, const gt_scene* scene, const gt_
   if (st != GT_OK) return st;
   ViewDev v = make_view(scene, *u, w, h, out, 0);
   v.u.aa = aa ? 1u : 0u;
+  st = assign_colours(ctx, &v, 1);
+  if (st != GT_OK) return st;
   API_CUDA(ctx, cudaEventRecord(ctx->call0, ctx->stream));
   API_CUDA(ctx, cudaMemsetAsync(ctx->d_ctr, 0, sizeof(DevCounters), ctx->stream));
   uint64_t slot = ring_slot(ctx);
@@ -803,10 +840,14 @@ extern "C" gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items
       API_CUDA(ctx, cudaMemcpyAsync(out, it.out_rgba, (size_t)it.w * it.h * sizeof(float4), cudaMemcpyHostToDevice,
                                     ctx->stream));
   }
+  st = assign_colours(ctx, ctx->h_views, count);
+  if (st != GT_OK) return st;
+  bool colours = false;  // (the graph holds the colour kernel or not)
+  for (uint32_t q = 0; q < count; ++q) colours = colours || ctx->h_views[q].rgb != nullptr;
   API_CUDA(ctx, cudaEventRecord(ctx->call0, ctx->stream));
   uint64_t slot = ring_slot(ctx);
   API_CUDA(ctx, cudaEventRecord(ctx->ring[2 * slot], ctx->stream));
-  // One graph per batch shape: counter reset + the persistent kernel.  A
+  // One graph per batch shape: colour tables, counter reset, the trace kernels.  A
   // shape tuned for batches of this shape (gt_autotune_batch) comes first.
   auto bt = ctx->batch_tune.find(std::make_tuple(count, total_tiles, kmax));
   LaunchShape shape = bt != ctx->batch_tune.end() ? shape_of(bt->second)
@@ -824,7 +865,8 @@ extern "C" gt_status gt_render_batch(gt_context* ctx, const gt_batch_item* items
   }
   // the kernels of the graph: warp-per-ray slots per lane, and with tile
   // packets their heap size and handoff
-  auto key = std::make_tuple(count, total_tiles, kmax | (any_debug ? 0x10000u : 0u) | (packet ? 0x20000u : 0u),
+  auto key = std::make_tuple(count, total_tiles,
+                             kmax | (any_debug ? 0x10000u : 0u) | (packet ? 0x20000u : 0u) | (colours ? 0x40000u : 0u),
                              shape.blocks_per_sm,
                              ((kb_max + 31u) / 32u) | (packet ? (pkb_max << 8) | (shape.handoff_after << 16) : 0u));
   auto it = ctx->graphs.find(key);
@@ -891,6 +933,8 @@ extern "C" gt_status gt_autotune(gt_context* ctx, const gt_scene* scene, const g
   st = ensure_views(ctx, 1);
   if (st != GT_OK) return st;
   ViewDev v = make_view(scene, *u, w, h, ctx->staging, 0);
+  st = assign_colours(ctx, &v, 1);  // as gt_render renders it
+  if (st != GT_OK) return st;
   Handoff hand;
   st = ensure_handoff(ctx, (uint64_t)w * h, &hand);
   if (st != GT_OK) return st;
@@ -1044,6 +1088,8 @@ extern "C" gt_status gt_autotune_batch(gt_context* ctx, const gt_batch_item* ite
     total_tiles += ctx->h_views[q].n_tiles;
     off += (size_t)it.w * it.h;
   }
+  st = assign_colours(ctx, ctx->h_views, count);  // as gt_render_batch renders it
+  if (st != GT_OK) return st;
   auto time_shape = [&](const LaunchShape& sh, int reps, float* out_ms) -> gt_status {
     float ms_min = 1e30f;
     for (int rep = 0; rep < reps; ++rep) {

@@ -297,4 +297,18 @@ __device__ __forceinline__ void sh_radiance(const float4* sh, uint32_t p, V3 d, 
   }
 }
 
+// The colour an entry of particle p adds for a ray from o
+// (src/GS_shader.ts:258-264,189): max(0, SH(normalize(mu - o))) per channel
+// (NaN and -0 become +0).  It does not depend on the ray's direction, so all
+// primary rays of a view (they share o) get the same colour for p.
+__device__ __forceinline__ void entry_colour(const float4* sh, uint32_t p, V3 mu, V3 o, uint32_t deg, float& x0,
+                                             float& x1, float& x2) {
+  const V3 dir = vnorm(vsub(mu, o));
+  float c[3];
+  sh_radiance(sh, p, dir, deg, c);
+  x0 = c[0] > 0.f ? c[0] : 0.f;
+  x1 = c[1] > 0.f ? c[1] : 0.f;
+  x2 = c[2] > 0.f ? c[2] : 0.f;
+}
+
 }  // namespace gt

@@ -58,6 +58,9 @@ struct gt_context {
   uint32_t h_views_cap = 0;
   float4* staging = nullptr;
   size_t staging_bytes = 0;
+  // per-view particle colour tables of the render calls (ViewDev::rgb)
+  float4* colours = nullptr;
+  uint64_t colours_cap = 0;  // float4 entries
   // pinned chunks through which host records are uploaded (double-buffered)
   struct CopyPool* copy_pool = nullptr;  // host threads of the pinned uploads (gt_api.cu)
   unsigned char* up_pinned[2] = {nullptr, nullptr};

@@ -128,6 +128,10 @@ struct ViewDev {
   float4* grad;         // backward: the scene's per-particle sums of the response terms (4 float4 a particle)
   float4* grad_sh;      // backward: this view's per-particle sums of the colour weights (1 float4 a particle)
   uint64_t n_particles;
+  // this view's colour of every particle, max(0, SH(normalize(mu - camera)))
+  // per channel (k_view_colours, before the trace launch), or null: the
+  // trace kernels evaluate the SH per composited entry
+  float4* rgb;
 };
 
 // Launch shape of the persistent trace kernel.

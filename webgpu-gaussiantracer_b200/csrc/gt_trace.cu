@@ -216,12 +216,14 @@ __device__ __forceinline__ float4 trace_ray_warp(const ViewDev& V, const FaceTab
         alpha = response(sd, R.o, R.d) * sd.opacity;
         contrib = V.u.alpha_min < alpha;
         if (contrib) {
-          V3 dir = vnorm(vsub(sd.mu, R.o));
-          float c[3];
-          sh_radiance(V.s.sh, ep, dir, V.u.deg, c);
-          c0 = c[0] > 0.f ? c[0] : 0.f;
-          c1 = c[1] > 0.f ? c[1] : 0.f;
-          c2 = c[2] > 0.f ? c[2] : 0.f;
+          if (V.rgb) {
+            const float4 q = __ldg(V.rgb + ep);
+            c0 = q.x;
+            c1 = q.y;
+            c2 = q.z;
+          } else {
+            entry_colour(V.s.sh, ep, sd.mu, R.o, V.u.deg, c0, c1, c2);
+          }
         }
         if (RECORD) {
           uint32_t e = R.n_entries + lane;
@@ -392,12 +394,41 @@ void apply_shape(ViewDev* views, uint32_t n_views, const LaunchShape& shape) {
   }
 }
 
+// The colour table of each view that has one: thread p of row v writes view
+// v's colour of particle p (entry_colour, the arithmetic of the trace
+// kernels' own evaluation, so the image bits do not depend on the table).
+// (A grid-stride loop: a launch captured in a batch graph serves later
+// batches of the same shape whose scenes hold more particles.)
+__global__ void k_view_colours(const ViewDev* __restrict__ views) {
+  const ViewDev& V = views[blockIdx.y];
+  if (!V.rgb) return;
+  const V3 o = mk(V.u.tw[12], V.u.tw[13], V.u.tw[14]);  // the rays' origin (ray_gen)
+  for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < V.n_particles;
+       p += (uint64_t)gridDim.x * blockDim.x) {
+    const V3 mu = load_shade(V.s.shade, (uint32_t)p).mu;
+    float x0, x1, x2;
+    entry_colour(V.s.sh, (uint32_t)p, mu, o, V.u.deg, x0, x1, x2);
+    V.rgb[p] = make_float4(x0, x1, x2, 0.0f);
+  }
+}
+
 Err launch_trace(ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
                  const FaceTable& faces, const LaunchShape& shape, int num_sms, cudaStream_t stream,
                  uint64_t* launches, ViewDev* d_views, const Ckpt* ckpt, const Handoff* handoff) {
   const bool packet = packet_launch(views, n_views, total_tiles, num_sms, shape, ckpt != nullptr);
   apply_shape(views, n_views, shape);
   GT_CUDA_TRY(cudaMemcpyAsync(d_views, views, sizeof(ViewDev) * n_views, cudaMemcpyHostToDevice, stream));
+  uint64_t colour_rows = 0;
+  for (uint32_t i = 0; i < n_views; ++i)
+    if (views[i].rgb) colour_rows = std::max<uint64_t>(colour_rows, views[i].n_particles);
+  if (colour_rows) {
+    if (n_views > 65535u) return Err{GT_ERR_INVALID_ARG, "colour tables for more than 65535 views"};
+    const uint32_t cb = 256;
+    const uint64_t blocks = std::min<uint64_t>((colour_rows + cb - 1) / cb, (uint64_t)num_sms * 16u);
+    k_view_colours<<<dim3((unsigned)blocks, n_views), cb, 0, stream>>>(d_views);
+    ++*launches;
+    GT_CUDA_TRY(cudaGetLastError());
+  }
   const bool hand = packet && handoff && handoff->rays && handoff->cap && shape.handoff_after;
   if (packet) {
     Err e = launch_trace_packet(views, d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches,
