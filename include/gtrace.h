@@ -135,7 +135,11 @@ typedef struct gt_scene_info {
 uint32_t gt_version(void);
 
 /* Creates a context on CUDA device `device`.  Replaces the adapter/device
- * request of src/main.ts:396-427. */
+ * request of src/main.ts:396-427.  Besides its scenes, a context keeps the
+ * scratch of its largest call so far: staging images, the hand-off buffer,
+ * checkpoints, and the colour tables of plain renders (16 bytes per
+ * particle per view of a call, at most 2 GiB; each particle's SH colour as
+ * seen from the view's camera, computed once per call before tracing). */
 gt_status gt_context_create(int device, gt_context** out);
 /* Destroys the context and every scene still alive on it (their handles
  * become invalid). */

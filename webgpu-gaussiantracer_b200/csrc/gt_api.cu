@@ -327,6 +327,7 @@ LaunchShape api_batch_shape_for(gt_context* ctx, const gt_scene* const* scenes, 
 void api_fill_stats(const DevCounters& c, gt_render_stats* st) { fill_stats(c, st); }
 gt_status api_ensure_views(gt_context* ctx, uint32_t n) { return ensure_views(ctx, n); }
 gt_status api_ensure_handoff(gt_context* ctx, uint64_t rays, Handoff* out) { return ensure_handoff(ctx, rays, out); }
+gt_status api_assign_colours(gt_context* ctx, ViewDev* views, uint32_t n) { return assign_colours(ctx, views, n); }
 }  // namespace gt
 
 // ============================================================== context

@@ -624,6 +624,8 @@ gt_status api_forward_ckpt(gt_context* ctx, const gt_scene* const* scenes, const
   Handoff hand;
   sst = api_ensure_handoff(ctx, rays, &hand);
   if (sst != GT_OK) return sst;
+  sst = api_assign_colours(ctx, vd.data(), count);  // as a plain render's
+  if (sst != GT_OK) return sst;
   for (int attempt = 0; attempt < 3; ++attempt) {
     if (want > 0xFFFFFFF0ull) return api_fail(ctx, GT_ERR_OOM, "checkpoint needs more than 2^32 records");
     uint32_t m = mode == 1 ? 1u : (mode == 2 ? 2u : (want * (kCkptHeader + kCkptChunk) * 4 <= budget ? 1u : 2u));

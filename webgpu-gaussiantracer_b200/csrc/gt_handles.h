@@ -106,6 +106,8 @@ LaunchShape api_batch_shape_for(gt_context* ctx, const gt_scene* const* scenes, 
 void api_fill_stats(const DevCounters& c, gt_render_stats* st);
 gt_status api_ensure_views(gt_context* ctx, uint32_t n);
 gt_status api_ensure_handoff(gt_context* ctx, uint64_t rays, Handoff* out);
+// Colour tables for the plain-render views of a launch (ViewDev::rgb).
+gt_status api_assign_colours(gt_context* ctx, ViewDev* views, uint32_t n);
 // Checkpointing forward (gt_backward.cu): renders the views into `outs`
 // (device, one per view) and keeps the round checkpoint in ctx->ckpt.
 gt_status api_forward_ckpt(gt_context* ctx, const gt_scene* const* scenes, const gt_uniforms* us, const uint32_t* ws,

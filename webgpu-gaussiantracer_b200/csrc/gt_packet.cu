@@ -626,7 +626,7 @@ __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__
               alpha = response(sd, o, d) * sd.opacity;
               if (V.u.alpha_min < alpha) {
                 contrib = true;
-                if (!CKPT && V.rgb) {  // (checkpointing views have no colour table)
+                if (V.rgb) {
                   const float4 q = __ldg(V.rgb + ep);
                   x0 = q.x;
                   x1 = q.y;
@@ -700,7 +700,7 @@ __global__ void __launch_bounds__(32) k_trace_packet(const ViewDev* __restrict__
             const float alpha = response(sd, o, d) * sd.opacity;
             if (V.u.alpha_min < alpha) {
               float x0, x1, x2;
-              if (!CKPT && V.rgb) {  // (checkpointing views have no colour table)
+              if (V.rgb) {
                 const float4 q = __ldg(V.rgb + ep);
                 x0 = q.x;
                 x1 = q.y;
