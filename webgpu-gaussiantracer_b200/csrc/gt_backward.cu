@@ -329,7 +329,18 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 4) k_backward(const ViewD
           resp = response(sd, o, d);
           alpha = resp * sd.opacity;
           contrib = V.u.alpha_min < alpha;
-          if (contrib) sh_radiance(V.s.sh, p, vnorm(vsub(sd.mu, o)), V.u.deg, craw);
+          if (contrib) {
+            if (V.rgb) {
+              // the view's colour table holds max(0, craw): the same signs
+              // and clamped values, which is all the adjoint uses of craw
+              const float4 q = __ldg(V.rgb + p);
+              craw[0] = q.x;
+              craw[1] = q.y;
+              craw[2] = q.z;
+            } else {
+              sh_radiance(V.s.sh, p, vnorm(vsub(sd.mu, o)), V.u.deg, craw);
+            }
+          }
         }
         const uint32_t cballot = __ballot_sync(kFull, contrib);
         const uint32_t cmask = (cballot >> seg_shift) & seg_bits;
@@ -797,6 +808,11 @@ gt_status backward_impl(gt_context* ctx, const BwdView* views, uint32_t count, c
   std::vector<ExpandView> hev(count);
   const LaunchShape shape = api_shape_for(ctx, views[0].scene, views[0].w, views[0].h, views[0].u.k);
   apply_shape(vd.data(), count, shape);
+  sst = api_assign_colours(ctx, vd.data(), count);  // filled before the first adjoint launch
+  if (sst != GT_OK) {
+    cleanup();
+    return sst;
+  }
   Ckpt ck;
   ck.head = cs.head;
   ck.pool = cs.pool;
@@ -831,6 +847,13 @@ gt_status backward_impl(gt_context* ctx, const BwdView* views, uint32_t count, c
       BWD_TRY(cudaMemsetAsync(G[s], 0, (size_t)std::max<uint64_t>(scenes[s]->n, 1) * 4 * sizeof(float4), st));
     BWD_TRY(cudaMemsetAsync(gs_all, 0, gs_off * sizeof(float4), st));
     BWD_TRY(cudaMemcpyAsync(ctx->d_views, vd.data(), sizeof(ViewDev) * count, cudaMemcpyHostToDevice, st));
+    if (gi == 0) {
+      Err ce = launch_view_colours(vd.data(), ctx->d_views, count, ctx->num_sms, st, &ctx->launches);
+      if (ce.code != GT_OK) {
+        cleanup();
+        return api_fail(ctx, ce.code, ce.msg);
+      }
+    }
     BWD_TRY(cudaMemsetAsync(&ctx->d_ctr->work, 0, sizeof(uint32_t), st));
     {
       const uint32_t tile0 = vd[g0].tile_begin;

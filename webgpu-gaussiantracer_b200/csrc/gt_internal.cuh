@@ -271,6 +271,10 @@ bool packet_launch(const ViewDev* views, uint32_t n_views, uint32_t total_tiles,
                    const LaunchShape& shape, bool ckpt);
 // Sets each view's k-buffer size and leaf batch for a launch of either kernel.
 void apply_shape(ViewDev* views, uint32_t n_views, const LaunchShape& shape);
+// Fills the colour table of every view that has one (ViewDev::rgb) from the
+// device copy of the view table.
+Err launch_view_colours(const ViewDev* views, const ViewDev* d_views, uint32_t n_views, int num_sms,
+                        cudaStream_t stream, uint64_t* launches);
 Err launch_trace(ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
                  const FaceTable& faces, const LaunchShape& shape, int num_sms, cudaStream_t stream,
                  uint64_t* launches, ViewDev* d_views_scratch, const Ckpt* ckpt = nullptr,

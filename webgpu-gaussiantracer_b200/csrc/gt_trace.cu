@@ -412,23 +412,29 @@ __global__ void k_view_colours(const ViewDev* __restrict__ views) {
   }
 }
 
+Err launch_view_colours(const ViewDev* views, const ViewDev* d_views, uint32_t n_views, int num_sms,
+                        cudaStream_t stream, uint64_t* launches) {
+  uint64_t colour_rows = 0;
+  for (uint32_t i = 0; i < n_views; ++i)
+    if (views[i].rgb) colour_rows = std::max<uint64_t>(colour_rows, views[i].n_particles);
+  if (colour_rows == 0) return Err{};
+  if (n_views > 65535u) return Err{GT_ERR_INVALID_ARG, "colour tables for more than 65535 views"};
+  const uint32_t cb = 256;
+  const uint64_t blocks = std::min<uint64_t>((colour_rows + cb - 1) / cb, (uint64_t)num_sms * 16u);
+  k_view_colours<<<dim3((unsigned)blocks, n_views), cb, 0, stream>>>(d_views);
+  ++*launches;
+  GT_CUDA_TRY(cudaGetLastError());
+  return Err{};
+}
+
 Err launch_trace(ViewDev* views, uint32_t n_views, uint32_t total_tiles, DevCounters* counters,
                  const FaceTable& faces, const LaunchShape& shape, int num_sms, cudaStream_t stream,
                  uint64_t* launches, ViewDev* d_views, const Ckpt* ckpt, const Handoff* handoff) {
   const bool packet = packet_launch(views, n_views, total_tiles, num_sms, shape, ckpt != nullptr);
   apply_shape(views, n_views, shape);
   GT_CUDA_TRY(cudaMemcpyAsync(d_views, views, sizeof(ViewDev) * n_views, cudaMemcpyHostToDevice, stream));
-  uint64_t colour_rows = 0;
-  for (uint32_t i = 0; i < n_views; ++i)
-    if (views[i].rgb) colour_rows = std::max<uint64_t>(colour_rows, views[i].n_particles);
-  if (colour_rows) {
-    if (n_views > 65535u) return Err{GT_ERR_INVALID_ARG, "colour tables for more than 65535 views"};
-    const uint32_t cb = 256;
-    const uint64_t blocks = std::min<uint64_t>((colour_rows + cb - 1) / cb, (uint64_t)num_sms * 16u);
-    k_view_colours<<<dim3((unsigned)blocks, n_views), cb, 0, stream>>>(d_views);
-    ++*launches;
-    GT_CUDA_TRY(cudaGetLastError());
-  }
+  Err ce = launch_view_colours(views, d_views, n_views, num_sms, stream, launches);
+  if (ce.code != GT_OK) return ce;
   const bool hand = packet && handoff && handoff->rays && handoff->cap && shape.handoff_after;
   if (packet) {
     Err e = launch_trace_packet(views, d_views, n_views, total_tiles, counters, faces, num_sms, stream, launches,
