@@ -581,6 +581,12 @@ def main():
                          "alg_bytes_per_launch": alg_bytes, "kernel_ms": k_ms,
                          "l2_hit_pct": prof.get("l2_hit_pct"), "l2_hit_source": prof.get("l2_hit_source"),
                          "issue": issue,
+                         # warp execution efficiency: active lanes per warp instruction of the
+                         # tile-packet kernel (a full ncu capture of the 960x540 case)
+                         "warp_exec_eff": ({"lanes_per_inst": prof["lanes_per_inst"],
+                                            "frac": prof["lanes_per_inst"] / 32.0,
+                                            "source": prof.get("lanes_source")}
+                                           if prof.get("lanes_per_inst") else None),
                          "timed": "a render's trace launches (large views: the tile-packet kernel and the "
                                   "warp-per-ray launch that finishes the rays it hands over)"},
             "cpu_baseline": cpu,
